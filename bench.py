@@ -1,0 +1,324 @@
+#!/usr/bin/env python3
+"""Benchmark of the FP64 gate-application path.
+
+Workload (one step): the 30-qubit random layered circuit — H on every qubit,
+then 20 layers of (a 1-qubit gate on each of the 30 qubits from {H, T, S, RX,
+RY, RZ, PHASESHIFT}, then CNOT/CZ/CPHASE on 15 disjoint random pairs) = 930
+gates on a 16 GiB complex128 state from |0..0>, reference CZ/CPHASE mask
+semantics. Seeded synthetic circuit (no dataset involved).
+
+  value  gates/s with the state resident in HBM (device time, CUDA events on
+         the engine's stream, max over ranks)
+  e2e    gates/s through the public C ABI call sequence with host buffers:
+         reset, qoa_apply of the host op list, qoa_get_state into pinned host
+         memory (16 GiB device->host each step)
+  roofline  the tile-pass kernel: 2 x 16 GiB algorithmic bytes per launch over
+         its CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs
+
+--impl reference times the reference's CPU algorithm (the oracle restatement,
+gate loops single-threaded as on x86-64, normalize on all cores) on the same
+circuit, a bounded number of gates per step.
+
+Multi-GPU: independent replicas, one per rank (the path has no exchange step);
+value = all ranks' gates / max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "random layered circuit, H layer + 20 layers", "n_qubits": 30, "gates": 930,
+            "state_bytes": 16 << 30, "dtype": "complex128", "cz_mask": "reference (index-as-mask)",
+            "l2_policy": "inputs larger than L2 (16 GiB state)", "seed": 1}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def aggregate(elapsed_ms: float, units: float, device=None):
+    """Max elapsed and summed units over ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return elapsed_ms, units
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_gates_per_s(ops_arr, n, max_gates, max_seconds):
+    """Times the oracle (faithful profile) gate by gate from the start of the
+    circuit; returns (gates/s, gates timed, threads)."""
+    from oracle import pyoracle as po
+    po.set_fast(False)
+    st = po.OracleState(n, 1)
+    t_total, k = 0.0, 0
+    for i in range(min(max_gates, len(ops_arr))):
+        t0 = time.perf_counter()
+        st.apply(ops_arr[i:i + 1])
+        t_total += time.perf_counter() - t0
+        k += 1
+        if t_total > max_seconds:
+            break
+    st.close()
+    return k / t_total, k, int(po.lib.orc_get_max_threads())
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+    from qoa_b200 import circuits as C
+    from oracle import pyoracle as po
+    n = WORKLOAD["n_qubits"]
+    ops = C.ops_to_array(C.layered_h_workload(n, 20, WORKLOAD["seed"]))
+    po.set_fast(False)
+    st = po.OracleState(n, 1)
+    per_step = args.ref_gates_per_step
+    pos = 0
+
+    def step():
+        nonlocal pos
+        for _ in range(per_step):
+            st.apply(ops[pos % len(ops): pos % len(ops) + 1])
+            pos += 1
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = args.steps * per_step / dt
+    threads = int(po.lib.orc_get_max_threads())
+    line = {"impl": "reference", "metric": "gates/s", "value": value, "unit": "gates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD),
+            "cpu_baseline": {"value": value, "unit": "gates/s", "cores": threads, "kind": "port",
+                             "sample": f"{per_step} gate(s) per step of the 930-gate circuit at n=30, in order, "
+                                       "faithful oracle: single-thread gate loop + all-core normalize"},
+            "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    st.close()
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+
+    n = WORKLOAD["n_qubits"]
+    ops_list = C.layered_h_workload(n, 20, WORKLOAD["seed"])
+    ops = C.ops_to_array(ops_list)
+    G = len(ops)
+
+    st = qb.QuantumState(n, compat_mask_quirk=True)
+    stream = torch.cuda.ExternalStream(st.stream_ptr(), device=dev)
+
+    def step():
+        st.apply_reset_all()
+        st.execute(ops)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    st.sync()
+    if ws > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = st.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    st.sync()
+    torch.cuda.synchronize()
+    launches = st.launch_count() - l0
+    elapsed = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    tmax, units = aggregate(elapsed, float(G * args.steps), dev if ws > 1 else None)
+    value = units / (tmax / 1e3)
+    ms_per_step = tmax / args.steps
+
+    # ---- roofline: per-launch times of the tile-pass kernel ----
+    prof = qb.QuantumState(n, compat_mask_quirk=True, profile=True)
+    prof.apply_reset_all()
+    prof.execute(ops)
+    prof.sync()
+    prof.launch_times()  # drop the warm-up records
+    prof.apply_reset_all()
+    prof.execute(ops)
+    ms, by, kind = prof.launch_times()
+    prof.close()
+    pass_ms = ms[kind == 0]
+    pass_bytes = by[kind == 0]
+    peak, peak_src = measured_peaks()
+    avg_ms = float(pass_ms.mean()) if pass_ms.size else float("nan")
+    achieved = float(pass_bytes.mean() / (avg_ms / 1e3) / 1e9) if pass_ms.size else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "kernel": "k_pass", "launches_per_step": int(pass_ms.size), "avg_launch_ms": avg_ms,
+                "algorithmic_bytes_per_launch": float(pass_bytes.mean()) if pass_ms.size else None,
+                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
+                "pass_share_of_step": float(pass_ms.sum() / ms.sum()) if ms.size else None}
+
+    # ---- e2e: host op list in, full state out to pinned host memory ----
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((1 << n) * 2, dtype=torch.float64, pin_memory=True)
+        hv = host.numpy().view(np.complex128)
+
+        def e2e_step():
+            st.apply_reset_all()
+            st.execute(ops)
+            st.get_state_vector(out=hv)
+
+        e2e_step()
+        st.sync()
+        if ws > 1:
+            dist.barrier()
+        k = max(1, min(args.steps, args.e2e_steps))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(k):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        et, eu = aggregate(e0.elapsed_time(e1), float(G * k), dev if ws > 1 else None)
+        e2e = {"value": eu / (et / 1e3), "unit": "gates/s", "h2d_bytes_per_step": int(ops.nbytes),
+               "d2h_bytes_per_step": int(hv.nbytes), "steps": k, "wall_s": wall}
+        del host
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        g, k, thr = cpu_gates_per_s(ops, n, args.cpu_gates, args.cpu_seconds)
+        cpu = {"value": g, "unit": "gates/s", "cores": thr, "kind": "port",
+               "sample": f"first {k} gates of the same 930-gate circuit at n=30 (16 GiB), faithful oracle: "
+                         "single-thread gate loop + all-core normalize after each gate"}
+
+    if rank == 0:
+        line = {"metric": "gates/s", "value": value, "unit": "gates/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD),
+                "effective_gbs": C.algorithmic_bytes(ops_list, n, quirk=True) * args.steps * ws / (tmax / 1e3) / 1e9,
+                "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "impl": "qoa_b200"}
+        print(json.dumps(line), flush=True)
+    st.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-gates", type=int, default=12)
+    ap.add_argument("--cpu-seconds", type=float, default=25.0)
+    ap.add_argument("--ref-gates-per-step", type=int, default=1)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

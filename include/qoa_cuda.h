@@ -1,0 +1,225 @@
+/*
+ * qoa_cuda.h — C ABI of the B200 (sm_100a) state-vector engine that replaces the
+ * gate-application hot path of the QOA executor.
+ *
+ * Two layers are exported:
+ *
+ *  (i)  The handle API (qoa_create ... qoa_last_error). It replaces the amplitude
+ *       ownership of `QuantumState` (src/runtime/quantum_state.rs:38-53) and the
+ *       per-gate methods that call into src/vectorization.rs. The amplitudes live
+ *       in HBM for the lifetime of the handle; gates are submitted as an op list
+ *       that uses the reference's opcode numbers (src/instructions.rs:631-830).
+ *
+ *  (ii) Slice-level shims (qoa_vec_*). One per `pub fn apply_*_vectorized` in
+ *       src/vectorization.rs:16-902, with the same argument meaning: the caller
+ *       owns a host `&mut [Complex64]` (interleaved re/im f64, `len` complex
+ *       elements) that is updated in place. Each call copies host->device,
+ *       runs one kernel and copies back, so they exist for line-for-line
+ *       compatibility, not speed.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: QOA_OK (0) or a QOA_E_* code.
+ *     No C++ exception crosses the ABI.
+ *   - Amplitude layout: interleaved {re, im} complex128 (num-complex
+ *     `Complex64` is #[repr(C)]), index bit q <-> qubit q (qubit 0 = LSB),
+ *     exactly as src/vectorization.rs:920-935 indexes it.
+ *   - Each handle owns one CUDA stream. Distinct handles may be used from
+ *     distinct threads; one handle must not be used from two threads at once
+ *     (the reference's QuantumState is not shared across threads either).
+ *   - Gate ops whose qubits are out of range (or equal where they must be
+ *     distinct) are skipped, the way QuantumState prints and no-ops them
+ *     (e.g. quantum_state.rs:189-195, 318-321); qoa_apply then returns
+ *     QOA_E_RANGE after applying every valid op, and qoa_last_error() names
+ *     the first skipped op.
+ *   - After every gate the reference renormalises (apply_noise -> normalize,
+ *     quantum_state.rs:839-907). The engine keeps that contract: the state that
+ *     any read observes is normalised, and a state whose squared norm is not
+ *     above 1e-12 (or is NaN) is reset to |0...0>, as normalize() does.
+ */
+#ifndef QOA_CUDA_H
+#define QOA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define QOA_OK        0
+#define QOA_E_RANGE   1  /* qubit index out of range / equal qubits: op skipped, state untouched */
+#define QOA_E_ARG     2  /* null pointer, size mismatch, bad enum value */
+#define QOA_E_OPCODE  3  /* opcode not supported by the engine */
+#define QOA_E_CUDA    4  /* a CUDA runtime call failed */
+#define QOA_E_OOM     5  /* device allocation failed */
+#define QOA_E_STATE   6  /* numerical status: NaN/Inf seen (see qoa_status) */
+#define QOA_E_NOGPU   7  /* no CUDA device visible */
+
+/* ---- precision -------------------------------------------------------- */
+#define QOA_PREC_F64  0  /* complex128 amplitudes: the plain (drop-in) method */
+
+/* ---- handle flags ------------------------------------------------------ */
+/* CZ / CPHASE condition mask. The reference's QuantumState passes the raw
+ * qubit INDICES into apply_cz_vectorized / apply_controlled_phase_rotation_
+ * vectorized, whose parameters are MASKS (quantum_state.rs:338,356-361 ->
+ * vectorization.rs:745,788), so the phase lands on every i with
+ * (i & (c|t)) == (c|t). With this flag the engine reproduces that; without it
+ * the mask is (1<<c)|(1<<t), the physical CZ. */
+#define QOA_FLAG_COMPAT_MASK_QUIRK  0x1u
+/* One kernel launch per gate (no multi-gate passes). For comparison runs. */
+#define QOA_FLAG_PER_GATE           0x2u
+/* Record a CUDA event pair around every launch (qoa_launch_times). */
+#define QOA_FLAG_PROFILE            0x4u
+/* Depolarising noise only on the qubits the gate touched (the reference
+ * applies it to every qubit after every gate, quantum_state.rs:872-885). */
+#define QOA_FLAG_NOISE_GATE_QUBITS  0x8u
+
+/* ---- opcodes: the reference byte code numbers (src/instructions.rs) ---- */
+#define QOA_OP_APPLYGATE   0x02  /* q[0]=qubit, q[1]= 'H','X','Y','Z','T','S' (execute_arithmetic APPLYGATE) */
+#define QOA_OP_QINIT       0x04  /* q[0]=qubit count: state re-created as max(n,1) qubits in |0..0> */
+#define QOA_OP_H           0x05
+#define QOA_OP_Z           0x06
+#define QOA_OP_X           0x07
+#define QOA_OP_P           0x08  /* PHASESHIFT(q, angle) */
+#define QOA_OP_RESET       0x0A
+#define QOA_OP_SWAP        0x0B
+#define QOA_OP_CSWAP       0x0C  /* q = {control, t1, t2} */
+#define QOA_OP_T           0x0D
+#define QOA_OP_S           0x0E
+#define QOA_OP_RZ          0x0F
+#define QOA_OP_ENTANGLE    0x11  /* = CNOT(q0,q1) */
+#define QOA_OP_EBELL       0x12  /* H(q0); CNOT(q0,q1) */
+#define QOA_OP_EMULTI      0x13  /* H(first); CNOT(first, q) for the rest (list op) */
+#define QOA_OP_ECLUSTER    0x14  /* H on all; CZ on neighbour pairs (list op) */
+#define QOA_OP_ESWAP       0x15  /* CNOT(a,c); CNOT(b,d); SWAP(c,d) */
+#define QOA_OP_ESWAPM      0x16  /* ESWAP then MEASURE c, MEASURE d */
+#define QOA_OP_CNOT        0x17
+#define QOA_OP_ECFB        0x19  /* = CNOT(q0,q1) */
+#define QOA_OP_EDIST       0x1A  /* no-op (placeholder in the reference) */
+#define QOA_OP_MEASB       0x1B  /* q[1] = 'X','Y','Z' basis */
+#define QOA_OP_RESETALL    0x1C
+#define QOA_OP_SETPHASE    0x1D  /* = PHASESHIFT */
+#define QOA_OP_CZ          0x1E
+#define QOA_OP_RX          0x22
+#define QOA_OP_RY          0x23
+#define QOA_OP_PHASE       0x24  /* = PHASESHIFT */
+#define QOA_OP_MEASURE     0x32
+#define QOA_OP_ROT         0x33  /* q[1] = 'X','Y','Z' axis */
+#define QOA_OP_CPHASE      0x35
+/* Engine extensions in the opcode range the reference leaves unused
+ * (0xF0-0xFE; 0xFF is HALT). Each names the QuantumState method it exposes. */
+#define QOA_OP_Y           0xF0  /* apply_y (quantum_state.rs:213) */
+#define QOA_OP_U1          0xF1  /* apply_custom_unitary: matrix = 4 complex (8 doubles), row-major */
+#define QOA_OP_U2          0xF2  /* apply_two_qubit_unitary(q0,q1): 16 complex (32 doubles) */
+#define QOA_OP_TOFFOLI     0xF3  /* apply_toffoli(c1,c2,t) */
+#define QOA_OP_CY          0xF4  /* apply_controlled_y(c,t) */
+
+/* One instruction. `nq` operands are in q[0..3]; list ops (EMULTI/ECLUSTER)
+ * with more than 4 qubits pass them through `qlist` instead. `matrix` is read
+ * only by U1/U2. */
+typedef struct qoa_op {
+    uint32_t opcode;
+    uint32_t nq;
+    uint32_t q[4];
+    double angle;
+    const uint32_t* qlist;
+    const double* matrix;
+} qoa_op;
+
+typedef struct qoa_state_s* qoa_state_t;
+
+/* Numerical status flags (Status{nan, div_by_zero, overflow},
+ * quantum_state.rs:27-35, plus the normalize() reset counter). */
+typedef struct qoa_status_t {
+    uint32_t nan_seen;
+    uint32_t inf_seen;
+    uint32_t zero_norm_resets;  /* times normalize() found norm^2 <= 1e-12 and reset to |0..0> */
+    uint32_t reserved;
+} qoa_status_t;
+
+/* ---- (i) handle API ----------------------------------------------------- */
+
+/* QuantumState::new (quantum_state.rs:56-90): n = max(n,1) qubits in |0..0>. */
+int qoa_create(uint32_t n, int precision, uint32_t flags, qoa_state_t* out);
+int qoa_destroy(qoa_state_t s);
+int qoa_num_qubits(qoa_state_t s, uint32_t* n);
+/* apply_reset_all (quantum_state.rs:183-186). */
+int qoa_reset_all(qoa_state_t s);
+/* The per-gate methods (quantum_state.rs:171-397) and execute_arithmetic's
+ * instruction dispatch (quantum_state.rs:460-565), for a list of ops. Work is
+ * queued on the handle's stream; MEASURE-type ops synchronise. */
+int qoa_apply(qoa_state_t s, const qoa_op* ops, size_t nops);
+/* measure (quantum_state.rs:399-458) with a caller-supplied uniform u in
+ * [0,1): outcome = (u < P0) ? 0 : 1. A negative u draws from the handle's
+ * counter-based RNG (qoa_seed). */
+int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome);
+/* Shots. mode 0 = measure_all order (quantum_state.rs:909-918): qubits 0..n-1
+ * measured one after another, n uniforms per shot (u[shot*n + q]); mode 1 =
+ * inverse-CDF over the full distribution, one uniform per shot. out[shot]
+ * holds the outcome bits (bit q = qubit q). The state is left unchanged, as
+ * measure_all measures a clone. */
+int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t* out);
+/* get_probabilities (quantum_state.rs:128-133): 2^n doubles. */
+int qoa_probabilities(qoa_state_t s, double* out);
+/* <Z_mask> = sum_i (-1)^popcount(i & mask) |a_i|^2 for k masks. */
+int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out);
+/* get_state_vector / set_state_vector (quantum_state.rs:1129-1145); set
+ * renormalises. bytes must be 2^n * 16. */
+int qoa_get_state(qoa_state_t s, void* host, size_t bytes);
+int qoa_set_state(qoa_state_t s, const void* host, size_t bytes);
+/* seed_rng (quantum_state.rs:956): seeds the handle's Philox4x32-10 stream. */
+int qoa_seed(qoa_state_t s, uint64_t seed);
+/* NoiseConfig (quantum_state.rs:15-24): mode 0 Ideal, 1 Fixed(p), 2 Random. */
+int qoa_set_noise(qoa_state_t s, int mode, double p);
+/* Selects the Philox stream of the noise and MEASURE draws (one per Pauli
+ * trajectory) and restarts its event counter. No reference counterpart: the
+ * reference's StdRng stream is not addressable (quantum_state.rs:76). */
+int qoa_set_trajectory(qoa_state_t s, uint64_t trajectory);
+int qoa_status(qoa_state_t s, qoa_status_t* out);
+/* Blocks until the handle's queued work is done. */
+int qoa_sync(qoa_state_t s);
+/* The handle's cudaStream_t, so a caller can order its own work against it. */
+int qoa_stream(qoa_state_t s, void** stream);
+/* Kernel launches issued by this handle since creation. */
+int qoa_launch_count(qoa_state_t s, uint64_t* count);
+/* With QOA_FLAG_PROFILE: per-launch device times (ms) and algorithmic bytes of
+ * the launches since the last call; returns the count in *n (<= cap). */
+int qoa_launch_times(qoa_state_t s, double* ms, double* bytes, int* kind, size_t cap, size_t* n);
+const char* qoa_last_error(qoa_state_t s);
+const char* qoa_strerror(int code);
+
+/* ---- plan introspection (host only, no GPU needed) ---------------------- */
+/* Runs the pass scheduler on an op list for an n-qubit state and writes, for
+ * each expanded gate in submission order, the index of the pass that applies
+ * it (pass_of[i]) and the order within the pass (order[i]); *npasses receives
+ * the pass count and *ngates the expanded gate count (<= cap). */
+int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t cap,
+             int32_t* pass_of, int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits,
+             double* gate_matrix, size_t* ngates, size_t* npasses);
+
+/* ---- (ii) slice-level shims: src/vectorization.rs pub fns ---------------- */
+/* `amps` points to `len` interleaved complex128 values in host memory. */
+int qoa_vec_apply_hadamard(double* amps, size_t len, double norm_re, double norm_im, size_t mask_bit); /* vectorization.rs:16 */
+int qoa_vec_apply_x(double* amps, size_t len, size_t mask_bit);                                         /* vectorization.rs:69 */
+int qoa_vec_apply_y(double* amps, size_t len, size_t mask_bit);                                         /* vectorization.rs:118 */
+int qoa_vec_apply_z(double* amps, size_t len, size_t mask_bit);                                         /* vectorization.rs:173 */
+int qoa_vec_apply_t(double* amps, size_t len, size_t mask_bit);                                         /* vectorization.rs:217 */
+int qoa_vec_apply_s(double* amps, size_t len, size_t mask_bit);                                         /* vectorization.rs:262 */
+int qoa_vec_apply_phaseshift(double* amps, size_t len, size_t mask_bit, double angle);                  /* vectorization.rs:307 */
+int qoa_vec_apply_reset(double* amps, size_t len, size_t mask_bit);                                     /* vectorization.rs:352 */
+int qoa_vec_apply_swap(double* amps, size_t len, size_t q1, size_t q2);                                 /* vectorization.rs:421 */
+int qoa_vec_apply_controlled_swap(double* amps, size_t len, size_t control, size_t target1, size_t target2); /* vectorization.rs:469 */
+int qoa_vec_apply_rx(double* amps, size_t len, size_t mask_bit, double angle);                          /* vectorization.rs:528 */
+int qoa_vec_apply_ry(double* amps, size_t len, size_t mask_bit, double angle);                          /* vectorization.rs:588 */
+int qoa_vec_apply_rz(double* amps, size_t len, size_t mask_bit, double angle);                          /* vectorization.rs:648 */
+int qoa_vec_apply_cnot(double* amps, size_t len, size_t control, size_t target);                        /* vectorization.rs:699 */
+int qoa_vec_apply_cz(double* amps, size_t len, size_t control_mask, size_t target_mask);                /* vectorization.rs:745 */
+int qoa_vec_apply_controlled_phase_rotation(double* amps, size_t len, size_t control_mask,
+                                            size_t target_mask, double angle);                          /* vectorization.rs:788 */
+int qoa_vec_apply_reset_all(double* amps, size_t len);                                                  /* vectorization.rs:857 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QOA_CUDA_H */

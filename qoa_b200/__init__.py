@@ -1,0 +1,356 @@
+"""qoa_b200 — B200 (sm_100a) state-vector engine for the QOA gate-application path.
+
+Python mirror of the reference's ``QuantumState`` (src/runtime/quantum_state.rs)
+over the C ABI of ``include/qoa_cuda.h`` (``libqoa_cuda.so``, built in-tree by
+``make -C qoa_b200``). Method names, argument meaning and error behaviour follow
+the reference: gate methods given an out-of-range qubit print an error and do
+nothing (quantum_state.rs:189-195); ``measure`` raises on a bad qubit
+(quantum_state.rs:400-402). There is no CPU fallback: importing this package
+without the CUDA library raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import circuits  # noqa: F401  (seeded circuit generators)
+from .circuits import OP_DTYPE, Op, ops_to_array
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqoa_cuda.so")
+
+QOA_OK, QOA_E_RANGE, QOA_E_ARG, QOA_E_OPCODE, QOA_E_CUDA, QOA_E_OOM, QOA_E_STATE, QOA_E_NOGPU = range(8)
+QOA_PREC_F64 = 0
+QOA_FLAG_COMPAT_MASK_QUIRK = 0x1
+QOA_FLAG_PER_GATE = 0x2
+QOA_FLAG_PROFILE = 0x4
+QOA_FLAG_NOISE_GATE_QUBITS = 0x8
+
+
+class QoaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class QoaStatus(ctypes.Structure):
+    _fields_ = [("nan_seen", ctypes.c_uint32), ("inf_seen", ctypes.c_uint32),
+                ("zero_norm_resets", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"qoa_b200: {LIB_PATH} is missing; build it with `make -C qoa_b200` "
+                          "(or __graft_entry__.build()). The engine has no CPU fallback.")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, u32, u64, sz, dbl, i32 = (ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t,
+                                  ctypes.c_double, ctypes.c_int)
+    P = ctypes.POINTER
+    sig = {
+        "qoa_create": (i32, [u32, i32, u32, P(vp)]),
+        "qoa_destroy": (i32, [vp]),
+        "qoa_num_qubits": (i32, [vp, P(u32)]),
+        "qoa_reset_all": (i32, [vp]),
+        "qoa_apply": (i32, [vp, vp, sz]),
+        "qoa_measure": (i32, [vp, u32, dbl, P(u32)]),
+        "qoa_sample": (i32, [vp, vp, sz, i32, vp]),
+        "qoa_probabilities": (i32, [vp, vp]),
+        "qoa_expect_z": (i32, [vp, vp, sz, vp]),
+        "qoa_get_state": (i32, [vp, vp, sz]),
+        "qoa_set_state": (i32, [vp, vp, sz]),
+        "qoa_seed": (i32, [vp, u64]),
+        "qoa_set_noise": (i32, [vp, i32, dbl]),
+        "qoa_set_trajectory": (i32, [vp, u64]),
+        "qoa_status": (i32, [vp, P(QoaStatus)]),
+        "qoa_sync": (i32, [vp]),
+        "qoa_stream": (i32, [vp, P(vp)]),
+        "qoa_launch_count": (i32, [vp, P(u64)]),
+        "qoa_launch_times": (i32, [vp, vp, vp, vp, sz, P(sz)]),
+        "qoa_last_error": (ctypes.c_char_p, [vp]),
+        "qoa_strerror": (ctypes.c_char_p, [i32]),
+        "qoa_plan": (i32, [u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, P(sz), P(sz)]),
+        "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
+        "qoa_vec_apply_x": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_y": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_z": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_t": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_s": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_phaseshift": (i32, [vp, sz, sz, dbl]),
+        "qoa_vec_apply_reset": (i32, [vp, sz, sz]),
+        "qoa_vec_apply_swap": (i32, [vp, sz, sz, sz]),
+        "qoa_vec_apply_controlled_swap": (i32, [vp, sz, sz, sz, sz]),
+        "qoa_vec_apply_rx": (i32, [vp, sz, sz, dbl]),
+        "qoa_vec_apply_ry": (i32, [vp, sz, sz, dbl]),
+        "qoa_vec_apply_rz": (i32, [vp, sz, sz, dbl]),
+        "qoa_vec_apply_cnot": (i32, [vp, sz, sz, sz]),
+        "qoa_vec_apply_cz": (i32, [vp, sz, sz, sz]),
+        "qoa_vec_apply_controlled_phase_rotation": (i32, [vp, sz, sz, sz, dbl]),
+        "qoa_vec_apply_reset_all": (i32, [vp, sz]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc: int, h=None, allow_range: bool = False) -> int:
+    if rc == QOA_OK:
+        return rc
+    msg = (lib.qoa_last_error(h) or b"").decode(errors="replace")
+    if rc == QOA_E_RANGE and allow_range:
+        # QuantumState prints the error and leaves the state untouched
+        print(f"error: {msg}", file=sys.stderr)
+        return rc
+    raise QoaError(rc, msg or lib.qoa_strerror(rc).decode())
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class NoiseConfig:
+    """NoiseConfig (quantum_state.rs:15-24): Random, Fixed(p) or Ideal."""
+
+    def __init__(self, kind: str, p: float = 0.0):
+        if kind not in ("random", "fixed", "ideal"):
+            raise ValueError(kind)
+        self.kind, self.p = kind, float(p)
+
+    @classmethod
+    def Random(cls):
+        return cls("random")
+
+    @classmethod
+    def Fixed(cls, p: float):
+        return cls("fixed", p)
+
+    @classmethod
+    def Ideal(cls):
+        return cls("ideal")
+
+    @property
+    def mode(self) -> int:
+        return {"ideal": 0, "fixed": 1, "random": 2}[self.kind]
+
+
+class QuantumState:
+    """Dense complex128 state vector resident in HBM (QuantumState::new,
+    quantum_state.rs:56-90)."""
+
+    def __init__(self, n_qubits: int, noise_config: Optional[NoiseConfig] = None, *,
+                 compat_mask_quirk: bool = False, per_gate: bool = False, profile: bool = False,
+                 noise_gate_qubits_only: bool = False, seed: int = 0):
+        flags = ((QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0)
+                 | (QOA_FLAG_PER_GATE if per_gate else 0)
+                 | (QOA_FLAG_PROFILE if profile else 0)
+                 | (QOA_FLAG_NOISE_GATE_QUBITS if noise_gate_qubits_only else 0))
+        h = ctypes.c_void_p()
+        _check(lib.qoa_create(max(int(n_qubits), 1), QOA_PREC_F64, flags, ctypes.byref(h)))
+        self._h = h
+        self.flags = flags
+        self.noise_config = noise_config
+        self.seed_rng(seed)
+        if noise_config is not None:
+            self.set_noise_config(noise_config)
+
+    # ---- lifetime -------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.qoa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def n(self) -> int:
+        v = ctypes.c_uint32()
+        _check(lib.qoa_num_qubits(self._h, ctypes.byref(v)), self._h)
+        return int(v.value)
+
+    def get_num_qubits(self) -> int:
+        return self.n
+
+    # ---- bulk execution ---------------------------------------------------
+    def execute(self, ops) -> int:
+        """Applies an op list (qoa_op records, reference opcode numbers)."""
+        arr = ops if isinstance(ops, np.ndarray) else ops_to_array(ops)
+        if arr.dtype != OP_DTYPE:
+            raise TypeError("ops must use circuits.OP_DTYPE")
+        arr = np.ascontiguousarray(arr)
+        return _check(lib.qoa_apply(self._h, _ptr(arr), len(arr)), self._h, allow_range=True)
+
+    def _one(self, opcode: int, *qs: int, angle: float = 0.0, matrix=None) -> int:
+        return self.execute([Op(opcode, list(qs), angle, matrix)])
+
+    # ---- gate methods (quantum_state.rs:171-397, 960-1212) -----------------
+    def apply_h(self, q): return self._one(0x05, q)
+    def apply_x(self, q): return self._one(0x07, q)
+    def apply_y(self, q): return self._one(0xF0, q)
+    def apply_phase_flip(self, q): return self._one(0x06, q)
+    def apply_t_gate(self, q): return self._one(0x0D, q)
+    def apply_s_gate(self, q): return self._one(0x0E, q)
+    def apply_phase_shift(self, q, angle): return self._one(0x08, q, angle=angle)
+    def apply_rx(self, q, angle): return self._one(0x22, q, angle=angle)
+    def apply_ry(self, q, angle): return self._one(0x23, q, angle=angle)
+    def apply_rz(self, q, angle): return self._one(0x0F, q, angle=angle)
+    def apply_cnot(self, c, t): return self._one(0x17, c, t)
+    def apply_cz(self, c, t): return self._one(0x1E, c, t)
+    def apply_controlled_phase(self, c, t, angle): return self._one(0x35, c, t, angle=angle)
+    def apply_swap(self, a, b): return self._one(0x0B, a, b)
+    def apply_controlled_swap(self, c, a, b): return self._one(0x0C, c, a, b)
+    def apply_toffoli(self, c1, c2, t): return self._one(0xF3, c1, c2, t)
+    def apply_controlled_y(self, c, t): return self._one(0xF4, c, t)
+    def reset_qubit(self, q): return self._one(0x0A, q)
+    def apply_reset_all(self): return _check(lib.qoa_reset_all(self._h), self._h)
+
+    def apply_custom_unitary(self, q, u: Sequence[complex]):
+        m = np.ascontiguousarray(np.asarray(u, dtype=np.complex128).reshape(4))
+        return self._one(0xF1, q, matrix=m)
+
+    def apply_two_qubit_unitary(self, q1, q2, u: Sequence[complex]):
+        m = np.ascontiguousarray(np.asarray(u, dtype=np.complex128).reshape(16))
+        return self._one(0xF2, q1, q2, matrix=m)
+
+    # ---- measurement --------------------------------------------------------
+    def measure(self, q: int, u: Optional[float] = None) -> int:
+        """measure (quantum_state.rs:399-458): outcome = (u < P0) ? 0 : 1. Without
+        `u` the handle's seeded Philox stream supplies the draw."""
+        out = ctypes.c_uint32()
+        _check(lib.qoa_measure(self._h, int(q), -1.0 if u is None else float(u), ctypes.byref(out)), self._h)
+        return int(out.value)
+
+    def sample(self, shots: int, u: Optional[np.ndarray] = None, mode: int = 0, rng_seed: int = 0) -> np.ndarray:
+        """Shots without disturbing the state. mode 0 reproduces measure_all's
+        qubit-by-qubit draw order (n uniforms per shot); mode 1 is inverse CDF."""
+        n = self.n
+        need = shots * n if mode == 0 else shots
+        if u is None:
+            u = np.random.default_rng(rng_seed).random(need)
+        u = np.ascontiguousarray(np.asarray(u, dtype=np.float64).reshape(-1))
+        if u.size != need:
+            raise ValueError(f"need {need} uniforms")
+        out = np.empty(shots, dtype=np.uint64)
+        _check(lib.qoa_sample(self._h, _ptr(u), shots, mode, _ptr(out)), self._h)
+        return out
+
+    def measure_all(self, u: Optional[np.ndarray] = None) -> list:
+        """measure_all (quantum_state.rs:909-918): one shot, outcome per qubit."""
+        bits = int(self.sample(1, u, mode=0)[0])
+        return [(bits >> q) & 1 for q in range(self.n)]
+
+    # ---- state access -------------------------------------------------------
+    def get_probabilities(self) -> np.ndarray:
+        out = np.empty(1 << self.n, dtype=np.float64)
+        _check(lib.qoa_probabilities(self._h, _ptr(out)), self._h)
+        return out
+
+    def get_state_vector(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        n = self.n
+        if out is None:
+            out = np.empty(1 << n, dtype=np.complex128)
+        _check(lib.qoa_get_state(self._h, _ptr(out), out.nbytes), self._h)
+        return out
+
+    def set_state_vector(self, amps: np.ndarray):
+        a = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128))
+        _check(lib.qoa_set_state(self._h, _ptr(a), a.nbytes), self._h)
+
+    def expect_z(self, masks: Iterable[int]) -> np.ndarray:
+        m = np.ascontiguousarray(np.asarray(list(masks), dtype=np.uint64))
+        out = np.empty(len(m), dtype=np.float64)
+        _check(lib.qoa_expect_z(self._h, _ptr(m), len(m), _ptr(out)), self._h)
+        return out
+
+    # ---- configuration --------------------------------------------------------
+    def seed_rng(self, seed: int):
+        _check(lib.qoa_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF), self._h)
+
+    def set_trajectory(self, t: int):
+        _check(lib.qoa_set_trajectory(self._h, int(t)), self._h)
+
+    def set_noise_config(self, cfg: Optional[NoiseConfig]):
+        self.noise_config = cfg
+        mode, p = (0, 0.0) if cfg is None else (cfg.mode, cfg.p)
+        _check(lib.qoa_set_noise(self._h, mode, p), self._h)
+
+    def get_noise_config(self):
+        return self.noise_config
+
+    def get_status(self) -> dict:
+        st = QoaStatus()
+        _check(lib.qoa_status(self._h, ctypes.byref(st)), self._h)
+        return {"nan": bool(st.nan_seen), "overflow": bool(st.inf_seen), "zero_norm_resets": st.zero_norm_resets}
+
+    # ---- engine plumbing --------------------------------------------------------
+    def sync(self):
+        _check(lib.qoa_sync(self._h), self._h)
+
+    def stream_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        _check(lib.qoa_stream(self._h, ctypes.byref(p)), self._h)
+        return int(p.value or 0)
+
+    def launch_count(self) -> int:
+        v = ctypes.c_uint64()
+        _check(lib.qoa_launch_count(self._h, ctypes.byref(v)), self._h)
+        return int(v.value)
+
+    def launch_times(self, cap: int = 1 << 16):
+        ms = np.empty(cap, dtype=np.float64)
+        by = np.empty(cap, dtype=np.float64)
+        kd = np.empty(cap, dtype=np.int32)
+        n = ctypes.c_size_t()
+        _check(lib.qoa_launch_times(self._h, _ptr(ms), _ptr(by), _ptr(kd), cap, ctypes.byref(n)), self._h)
+        k = n.value
+        return ms[:k].copy(), by[:k].copy(), kd[:k].copy()
+
+
+def plan(n: int, ops, flags: int = 0):
+    """Runs the host pass scheduler without a GPU. Returns per expanded gate
+    (pass index, order in pass, kind code, qubits[4], matrix[16] complex) and the
+    pass count."""
+    arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
+    ng, npasses = ctypes.c_size_t(), ctypes.c_size_t()
+    lib.qoa_plan(n, flags, _ptr(arr), len(arr), 0, None, None, None, None, None, ctypes.byref(ng), ctypes.byref(npasses))
+    cap = ng.value
+    pass_of = np.empty(max(cap, 1), dtype=np.int32)
+    order = np.empty(max(cap, 1), dtype=np.int32)
+    kind = np.empty(max(cap, 1), dtype=np.int32)
+    qubits = np.empty((max(cap, 1), 4), dtype=np.uint32)
+    mat = np.empty((max(cap, 1), 16), dtype=np.complex128)
+    _check(lib.qoa_plan(n, flags, _ptr(arr), len(arr), cap, _ptr(pass_of), _ptr(order), _ptr(kind), _ptr(qubits),
+                        _ptr(mat), ctypes.byref(ng), ctypes.byref(npasses)))
+    k = ng.value
+    return {"pass_of": pass_of[:k], "order": order[:k], "kind": kind[:k], "qubits": qubits[:k],
+            "matrix": mat[:k], "npasses": npasses.value}
+
+
+def vec_call(name: str, amps: np.ndarray, *args) -> int:
+    """Calls a vectorization.rs shim (qoa_vec_apply_<name>) on a host
+    complex128 array in place."""
+    if amps.dtype != np.complex128 or not amps.flags.c_contiguous:
+        raise TypeError("amps must be a C-contiguous complex128 array")
+    f = getattr(lib, "qoa_vec_apply_" + name)
+    return _check(f(_ptr(amps), amps.size, *args))

@@ -1,0 +1,1367 @@
+// qoa_engine.cpp — host side of the engine: the C ABI of include/qoa_cuda.h,
+// instruction expansion with QuantumState's semantics, the pass scheduler that
+// groups gates into single-sweep tile passes, and the vectorization.rs shims.
+//
+// Reference correspondence (paths inside planetryan/qoa):
+//   QuantumState gate methods      src/runtime/quantum_state.rs:171-397
+//   execute_arithmetic dispatch    src/runtime/quantum_state.rs:460-705
+//   measure / measure_all          src/runtime/quantum_state.rs:399-458, 909-918
+//   apply_noise / normalize        src/runtime/quantum_state.rs:839-907
+//   matrix set-up per gate         src/vectorization.rs:16-902
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qoa_cuda.h"
+#include "qoa_kernels.cuh"
+
+namespace qoa {
+cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials, cudaStream_t st);
+cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st);
+int reduce_blocks(uint64_t len);
+cudaError_t launch_norm(const double2* a, uint64_t len, double* partials, double* out, uint32_t* status, cudaStream_t st);
+cudaError_t launch_p01(const double2* a, uint64_t len, uint32_t q, double* partials, double* out2, const double* norm2,
+                       cudaStream_t st);
+cudaError_t launch_expz(const double2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials, double* out,
+                        const double* norm2, cudaStream_t st);
+cudaError_t launch_reduce_partials(const double* partials, uint32_t count, double* out, uint32_t* status, cudaStream_t st);
+cudaError_t launch_collapse(double2* a, uint64_t len, uint32_t q, uint32_t outcome, double f, double* partials,
+                            double* norm2_out, uint32_t* status, cudaStream_t st);
+cudaError_t launch_materialize(double2* a, uint64_t len, double* norm2, double* partials, uint32_t* status, cudaStream_t st);
+cudaError_t launch_set_scalar(double* p, double v, cudaStream_t st);
+cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const double* norm2, double* out, cudaStream_t st);
+cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st);
+cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
+                          uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
+}  // namespace qoa
+
+using namespace qoa;
+
+namespace {
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Draw (seed; stream,
+// event, slot) -> uniform double in [0,1) from the top 53 bits of words 0-1.
+void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+double uniform01(uint64_t seed, uint64_t stream, uint64_t event, uint32_t slot) {
+    uint32_t c[4] = {(uint32_t)event, (uint32_t)(event >> 32), slot, (uint32_t)stream};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t bits = ((uint64_t)c[0] << 32) | c[1];
+    return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+const uint64_t kMeasStreamXor = 0x6d656173ull;
+
+// ------------------------------------------------------------------ gates
+enum GateKind { K_G1 = 0, K_DIAG = 1, K_SWAP = 2, K_U2 = 3, K_MEASURE = 4, K_RESET = 5, K_RESETALL = 6, K_QINIT = 7 };
+
+struct Gate {
+    int kind = K_G1;
+    int sub = G1_GEN;
+    int t = 0, t2 = 0;      // target(s); K_DIAG: selector qubit or -1
+    uint64_t cmask = 0;     // condition mask over global qubits
+    bool neg = false;       // K_DIAG: factor -1
+    double2 m[16];
+    uint64_t nmask = 0;     // qubits acted on non-diagonally
+    uint64_t dmask = 0;     // qubits acted on diagonally (controls, phase masks, selector)
+    int src = -1;           // source op index
+    double u = -1.0;        // K_MEASURE: uniform
+};
+
+inline double2 d2(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
+inline double2 from_polar(double r, double t) { return d2(r * std::cos(t), r * std::sin(t)); }
+
+bool is_pass_gate(const Gate& g) { return g.kind == K_G1 || g.kind == K_DIAG; }
+bool is_barrier(const Gate& g) { return g.kind >= K_MEASURE; }
+
+// Algorithmic bytes of one per-gate application, S = 2^n * 16.
+double gate_bytes(const Gate& g, uint32_t n) {
+    const double S = std::ldexp(16.0, (int)n);
+    auto pc = [](uint64_t x) { return (double)__builtin_popcountll(x); };
+    switch (g.kind) {
+        case K_G1: return 2.0 * S / std::ldexp(1.0, (int)pc(g.cmask));
+        case K_DIAG: return g.t >= 0 ? 2.0 * S : 2.0 * S / std::ldexp(1.0, (int)pc(g.cmask));
+        case K_SWAP: return S / std::ldexp(1.0, (int)pc(g.cmask));
+        case K_U2: return 2.0 * S;
+        default: return 2.0 * S;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ handle
+struct qoa_state_s {
+    uint32_t n = 1;
+    uint32_t flags = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double2* amps = nullptr;
+    double* scal = nullptr;       // [0] norm2, [1] P0, [2] P1, [3..] scratch
+    uint32_t* status = nullptr;   // device status words
+    double* partials = nullptr;
+    size_t partials_cap = 0;
+    double* host_scal = nullptr;  // pinned mirror of scal
+    uint64_t seed = 0;
+    uint64_t noise_stream = 0;
+    uint64_t noise_event = 0;
+    uint64_t meas_draws = 0;
+    int noise_mode = 0;
+    double noise_p = 0.0;
+    uint64_t launches = 0;
+    uint32_t host_resets = 0;     // normalize() resets decided on the host
+    std::string err;
+    // profiling
+    struct Rec { cudaEvent_t a, b; double bytes; int kind; };
+    std::vector<Rec> recs;
+};
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;  // errors before a handle exists
+
+int set_err(qoa_state_t s, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    else {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return set_err(s, e_ == cudaErrorMemoryAllocation ? QOA_E_OOM : QOA_E_CUDA,   \
+                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+uint64_t state_len(const qoa_state_t s) { return 1ull << s->n; }
+
+size_t partials_needed(uint32_t n) {
+    size_t a = (n >= (uint32_t)TILE_BITS) ? (size_t)1 << (n - TILE_BITS) : 1;
+    size_t b = (size_t)8 * (size_t)reduce_blocks(1ull << n);
+    return std::max(a, b);
+}
+
+int alloc_state(qoa_state_t s, uint32_t n) {
+    if (s->amps) { cudaFree(s->amps); s->amps = nullptr; }
+    if (s->partials) { cudaFree(s->partials); s->partials = nullptr; }
+    s->n = n;
+    CK(cudaMalloc(&s->amps, sizeof(double2) << n));
+    s->partials_cap = partials_needed(n);
+    CK(cudaMalloc(&s->partials, s->partials_cap * sizeof(double)));
+    return QOA_OK;
+}
+
+struct Timer {
+    qoa_state_t s;
+    cudaEvent_t a = nullptr;
+    double bytes;
+    int kind;
+    Timer(qoa_state_t st, double b, int k) : s(st), bytes(b), kind(k) {
+        if (s->flags & QOA_FLAG_PROFILE) {
+            cudaEventCreate(&a);
+            cudaEventRecord(a, s->stream);
+        }
+    }
+    ~Timer() {
+        if (a) {
+            cudaEvent_t b;
+            cudaEventCreate(&b);
+            cudaEventRecord(b, s->stream);
+            s->recs.push_back({a, b, bytes, kind});
+        }
+    }
+};
+
+// -------------------------------------------------------------- expansion
+struct Expander {
+    uint32_t n;
+    uint32_t flags;
+    qoa_state_t s;                 // for noise draws (may be null in plan mode)
+    std::vector<Gate> out;
+    int first_err = QOA_OK;
+    std::string err;
+    int cur = -1;
+
+    void skip(int code, const char* what) {
+        if (first_err == QOA_OK) {
+            first_err = code;
+            char b[256];
+            snprintf(b, sizeof b, "op %d skipped: %s", cur, what);
+            err = b;
+        }
+    }
+
+    // QuantumState::apply_noise (quantum_state.rs:839-869) after a gate event:
+    // depolarising draws become explicit X / Y / Z gates.
+    void noise_event(uint64_t touched) {
+        if (!s || s->noise_mode == 0) return;
+        const uint64_t ev = s->noise_event++;
+        double p = s->noise_p;
+        if (s->noise_mode == 2) p = 0.1 + 0.9 * uniform01(s->seed, s->noise_stream, ev, 0);
+        if (s->noise_mode == 1 && !(p > 0.0)) return;
+        for (uint32_t q = 0; q < n; ++q) {
+            if ((flags & QOA_FLAG_NOISE_GATE_QUBITS) && !((touched >> q) & 1)) continue;
+            const double r = uniform01(s->seed, s->noise_stream, ev, 2 * q + 1);
+            if (r < p) {
+                const double u2 = uniform01(s->seed, s->noise_stream, ev, 2 * q + 2);
+                int e = (int)(u2 * 3.0);
+                if (e > 2) e = 2;
+                Gate g;
+                g.src = cur;
+                if (e == 0) g1(g, q, G1_X, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
+                else if (e == 1) g1(g, q, G1_Y, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
+                else diag_neg(g, 1ull << q);
+                out.push_back(g);
+            }
+        }
+    }
+
+    static void g1(Gate& g, uint32_t t, int sub, double2 m0, double2 m1, double2 m2, double2 m3, uint64_t cm) {
+        g.kind = K_G1; g.sub = sub; g.t = (int)t; g.cmask = cm;
+        g.m[0] = m0; g.m[1] = m1; g.m[2] = m2; g.m[3] = m3;
+        g.nmask = 1ull << t; g.dmask = cm;
+    }
+    static void diag_neg(Gate& g, uint64_t mask) {
+        g.kind = K_DIAG; g.t = -1; g.neg = true; g.cmask = mask; g.m[0] = g.m[1] = d2(-1, 0);
+        g.nmask = 0; g.dmask = mask;
+    }
+    static void diag_phase(Gate& g, uint64_t mask, double2 f) {
+        g.kind = K_DIAG; g.t = -1; g.neg = false; g.cmask = mask; g.m[0] = g.m[1] = f;
+        g.nmask = 0; g.dmask = mask;
+    }
+
+    void push(Gate g, uint64_t touched) {
+        g.src = cur;
+        out.push_back(g);
+        noise_event(touched);
+    }
+
+    // ---- QuantumState methods (bounds-checked; out of range -> no-op) ----
+    void h(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "H qubit out of range");
+        Gate g;
+        // apply_h: norm_factor = Complex64::new(1.0 / SQRT_2, 0.0) (quantum_state.rs:196)
+        g1(g, q, G1_H, d2(1.0 / M_SQRT2, 0.0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
+        push(g, 1ull << q);
+    }
+    void x(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "X qubit out of range");
+        Gate g; g1(g, q, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 0); push(g, 1ull << q);
+    }
+    void y(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "Y qubit out of range");
+        Gate g; g1(g, q, G1_Y, d2(0, 0), d2(0, -1), d2(0, 1), d2(0, 0), 0); push(g, 1ull << q);
+    }
+    void z(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "Z qubit out of range");
+        Gate g; diag_neg(g, 1ull << q); push(g, 1ull << q);
+    }
+    void phase(uint32_t q, double2 f) {
+        if (q >= n) return skip(QOA_E_RANGE, "phase qubit out of range");
+        Gate g; diag_phase(g, 1ull << q, f); push(g, 1ull << q);
+    }
+    void rx(uint32_t q, double a) {
+        if (q >= n) return skip(QOA_E_RANGE, "RX qubit out of range");
+        const double c = std::cos(a / 2.0), sn = std::sin(a / 2.0);
+        Gate g; g1(g, q, G1_RX, d2(c, sn), d2(0, -sn), d2(0, -sn), d2(c, 0), 0); push(g, 1ull << q);
+    }
+    void ry(uint32_t q, double a) {
+        if (q >= n) return skip(QOA_E_RANGE, "RY qubit out of range");
+        const double c = std::cos(a / 2.0), sn = std::sin(a / 2.0);
+        Gate g; g1(g, q, G1_RY, d2(c, sn), d2(-sn, 0), d2(sn, 0), d2(c, 0), 0); push(g, 1ull << q);
+    }
+    void rz(uint32_t q, double a) {
+        if (q >= n) return skip(QOA_E_RANGE, "RZ qubit out of range");
+        Gate g;
+        g.kind = K_DIAG; g.t = (int)q; g.cmask = 0;
+        g.m[0] = from_polar(1.0, -a / 2.0);
+        g.m[1] = from_polar(1.0, a / 2.0);
+        g.nmask = 0; g.dmask = 1ull << q;
+        push(g, 1ull << q);
+    }
+    void cnot(uint32_t c, uint32_t t) {
+        if (c >= n || t >= n) return skip(QOA_E_RANGE, "CNOT qubit out of range");
+        if (c == t) return skip(QOA_E_RANGE, "CNOT control == target");
+        Gate g; g1(g, t, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 1ull << c); push(g, (1ull << c) | (1ull << t));
+    }
+    uint64_t cz_mask(uint32_t c, uint32_t t) const {
+        return (flags & QOA_FLAG_COMPAT_MASK_QUIRK) ? ((uint64_t)c | (uint64_t)t) : ((1ull << c) | (1ull << t));
+    }
+    void cz(uint32_t c, uint32_t t) {
+        if (c >= n || t >= n) return skip(QOA_E_RANGE, "CZ qubit out of range");
+        if (c == t) return skip(QOA_E_RANGE, "CZ control == target");
+        Gate g; diag_neg(g, cz_mask(c, t)); push(g, (1ull << c) | (1ull << t));
+    }
+    void cphase(uint32_t c, uint32_t t, double a) {
+        if (c >= n || t >= n) return skip(QOA_E_RANGE, "CPHASE qubit out of range");
+        if (c == t) return skip(QOA_E_RANGE, "CPHASE control == target");
+        Gate g; diag_phase(g, cz_mask(c, t), from_polar(1.0, a)); push(g, (1ull << c) | (1ull << t));
+    }
+    void swap(uint32_t a, uint32_t b, int ctrl) {
+        if (a >= n || b >= n || (ctrl >= 0 && (uint32_t)ctrl >= n)) return skip(QOA_E_RANGE, "SWAP qubit out of range");
+        if (a == b || (ctrl >= 0 && ((uint32_t)ctrl == a || (uint32_t)ctrl == b)))
+            return skip(QOA_E_RANGE, "SWAP qubits not distinct");
+        Gate g;
+        g.kind = K_SWAP; g.t = (int)a; g.t2 = (int)b;
+        g.cmask = ctrl >= 0 ? 1ull << ctrl : 0;
+        g.nmask = (1ull << a) | (1ull << b); g.dmask = g.cmask;
+        push(g, g.nmask | g.cmask);
+    }
+    void toffoli(uint32_t c1, uint32_t c2, uint32_t t) {
+        if (c1 >= n || c2 >= n || t >= n) return skip(QOA_E_RANGE, "TOFFOLI qubit out of range");
+        if (c1 == c2 || c1 == t || c2 == t) return skip(QOA_E_RANGE, "TOFFOLI qubits not distinct");
+        Gate g; g1(g, t, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), (1ull << c1) | (1ull << c2));
+        push(g, (1ull << c1) | (1ull << c2) | (1ull << t));
+    }
+    void cy(uint32_t c, uint32_t t) {
+        if (c >= n || t >= n) return skip(QOA_E_RANGE, "CY qubit out of range");
+        if (c == t) return skip(QOA_E_RANGE, "CY control == target");
+        Gate g; g1(g, t, G1_Y, d2(0, 0), d2(0, -1), d2(0, 1), d2(0, 0), 1ull << c); push(g, (1ull << c) | (1ull << t));
+    }
+    void u1(uint32_t q, const double* m) {
+        if (q >= n) return skip(QOA_E_RANGE, "U1 qubit out of range");
+        if (!m) return skip(QOA_E_ARG, "U1 without matrix");
+        Gate g; g1(g, q, G1_GEN, d2(m[0], m[1]), d2(m[2], m[3]), d2(m[4], m[5]), d2(m[6], m[7]), 0);
+        push(g, 1ull << q);
+    }
+    void u2(uint32_t q1, uint32_t q2, const double* m) {
+        if (q1 >= n || q2 >= n) return skip(QOA_E_RANGE, "U2 qubit out of range");
+        if (q1 == q2) return skip(QOA_E_RANGE, "U2 qubits equal");
+        if (!m) return skip(QOA_E_ARG, "U2 without matrix");
+        Gate g;
+        g.kind = K_U2; g.t = (int)std::min(q1, q2); g.t2 = (int)std::max(q1, q2);
+        for (int k = 0; k < 16; ++k) g.m[k] = d2(m[2 * k], m[2 * k + 1]);
+        g.nmask = (1ull << q1) | (1ull << q2);
+        push(g, g.nmask);
+    }
+    void measure(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "MEASURE qubit out of range");
+        Gate g; g.kind = K_MEASURE; g.t = (int)q; g.nmask = ~0ull;
+        push(g, 1ull << q);
+    }
+    void reset(uint32_t q) {
+        if (q >= n) return skip(QOA_E_RANGE, "RESET qubit out of range");
+        Gate g; g.kind = K_RESET; g.t = (int)q; g.nmask = ~0ull;
+        push(g, 1ull << q);
+    }
+    void reset_all() {
+        Gate g; g.kind = K_RESETALL; g.nmask = ~0ull;
+        push(g, 0);
+    }
+
+    uint32_t qat(const qoa_op& op, uint32_t k) const { return (op.nq > 4 && op.qlist) ? op.qlist[k] : op.q[k]; }
+
+    // execute_arithmetic (quantum_state.rs:460-705)
+    void op(const qoa_op& o) {
+        const uint32_t q0 = o.q[0], q1 = o.q[1], q2 = o.q[2], q3 = o.q[3];
+        const double a = o.angle;
+        switch (o.opcode) {
+            case QOA_OP_QINIT: {
+                Gate g; g.kind = K_QINIT; g.t = (int)std::max<uint32_t>(q0, 1); g.nmask = ~0ull; g.src = cur;
+                out.push_back(g);
+                n = (uint32_t)g.t;
+                break;
+            }
+            case QOA_OP_RESET: reset(q0); break;
+            case QOA_OP_RESETALL: reset_all(); break;
+            case QOA_OP_H: h(q0); break;
+            case QOA_OP_X: x(q0); break;
+            case QOA_OP_Y: y(q0); break;
+            case QOA_OP_Z: z(q0); break;
+            case QOA_OP_T: phase(q0, from_polar(1.0, M_PI / 4.0)); break;   // vectorization.rs:218
+            case QOA_OP_S: phase(q0, from_polar(1.0, M_PI / 2.0)); break;   // vectorization.rs:263
+            case QOA_OP_P: case QOA_OP_SETPHASE: case QOA_OP_PHASE: phase(q0, from_polar(1.0, a)); break;
+            case QOA_OP_RX: rx(q0, a); break;
+            case QOA_OP_RY: ry(q0, a); break;
+            case QOA_OP_RZ: rz(q0, a); break;
+            case QOA_OP_CNOT: case QOA_OP_ENTANGLE: case QOA_OP_ECFB: cnot(q0, q1); break;
+            case QOA_OP_CZ: cz(q0, q1); break;
+            case QOA_OP_CPHASE: cphase(q0, q1, a); break;
+            case QOA_OP_EBELL: h(q0); cnot(q0, q1); break;
+            case QOA_OP_EMULTI: {
+                if (o.nq == 0) { skip(QOA_E_ARG, "empty qubit list for entanglemulti"); break; }
+                const uint32_t first = qat(o, 0);
+                h(first);
+                for (uint32_t k = 1; k < o.nq; ++k) cnot(first, qat(o, k));
+                break;
+            }
+            case QOA_OP_ECLUSTER:
+                for (uint32_t k = 0; k < o.nq; ++k) h(qat(o, k));
+                for (uint32_t k = 0; k + 1 < o.nq; ++k) cz(qat(o, k), qat(o, k + 1));
+                break;
+            case QOA_OP_APPLYGATE:
+                switch (q1) {
+                    case 'H': h(q0); break;
+                    case 'X': x(q0); break;
+                    case 'Y': y(q0); break;
+                    case 'Z': z(q0); break;
+                    case 'T': phase(q0, from_polar(1.0, M_PI / 4.0)); break;
+                    case 'S': phase(q0, from_polar(1.0, M_PI / 2.0)); break;
+                    default: skip(QOA_E_OPCODE, "unknown gate name for applygate");
+                }
+                break;
+            case QOA_OP_ESWAP: cnot(q0, q2); cnot(q1, q3); swap(q2, q3, -1); break;
+            case QOA_OP_ESWAPM: cnot(q0, q2); cnot(q1, q3); swap(q2, q3, -1); measure(q2); measure(q3); break;
+            case QOA_OP_EDIST: break;
+            case QOA_OP_MEASB:
+                if (q0 >= n) { skip(QOA_E_RANGE, "MEASB qubit out of range"); break; }
+                if (q1 == 'X') { h(q0); measure(q0); h(q0); }
+                else if (q1 == 'Y') {
+                    phase(q0, from_polar(1.0, M_PI / 2.0)); h(q0); measure(q0); h(q0);
+                    phase(q0, from_polar(1.0, M_PI / 2.0)); z(q0);
+                } else if (q1 == 'Z') measure(q0);
+                else skip(QOA_E_OPCODE, "unsupported measurement basis");
+                break;
+            case QOA_OP_MEASURE: measure(q0); break;
+            case QOA_OP_ROT:
+                if (q1 == 'X') rx(q0, a);
+                else if (q1 == 'Y') ry(q0, a);
+                else if (q1 == 'Z') rz(q0, a);
+                else skip(QOA_E_OPCODE, "unsupported rotation axis");
+                break;
+            case QOA_OP_SWAP: swap(q0, q1, -1); break;
+            case QOA_OP_CSWAP: swap(q1, q2, (int)q0); break;
+            case QOA_OP_TOFFOLI: toffoli(q0, q1, q2); break;
+            case QOA_OP_U1: u1(q0, o.matrix); break;
+            case QOA_OP_U2: u2(q0, q1, o.matrix); break;
+            case QOA_OP_CY: cy(q0, q1); break;
+            default: skip(QOA_E_OPCODE, "unsupported opcode");
+        }
+    }
+};
+
+// -------------------------------------------------------------- scheduler
+// A step is either a tile pass (a set of K_G1 / K_DIAG gates) or a single
+// gate that runs on its own kernel (SWAP, U2, barriers).
+struct Step {
+    bool pass = false;
+    std::vector<int> gates;        // indices into the gate list, in application order
+    std::vector<int> slots;        // pass: high qubits of the tile (HIGH_SLOTS)
+};
+
+// Greedy list scheduling. Gate g may run in the current pass when every
+// earlier gate still waiting commutes with it: for each shared qubit both act
+// diagonally (controls, phases). Non-diagonal targets must be in the tile:
+// qubits 0..4 always are; up to HIGH_SLOTS higher qubits are claimed in the
+// order gates ask for them.
+std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate) {
+    std::vector<Step> steps;
+    const size_t N = G.size();
+    std::vector<char> done(N, 0);
+    size_t first = 0;
+    const bool tiles = !per_gate && n >= (uint32_t)TILE_BITS;
+    while (true) {
+        while (first < N && done[first]) ++first;
+        if (first >= N) break;
+        const Gate& g0 = G[first];
+        if (!tiles || !is_pass_gate(g0)) {
+            Step st;
+            st.gates.push_back((int)first);
+            done[first] = 1;
+            steps.push_back(st);
+            continue;
+        }
+        Step st;
+        st.pass = true;
+        uint64_t tile = 0x1Full;  // lane qubits
+        int nslots = 0;
+        uint64_t bN = 0, bD = 0;  // qubits blocked by waiting gates (non-diagonal / diagonal action)
+        int budget_ops = MAX_PASS_OPS - 24;  // leave room for exchanges
+        int budget_coef = MAX_PASS_COEF - 8;
+        for (size_t i = first; i < N; ++i) {
+            if (done[i]) continue;
+            const Gate& g = G[i];
+            if (is_barrier(g)) break;
+            bool ok = is_pass_gate(g) && !(g.nmask & (bN | bD)) && !(g.dmask & bN);
+            if (ok) {
+                const uint64_t need = g.nmask & ~tile;
+                const int k = __builtin_popcountll(need);
+                const int nc = g.kind == K_G1 ? 4 : 2;
+                if (nslots + k > HIGH_SLOTS || budget_ops < 1 || budget_coef < nc) ok = false;
+                else {
+                    tile |= need;
+                    nslots += k;
+                    budget_ops -= 1;
+                    budget_coef -= nc;
+                }
+            }
+            if (ok) {
+                st.gates.push_back((int)i);
+                done[i] = 1;
+            } else {
+                bN |= g.nmask;
+                bD |= g.dmask;
+                const uint64_t full = (n >= 64) ? ~0ull : ((1ull << n) - 1);
+                if ((bN & full) == full) break;  // every qubit blocked: nothing else can join
+            }
+        }
+        // the tile's high slots: claimed qubits, padded with unused ones >= 5
+        for (uint32_t q = LANE_BITS; q < n; ++q)
+            if ((tile >> q) & 1) st.slots.push_back((int)q);
+        for (uint32_t q = LANE_BITS; q < n && (int)st.slots.size() < HIGH_SLOTS; ++q)
+            if (!((tile >> q) & 1)) st.slots.push_back((int)q);
+        steps.push_back(st);
+    }
+    return steps;
+}
+
+// Builds the kernel op stream of a pass: picks which slots sit in registers
+// (Belady: keep the slots needed soonest) and translates every gate's qubits
+// into lane / register / warp / outer positions of the mapping in force.
+int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParams& P) {
+    memset(&P, 0, sizeof P);
+    P.n = n;
+    int slot_of[64];
+    for (int q = 0; q < 64; ++q) slot_of[q] = -1;
+    for (int s = 0; s < HIGH_SLOTS; ++s) {
+        P.slot_qubit[s] = (uint8_t)st.slots[s];
+        slot_of[st.slots[s]] = s;
+    }
+    int no = 0;
+    for (uint32_t q = LANE_BITS; q < n; ++q)
+        if (slot_of[q] < 0) P.outer_qubits[no++] = (uint8_t)q;
+
+    // next-use table over the gate sequence (register demand only)
+    const int ng = (int)st.gates.size();
+    std::vector<int> need_slot(ng, -1);
+    for (int i = 0; i < ng; ++i) {
+        const Gate& g = G[st.gates[i]];
+        if (g.kind == K_G1 && g.t >= LANE_BITS) need_slot[i] = slot_of[g.t];
+    }
+    auto next_use = [&](int from, int slot) {
+        for (int i = from; i < ng; ++i)
+            if (need_slot[i] == slot) return i;
+        return 1 << 30;
+    };
+    auto choose_regs = [&](int from, int must, int (&rs)[REG_BITS], const int (&cur)[REG_BITS], bool have_cur) {
+        // candidates ordered by next use; `must` first
+        std::vector<std::pair<int, int>> c;
+        for (int s = 0; s < HIGH_SLOTS; ++s) c.push_back({s == must ? -1 : next_use(from, s), s});
+        std::sort(c.begin(), c.end());
+        int chosen[REG_BITS];
+        for (int k = 0; k < REG_BITS; ++k) chosen[k] = c[k].second;
+        // keep register positions of slots that stay
+        bool used[REG_BITS] = {false, false, false, false};
+        bool placed[REG_BITS] = {false, false, false, false};
+        int res[REG_BITS] = {-1, -1, -1, -1};
+        if (have_cur) {
+            for (int k = 0; k < REG_BITS; ++k)
+                for (int j = 0; j < REG_BITS; ++j)
+                    if (!placed[j] && chosen[j] == cur[k]) { res[k] = chosen[j]; placed[j] = true; used[k] = true; }
+        }
+        for (int j = 0; j < REG_BITS; ++j) {
+            if (placed[j]) continue;
+            for (int k = 0; k < REG_BITS; ++k)
+                if (!used[k]) { res[k] = chosen[j]; used[k] = true; break; }
+        }
+        for (int k = 0; k < REG_BITS; ++k) rs[k] = res[k];
+    };
+    auto warps_from = [&](const int (&rs)[REG_BITS], int (&ws)[WARP_BITS], const int (&curw)[WARP_BITS], bool have) {
+        bool inreg[HIGH_SLOTS] = {};
+        for (int k = 0; k < REG_BITS; ++k) inreg[rs[k]] = true;
+        std::vector<int> rest;
+        for (int s = 0; s < HIGH_SLOTS; ++s)
+            if (!inreg[s]) rest.push_back(s);
+        // keep warp positions of slots that stay in warps
+        int res[WARP_BITS] = {-1, -1, -1};
+        std::vector<char> taken(HIGH_SLOTS, 0);
+        if (have)
+            for (int k = 0; k < WARP_BITS; ++k)
+                if (!inreg[curw[k]]) { res[k] = curw[k]; taken[curw[k]] = 1; }
+        size_t ri = 0;
+        for (int k = 0; k < WARP_BITS; ++k) {
+            if (res[k] >= 0) continue;
+            while (ri < rest.size() && taken[rest[ri]]) ++ri;
+            res[k] = rest[ri];
+            taken[rest[ri]] = 1;
+        }
+        for (int k = 0; k < WARP_BITS; ++k) ws[k] = res[k];
+    };
+
+    int rs[REG_BITS], ws[WARP_BITS];
+    {
+        int dummy_r[REG_BITS] = {0, 0, 0, 0};
+        int dummy_w[WARP_BITS] = {0, 0, 0};
+        choose_regs(0, -1, rs, dummy_r, false);
+        warps_from(rs, ws, dummy_w, false);
+    }
+    for (int k = 0; k < REG_BITS; ++k) P.reg_slot0[k] = (uint8_t)rs[k];
+    for (int k = 0; k < WARP_BITS; ++k) P.warp_slot0[k] = (uint8_t)ws[k];
+
+    int nops = 0, ncoef = 0;
+    auto where = [&](int q, int& loc, int& idx) {
+        if (q < LANE_BITS) { loc = SEL_LANE; idx = q; return; }
+        const int s = slot_of[q];
+        if (s < 0) { loc = SEL_OUTER; idx = q; return; }
+        for (int k = 0; k < REG_BITS; ++k)
+            if (rs[k] == s) { loc = SEL_REG; idx = k; return; }
+        for (int k = 0; k < WARP_BITS; ++k)
+            if (ws[k] == s) { loc = SEL_WARP; idx = k; return; }
+        loc = -1; idx = -1;
+    };
+    auto cond = [&](uint64_t mask, PassOp& op) {
+        for (int q = 0; q < 64; ++q) {
+            if (!((mask >> q) & 1)) continue;
+            int loc, idx;
+            where(q, loc, idx);
+            if (loc == SEL_LANE) op.cond_lane |= (uint8_t)(1u << idx);
+            else if (loc == SEL_REG) op.cond_reg |= (uint8_t)(1u << idx);
+            else if (loc == SEL_WARP) op.cond_warp |= (uint8_t)(1u << idx);
+            else op.cond_outer |= 1ull << q;
+        }
+    };
+    for (int i = 0; i < ng; ++i) {
+        const Gate& g = G[st.gates[i]];
+        if (nops >= MAX_PASS_OPS - 1) return -1;
+        if (g.kind == K_G1 && g.t >= LANE_BITS) {
+            const int s = slot_of[g.t];
+            bool inreg = false;
+            for (int k = 0; k < REG_BITS; ++k) inreg |= rs[k] == s;
+            if (!inreg) {
+                int nrs[REG_BITS], nws[WARP_BITS];
+                choose_regs(i, s, nrs, rs, true);
+                warps_from(nrs, nws, ws, true);
+                PassOp& x = P.ops[nops++];
+                memset(&x, 0, sizeof x);
+                x.kind = PK_XCHG;
+                for (int k = 0; k < REG_BITS; ++k) { x.xreg[k] = (uint8_t)nrs[k]; rs[k] = nrs[k]; }
+                for (int k = 0; k < WARP_BITS; ++k) { x.xwarp[k] = (uint8_t)nws[k]; ws[k] = nws[k]; }
+            }
+        }
+        if (nops >= MAX_PASS_OPS) return -1;
+        PassOp& op = P.ops[nops++];
+        memset(&op, 0, sizeof op);
+        op.coef = (uint16_t)ncoef;
+        if (g.kind == K_G1) {
+            int loc, idx;
+            where(g.t, loc, idx);
+            op.kind = (loc == SEL_LANE) ? PK_G1_LANE : PK_G1_REG;
+            op.sub = (uint8_t)g.sub;
+            op.t0 = (uint8_t)idx;
+            cond(g.cmask, op);
+            for (int k = 0; k < 4; ++k) P.coef[ncoef++] = g.m[k];
+        } else {  // K_DIAG
+            op.kind = PK_DIAG;
+            int loc = SEL_NONE, idx = 0;
+            if (g.t >= 0) where(g.t, loc, idx);
+            op.sub = (uint8_t)(loc | (g.neg ? 0x80 : 0));
+            op.t0 = (uint8_t)idx;
+            cond(g.cmask, op);
+            op.reg_free = (uint8_t)((loc != SEL_REG && op.cond_reg == 0) ? 1 : 0);
+            P.coef[ncoef++] = g.m[0];
+            P.coef[ncoef++] = g.m[1];
+        }
+        if (ncoef > MAX_PASS_COEF) return -1;
+    }
+    P.nops = (uint32_t)nops;
+    P.ncoef = (uint32_t)ncoef;
+    return 0;
+}
+
+// ------------------------------------------------------------- execution
+GGate to_ggate(const Gate& g) {
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.cmask = g.cmask;
+    if (g.kind == K_G1) {
+        k.kind = GG_G1; k.sub = (uint8_t)g.sub; k.t = (uint8_t)g.t;
+        for (int j = 0; j < 4; ++j) k.m[j] = g.m[j];
+    } else if (g.kind == K_DIAG) {
+        k.kind = GG_DIAG; k.sub = g.neg ? 0x80 : 0; k.t = g.t >= 0 ? (uint8_t)g.t : 64;
+        k.m[0] = g.m[0]; k.m[1] = g.m[1];
+    } else if (g.kind == K_SWAP) {
+        k.kind = GG_SWAP; k.t = (uint8_t)g.t; k.t2 = (uint8_t)g.t2;
+    } else if (g.kind == K_U2) {
+        k.kind = GG_U2; k.t = (uint8_t)g.t; k.t2 = (uint8_t)g.t2;
+        for (int j = 0; j < 16; ++j) k.m[j] = g.m[j];
+    }
+    return k;
+}
+
+int run_gate(qoa_state_t s, const Gate& g) {
+    const GGate k = to_ggate(g);
+    Timer tm(s, gate_bytes(g, s->n), 1);
+    CK(launch_gate(s->amps, state_len(s), k, s->stream));
+    s->launches++;
+    return QOA_OK;
+}
+
+int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
+    static thread_local PassParams P;
+    if (build_pass(G, st, s->n, P) != 0) {
+        // op stream too long for one launch: fall back to per-gate kernels
+        for (int gi : st.gates) {
+            int rc = run_gate(s, G[gi]);
+            if (rc) return rc;
+        }
+        return QOA_OK;
+    }
+    {
+        Timer tm(s, 2.0 * std::ldexp(16.0, (int)s->n), 0);
+        CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
+    }
+    CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
+    s->launches += 2;
+    return QOA_OK;
+}
+
+// Reads norm2, P0, P1 of qubit q (logical probabilities) to the host.
+int read_p01(qoa_state_t s, uint32_t q, double& p0, double& p1, double& norm2) {
+    CK(launch_p01(s->amps, state_len(s), q, s->partials, s->scal + 1, s->scal, s->stream));
+    s->launches += 2;
+    CK(cudaMemcpyAsync(s->host_scal, s->scal, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    norm2 = s->host_scal[0];
+    if (!(norm2 > 1e-12)) {  // logical state is |0..0>
+        p0 = 1.0; p1 = 0.0;
+    } else {
+        p0 = s->host_scal[1]; p1 = s->host_scal[2];
+    }
+    return QOA_OK;
+}
+
+int do_reset_all(qoa_state_t s) {
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_RESET_ALL;
+    CK(launch_gate(s->amps, state_len(s), k, s->stream));
+    CK(launch_set_scalar(s->scal, 1.0, s->stream));
+    s->launches += 2;
+    return QOA_OK;
+}
+
+// measure (quantum_state.rs:399-458) with uniform u
+int do_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome) {
+    double p0, p1, norm2;
+    int rc = read_p01(s, q, p0, p1, norm2);
+    if (rc) return rc;
+    const uint32_t res = (u < p0) ? 0u : 1u;
+    const double p = res ? p1 : p0;
+    if (outcome) *outcome = res;
+    if (!(p > 1e-12)) {
+        // normalization_factor 0 zeroes the state; normalize() then resets it
+        // to |0..0> (quantum_state.rs:431-443, 895-906)
+        s->host_resets++;
+        return do_reset_all(s);
+    }
+    const double f = 1.0 / std::sqrt(p);
+    if (!(norm2 > 1e-12)) {
+        rc = do_reset_all(s);
+        if (rc) return rc;
+        norm2 = 1.0;
+    }
+    CK(launch_collapse(s->amps, state_len(s), q, res, f / std::sqrt(norm2), s->partials, s->scal, s->status,
+                       s->stream));
+    s->launches += 2;
+    return QOA_OK;
+}
+
+// apply_reset_simd (vectorization.rs:1020-1056)
+int do_reset_qubit(qoa_state_t s, uint32_t q) {
+    double p0, p1, norm2;
+    int rc = read_p01(s, q, p0, p1, norm2);
+    if (rc) return rc;
+    if (!(norm2 > 1e-12)) return do_reset_all(s);
+    if (p0 > 1e-12) {
+        CK(launch_collapse(s->amps, state_len(s), q, 0, (1.0 / std::sqrt(p0)) / std::sqrt(norm2), s->partials,
+                           s->scal, s->status, s->stream));
+        s->launches += 2;
+        return QOA_OK;
+    }
+    return do_reset_all(s);
+}
+
+double next_meas_uniform(qoa_state_t s) {
+    return uniform01(s->seed, s->noise_stream ^ kMeasStreamXor, s->meas_draws++, 0);
+}
+
+int execute(qoa_state_t s, std::vector<Gate>& G) {
+    const bool per_gate = (s->flags & QOA_FLAG_PER_GATE) != 0;
+    // Split at QINIT (changes n) and run each segment through the scheduler.
+    size_t i = 0;
+    while (i < G.size()) {
+        size_t j = i;
+        while (j < G.size() && G[j].kind != K_QINIT) ++j;
+        std::vector<Gate> seg(G.begin() + i, G.begin() + j);
+        std::vector<Step> steps = schedule(seg, s->n, per_gate);
+        for (const Step& st : steps) {
+            int rc;
+            if (st.pass) rc = run_pass(s, seg, st);
+            else {
+                const Gate& g = seg[st.gates[0]];
+                switch (g.kind) {
+                    case K_MEASURE: {
+                        const double u = g.u >= 0 ? g.u : next_meas_uniform(s);
+                        rc = do_measure(s, (uint32_t)g.t, u, nullptr);
+                        break;
+                    }
+                    case K_RESET: rc = do_reset_qubit(s, (uint32_t)g.t); break;
+                    case K_RESETALL: rc = do_reset_all(s); break;
+                    default: rc = run_gate(s, g);
+                }
+            }
+            if (rc) return rc;
+        }
+        if (j < G.size()) {  // QINIT
+            const uint32_t nn = (uint32_t)G[j].t;
+            if (nn != s->n) {
+                CK(cudaStreamSynchronize(s->stream));
+                int rc = alloc_state(s, nn);
+                if (rc) return rc;
+            }
+            int rc = do_reset_all(s);
+            if (rc) return rc;
+            ++j;
+        }
+        i = j;
+    }
+    return QOA_OK;
+}
+
+int check_handle(qoa_state_t s) {
+    if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
+    if (cudaSetDevice(s->device) != cudaSuccess) return set_err(s, QOA_E_CUDA, "cudaSetDevice failed");
+    return QOA_OK;
+}
+
+// -------------------------------------------------------------- shims
+std::mutex g_shim_mu;
+double2* g_shim_buf = nullptr;
+size_t g_shim_cap = 0;
+double* g_shim_scr = nullptr;
+cudaStream_t g_shim_stream = nullptr;
+int g_shim_dev = -1;
+
+int shim_begin(double* amps, size_t len, double2** dev) {
+    qoa_state_t s = nullptr;
+    if (!amps && len) return set_err(nullptr, QOA_E_ARG, "null amps");
+    int dev_id = 0;
+    CK(cudaGetDevice(&dev_id));
+    if (g_shim_dev != dev_id) {
+        g_shim_buf = nullptr; g_shim_cap = 0; g_shim_scr = nullptr; g_shim_stream = nullptr;
+        g_shim_dev = dev_id;
+    }
+    if (!g_shim_stream) CK(cudaStreamCreateWithFlags(&g_shim_stream, cudaStreamNonBlocking));
+    if (len > g_shim_cap) {
+        if (g_shim_buf) cudaFree(g_shim_buf);
+        if (g_shim_scr) cudaFree(g_shim_scr);
+        g_shim_buf = nullptr; g_shim_scr = nullptr; g_shim_cap = 0;
+        CK(cudaMalloc(&g_shim_buf, len * sizeof(double2)));
+        CK(cudaMalloc(&g_shim_scr, (size_t)(2 * reduce_blocks(len) + 8) * sizeof(double)));
+        g_shim_cap = len;
+    }
+    if (len) CK(cudaMemcpyAsync(g_shim_buf, amps, len * sizeof(double2), cudaMemcpyHostToDevice, g_shim_stream));
+    *dev = g_shim_buf;
+    return QOA_OK;
+}
+int shim_end(double* amps, size_t len) {
+    qoa_state_t s = nullptr;
+    if (len) CK(cudaMemcpyAsync(amps, g_shim_buf, len * sizeof(double2), cudaMemcpyDeviceToHost, g_shim_stream));
+    CK(cudaStreamSynchronize(g_shim_stream));
+    return QOA_OK;
+}
+int shim_gate(double* amps, size_t len, const GGate& k) {
+    std::lock_guard<std::mutex> lk(g_shim_mu);
+    qoa_state_t s = nullptr;
+    double2* dev;
+    int rc = shim_begin(amps, len, &dev);
+    if (rc) return rc;
+    if (len) CK(launch_gate(dev, len, k, g_shim_stream));
+    return shim_end(amps, len);
+}
+GGate shim_g1(size_t t, int sub, double2 m0, double2 m1, double2 m2, double2 m3, uint64_t cm) {
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_G1; k.sub = (uint8_t)sub; k.t = (uint8_t)t; k.cmask = cm;
+    k.m[0] = m0; k.m[1] = m1; k.m[2] = m2; k.m[3] = m3;
+    return k;
+}
+GGate shim_diag(int sel, double2 d0, double2 d1, uint64_t cm, bool neg) {
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_DIAG; k.sub = neg ? 0x80 : 0; k.t = sel >= 0 ? (uint8_t)sel : 64; k.cmask = cm;
+    k.m[0] = d0; k.m[1] = d1;
+    return k;
+}
+// A bit index >= 64 makes every reference loop a no-op (no index has it).
+inline bool shim_bit_ok(size_t b) { return b < 64; }
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+const char* qoa_strerror(int code) {
+    switch (code) {
+        case QOA_OK: return "ok";
+        case QOA_E_RANGE: return "qubit index out of range (op skipped)";
+        case QOA_E_ARG: return "invalid argument";
+        case QOA_E_OPCODE: return "unsupported opcode";
+        case QOA_E_CUDA: return "CUDA error";
+        case QOA_E_OOM: return "device out of memory";
+        case QOA_E_STATE: return "numerical status";
+        case QOA_E_NOGPU: return "no CUDA device";
+        default: return "unknown";
+    }
+}
+
+const char* qoa_last_error(qoa_state_t s) {
+    if (s) return s->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_err.c_str();
+}
+
+int qoa_create(uint32_t n, int precision, uint32_t flags, qoa_state_t* out) {
+    qoa_state_t s = nullptr;
+    if (!out) return set_err(nullptr, QOA_E_ARG, "null out");
+    *out = nullptr;
+    if (precision != QOA_PREC_F64) return set_err(nullptr, QOA_E_ARG, "unsupported precision %d", precision);
+    if (n < 1) n = 1;
+    if (n > 40) return set_err(nullptr, QOA_E_ARG, "n=%u qubits exceeds the engine limit", n);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(nullptr, QOA_E_NOGPU, "no CUDA device");
+    s = new qoa_state_s();
+    s->flags = flags;
+    cudaGetDevice(&s->device);
+    auto fail = [&](int rc) {
+        std::string m = s->err;
+        qoa_destroy(s);
+        set_err(nullptr, rc, "%s", m.c_str());
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_err(s, QOA_E_CUDA, "stream create failed"));
+    if (cudaMalloc(&s->scal, 16 * sizeof(double)) != cudaSuccess) return fail(set_err(s, QOA_E_OOM, "scalar alloc"));
+    if (cudaMalloc(&s->status, 4 * sizeof(uint32_t)) != cudaSuccess) return fail(set_err(s, QOA_E_OOM, "status alloc"));
+    if (cudaMemsetAsync(s->status, 0, 4 * sizeof(uint32_t), s->stream) != cudaSuccess)
+        return fail(set_err(s, QOA_E_CUDA, "status memset"));
+    if (cudaMallocHost(&s->host_scal, 16 * sizeof(double)) != cudaSuccess) return fail(set_err(s, QOA_E_OOM, "pinned alloc"));
+    int rc = alloc_state(s, n);
+    if (rc) return fail(rc);
+    rc = do_reset_all(s);
+    if (rc) return fail(rc);
+    *out = s;
+    return QOA_OK;
+}
+
+int qoa_destroy(qoa_state_t s) {
+    if (!s) return QOA_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& r : s->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    if (s->amps) cudaFree(s->amps);
+    if (s->partials) cudaFree(s->partials);
+    if (s->scal) cudaFree(s->scal);
+    if (s->status) cudaFree(s->status);
+    if (s->host_scal) cudaFreeHost(s->host_scal);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return QOA_OK;
+}
+
+int qoa_num_qubits(qoa_state_t s, uint32_t* n) {
+    if (!s || !n) return set_err(s, QOA_E_ARG, "null argument");
+    *n = s->n;
+    return QOA_OK;
+}
+
+int qoa_reset_all(qoa_state_t s) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    return do_reset_all(s);
+}
+
+int qoa_apply(qoa_state_t s, const qoa_op* ops, size_t nops) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!ops && nops) return set_err(s, QOA_E_ARG, "null ops");
+    Expander ex;
+    ex.n = s->n;
+    ex.flags = s->flags;
+    ex.s = s;
+    ex.out.reserve(nops * 2 + 8);
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    rc = execute(s, ex.out);
+    if (rc) return rc;
+    if (ex.first_err != QOA_OK) return set_err(s, ex.first_err, "%s", ex.err.c_str());
+    return QOA_OK;
+}
+
+int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (q >= s->n) return set_err(s, QOA_E_RANGE, "qubit index %u out of bounds", q);
+    if (u < 0) u = next_meas_uniform(s);
+    rc = do_measure(s, q, u, outcome);
+    if (rc) return rc;
+    // apply_noise after the measurement (quantum_state.rs:455)
+    Expander ex;
+    ex.n = s->n; ex.flags = s->flags; ex.s = s; ex.cur = -1;
+    ex.noise_event(1ull << q);
+    return execute(s, ex.out);
+}
+
+int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t* out) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!u || !out || (mode != 0 && mode != 1)) return set_err(s, QOA_E_ARG, "bad sample arguments");
+    if (shots == 0) return QOA_OK;
+    const uint32_t n = s->n;
+    const size_t nu = mode == 0 ? shots * n : shots;
+    double* d_tree = nullptr;
+    double* d_u = nullptr;
+    unsigned long long* d_out = nullptr;
+    const size_t tree_len = (n >= 2) ? ((1ull << n) - 2) : 1;
+    CK(cudaMallocAsync(&d_tree, tree_len * sizeof(double), s->stream));
+    CK(cudaMallocAsync(&d_u, nu * sizeof(double), s->stream));
+    CK(cudaMallocAsync(&d_out, shots * sizeof(unsigned long long), s->stream));
+    CK(cudaMemcpyAsync(d_u, u, nu * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(launch_tree(s->amps, n, s->scal, d_tree, s->stream));
+    CK(launch_sample(s->amps, n, s->scal, d_tree, d_u, shots, mode, d_out, s->stream));
+    s->launches += (n >= 2 ? (n - 1) : 0) + 1;
+    CK(cudaMemcpyAsync(out, d_out, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaFreeAsync(d_tree, s->stream));
+    CK(cudaFreeAsync(d_u, s->stream));
+    CK(cudaFreeAsync(d_out, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
+int qoa_probabilities(qoa_state_t s, double* out) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!out) return set_err(s, QOA_E_ARG, "null out");
+    const uint64_t len = state_len(s);
+    const uint64_t chunk = std::min<uint64_t>(len, 1ull << 24);
+    double* d = nullptr;
+    CK(cudaMallocAsync(&d, chunk * sizeof(double), s->stream));
+    for (uint64_t off = 0; off < len; off += chunk) {
+        const uint64_t cnt = std::min(chunk, len - off);
+        CK(launch_probs(s->amps, off, cnt, s->scal, d, s->stream));
+        s->launches++;
+        CK(cudaMemcpyAsync(out + off, d, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    }
+    CK(cudaFreeAsync(d, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
+int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if ((!masks || !out) && k) return set_err(s, QOA_E_ARG, "null argument");
+    for (size_t i = 0; i < k; i += 8) {
+        const uint32_t kk = (uint32_t)std::min<size_t>(8, k - i);
+        CK(launch_expz(s->amps, state_len(s), masks + i, kk, s->partials, s->scal + 8, s->scal, s->stream));
+        s->launches += 2;
+        CK(cudaMemcpyAsync(s->host_scal + 8, s->scal + 8, kk * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        for (uint32_t j = 0; j < kk; ++j) out[i + j] = s->host_scal[8 + j];
+    }
+    return QOA_OK;
+}
+
+int qoa_get_state(qoa_state_t s, void* host, size_t bytes) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!host || bytes != state_len(s) * sizeof(double2))
+        return set_err(s, QOA_E_ARG, "get_state needs %llu bytes", (unsigned long long)(state_len(s) * sizeof(double2)));
+    CK(launch_materialize(s->amps, state_len(s), s->scal, s->partials, s->status, s->stream));
+    s->launches += 2;
+    CK(cudaMemcpyAsync(host, s->amps, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
+int qoa_set_state(qoa_state_t s, const void* host, size_t bytes) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!host || bytes != state_len(s) * sizeof(double2))
+        return set_err(s, QOA_E_ARG, "set_state needs %llu bytes", (unsigned long long)(state_len(s) * sizeof(double2)));
+    CK(cudaMemcpyAsync(s->amps, host, bytes, cudaMemcpyHostToDevice, s->stream));
+    CK(launch_norm(s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
+    s->launches += 2;
+    // set_state_vector normalises at once (quantum_state.rs:1143): a zero or
+    // NaN vector becomes |0..0> before any gate sees it.
+    CK(cudaMemcpyAsync(s->host_scal, s->scal, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (!(s->host_scal[0] > 1e-12)) {
+        s->host_resets++;
+        return do_reset_all(s);
+    }
+    return QOA_OK;
+}
+
+int qoa_seed(qoa_state_t s, uint64_t seed) {
+    if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
+    s->seed = seed;
+    s->noise_event = 0;
+    s->meas_draws = 0;
+    return QOA_OK;
+}
+
+int qoa_set_noise(qoa_state_t s, int mode, double p) {
+    if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
+    if (mode < 0 || mode > 2 || (mode == 1 && !(p >= 0.0 && p <= 1.0))) return set_err(s, QOA_E_ARG, "bad noise config");
+    s->noise_mode = mode;
+    s->noise_p = p;
+    return QOA_OK;
+}
+
+int qoa_set_trajectory(qoa_state_t s, uint64_t stream) {
+    if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
+    s->noise_stream = stream;
+    s->noise_event = 0;
+    return QOA_OK;
+}
+
+int qoa_status(qoa_state_t s, qoa_status_t* out) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!out) return set_err(s, QOA_E_ARG, "null out");
+    uint32_t h[4];
+    CK(cudaMemcpyAsync(h, s->status, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    out->nan_seen = h[0];
+    out->inf_seen = h[1];
+    out->zero_norm_resets = h[2] + s->host_resets;
+    out->reserved = 0;
+    return QOA_OK;
+}
+
+int qoa_sync(qoa_state_t s) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
+int qoa_stream(qoa_state_t s, void** stream) {
+    if (!s || !stream) return set_err(s, QOA_E_ARG, "null argument");
+    *stream = (void*)s->stream;
+    return QOA_OK;
+}
+
+int qoa_launch_count(qoa_state_t s, uint64_t* count) {
+    if (!s || !count) return set_err(s, QOA_E_ARG, "null argument");
+    *count = s->launches;
+    return QOA_OK;
+}
+
+int qoa_launch_times(qoa_state_t s, double* ms, double* bytes, int* kind, size_t cap, size_t* n) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!n) return set_err(s, QOA_E_ARG, "null n");
+    CK(cudaStreamSynchronize(s->stream));
+    size_t k = 0;
+    for (auto& r : s->recs) {
+        if (k < cap) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, r.a, r.b);
+            if (ms) ms[k] = t;
+            if (bytes) bytes[k] = r.bytes;
+            if (kind) kind[k] = r.kind;
+            ++k;
+        }
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    s->recs.clear();
+    *n = k;
+    return QOA_OK;
+}
+
+int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t cap, int32_t* pass_of,
+             int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits, double* gate_matrix, size_t* ngates,
+             size_t* npasses) {
+    qoa_state_t s = nullptr;
+    if ((!ops && nops) || !ngates || !npasses) return set_err(nullptr, QOA_E_ARG, "null argument");
+    Expander ex;
+    ex.n = std::max<uint32_t>(n, 1);
+    ex.flags = flags;
+    ex.s = nullptr;
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    const std::vector<Gate>& G = ex.out;
+    for (const Gate& g : G)
+        if (g.kind == K_QINIT) return set_err(nullptr, QOA_E_ARG, "qoa_plan does not take QINIT");
+    std::vector<Step> steps = schedule(G, ex.n, (flags & QOA_FLAG_PER_GATE) != 0);
+    *ngates = G.size();
+    *npasses = steps.size();
+    if (G.size() > cap) return set_err(nullptr, QOA_E_ARG, "cap too small: %zu gates", G.size());
+    for (size_t si = 0; si < steps.size(); ++si) {
+        for (size_t k = 0; k < steps[si].gates.size(); ++k) {
+            const int gi = steps[si].gates[k];
+            if (pass_of) pass_of[gi] = (int32_t)si;
+            if (order) order[gi] = (int32_t)k;
+        }
+        if (steps[si].pass) {  // make sure the kernel op stream builds
+            static thread_local PassParams P;
+            if (build_pass(G, steps[si], ex.n, P) != 0)
+                return set_err(nullptr, QOA_E_ARG, "pass %zu does not fit one launch", si);
+        }
+    }
+    for (size_t gi = 0; gi < G.size(); ++gi) {
+        const Gate& g = G[gi];
+        if (gate_kind) gate_kind[gi] = g.kind * 16 + (g.kind == K_G1 ? g.sub : (g.neg ? 1 : 0));
+        if (gate_qubits) {
+            gate_qubits[4 * gi + 0] = (uint32_t)g.t;
+            gate_qubits[4 * gi + 1] = (uint32_t)g.t2;
+            gate_qubits[4 * gi + 2] = (uint32_t)g.cmask;
+            gate_qubits[4 * gi + 3] = (uint32_t)(g.cmask >> 32);
+        }
+        if (gate_matrix)
+            for (int k = 0; k < 16; ++k) {
+                gate_matrix[32 * gi + 2 * k] = g.m[k].x;
+                gate_matrix[32 * gi + 2 * k + 1] = g.m[k].y;
+            }
+    }
+    return QOA_OK;
+}
+
+// ---- vectorization.rs shims ------------------------------------------------
+int qoa_vec_apply_hadamard(double* amps, size_t len, double nre, double nim, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    // norm_factor * (a +/- b); a real factor takes the exact (a+b)*f form
+    const double2 f = d2(nre, nim);
+    if (nim == 0.0) return shim_gate(amps, len, shim_g1(bit, G1_H, f, d2(0, 0), d2(0, 0), d2(0, 0), 0));
+    return shim_gate(amps, len, shim_g1(bit, G1_GEN, f, f, f, d2(-f.x, -f.y), 0));
+}
+int qoa_vec_apply_x(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    return shim_gate(amps, len, shim_g1(bit, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 0));
+}
+int qoa_vec_apply_y(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    return shim_gate(amps, len, shim_g1(bit, G1_Y, d2(0, 0), d2(0, -1), d2(0, 1), d2(0, 0), 0));
+}
+int qoa_vec_apply_z(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    return shim_gate(amps, len, shim_diag(-1, d2(-1, 0), d2(-1, 0), 1ull << bit, true));
+}
+int qoa_vec_apply_t(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    const double2 f = from_polar(1.0, M_PI / 4.0);
+    return shim_gate(amps, len, shim_diag(-1, f, f, 1ull << bit, false));
+}
+int qoa_vec_apply_s(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    const double2 f = from_polar(1.0, M_PI / 2.0);
+    return shim_gate(amps, len, shim_diag(-1, f, f, 1ull << bit, false));
+}
+int qoa_vec_apply_phaseshift(double* amps, size_t len, size_t bit, double angle) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    const double2 f = from_polar(1.0, angle);
+    return shim_gate(amps, len, shim_diag(-1, f, f, 1ull << bit, false));
+}
+int qoa_vec_apply_reset(double* amps, size_t len, size_t bit) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    std::lock_guard<std::mutex> lk(g_shim_mu);
+    qoa_state_t s = nullptr;
+    double2* dev;
+    int rc = shim_begin(amps, len, &dev);
+    if (rc) return rc;
+    if (len) {
+        CK(launch_p01(dev, len, (uint32_t)bit, g_shim_scr + 8, g_shim_scr, nullptr, g_shim_stream));
+        double p[2];
+        CK(cudaMemcpyAsync(p, g_shim_scr, sizeof p, cudaMemcpyDeviceToHost, g_shim_stream));
+        CK(cudaStreamSynchronize(g_shim_stream));
+        if (p[0] > 1e-12) {
+            CK(launch_collapse(dev, len, (uint32_t)bit, 0, 1.0 / std::sqrt(p[0]), g_shim_scr + 8, g_shim_scr + 2,
+                               nullptr, g_shim_stream));
+        } else {
+            GGate k;
+            memset(&k, 0, sizeof k);
+            k.kind = GG_RESET_ALL;
+            CK(launch_gate(dev, len, k, g_shim_stream));
+        }
+    }
+    return shim_end(amps, len);
+}
+int qoa_vec_apply_swap(double* amps, size_t len, size_t q1, size_t q2) {
+    if (!shim_bit_ok(q1) || !shim_bit_ok(q2)) return QOA_OK;
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_SWAP; k.t = (uint8_t)q1; k.t2 = (uint8_t)q2;
+    return shim_gate(amps, len, k);
+}
+int qoa_vec_apply_controlled_swap(double* amps, size_t len, size_t c, size_t t1, size_t t2) {
+    if (!shim_bit_ok(c) || !shim_bit_ok(t1) || !shim_bit_ok(t2)) return QOA_OK;
+    // apply_controlled_swap_simd (vectorization.rs:1200-1232): for base i with
+    // control, t1, t2 all 0, swap i|c|t2 <-> i|c|t1. With coinciding indices
+    // that degenerates to a controlled X (or to nothing), reproduced here.
+    if (t1 == t2) return QOA_OK;
+    if (c == t1) return shim_gate(amps, len, shim_g1(t2, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 1ull << c));
+    if (c == t2) return shim_gate(amps, len, shim_g1(t1, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 1ull << c));
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_SWAP; k.t = (uint8_t)t1; k.t2 = (uint8_t)t2; k.cmask = 1ull << c;
+    return shim_gate(amps, len, k);
+}
+int qoa_vec_apply_rx(double* amps, size_t len, size_t bit, double angle) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    const double c = std::cos(angle / 2.0), sn = std::sin(angle / 2.0);
+    return shim_gate(amps, len, shim_g1(bit, G1_RX, d2(c, sn), d2(0, -sn), d2(0, -sn), d2(c, 0), 0));
+}
+int qoa_vec_apply_ry(double* amps, size_t len, size_t bit, double angle) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    const double c = std::cos(angle / 2.0), sn = std::sin(angle / 2.0);
+    return shim_gate(amps, len, shim_g1(bit, G1_RY, d2(c, sn), d2(-sn, 0), d2(sn, 0), d2(c, 0), 0));
+}
+int qoa_vec_apply_rz(double* amps, size_t len, size_t bit, double angle) {
+    if (!shim_bit_ok(bit)) return QOA_OK;
+    return shim_gate(amps, len, shim_diag((int)bit, from_polar(1.0, -angle / 2.0), from_polar(1.0, angle / 2.0), 0, false));
+}
+int qoa_vec_apply_cnot(double* amps, size_t len, size_t control, size_t target) {
+    if (!shim_bit_ok(control) || !shim_bit_ok(target)) return QOA_OK;
+    if (control == target) return QOA_OK;  // (i & cm) == cm && (i & tm) == 0 never holds
+    return shim_gate(amps, len, shim_g1(target, G1_X, d2(0, 0), d2(1, 0), d2(1, 0), d2(0, 0), 1ull << control));
+}
+int qoa_vec_apply_cz(double* amps, size_t len, size_t control_mask, size_t target_mask) {
+    return shim_gate(amps, len, shim_diag(-1, d2(-1, 0), d2(-1, 0), (uint64_t)(control_mask | target_mask), true));
+}
+int qoa_vec_apply_controlled_phase_rotation(double* amps, size_t len, size_t control_mask, size_t target_mask,
+                                            double angle) {
+    const double2 f = from_polar(1.0, angle);
+    return shim_gate(amps, len, shim_diag(-1, f, f, (uint64_t)(control_mask | target_mask), false));
+}
+int qoa_vec_apply_reset_all(double* amps, size_t len) {
+    GGate k;
+    memset(&k, 0, sizeof k);
+    k.kind = GG_RESET_ALL;
+    return shim_gate(amps, len, k);
+}
+
+}  // extern "C"

@@ -1,0 +1,726 @@
+// qoa_kernels.cu — sm_100a kernels of the state-vector engine.
+//
+// Hot path: k_pass, one HBM read + write of the whole state for a run of gates
+// whose non-diagonal targets fall inside a 12-qubit tile (5 lane qubits that
+// keep every warp access 512 contiguous bytes, 4 register qubits, 3 warp
+// qubits). It replaces the per-gate sweeps of src/vectorization.rs:915-1260
+// plus the two normalize() sweeps that follow every gate
+// (src/runtime/quantum_state.rs:839-907): the pass scales its input by the
+// pending 1/||psi|| and leaves per-CTA partial sums of |a|^2 for the next one.
+//
+// The rest: per-gate kernels over global memory (fallback, per-gate mode and
+// the vectorization.rs shims), the measurement reductions and collapse of
+// quantum_state.rs:399-458, the marginal tree behind measure_all-order
+// sampling (quantum_state.rs:909-918), and expectation values.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "qoa_kernels.cuh"
+
+namespace qoa {
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 c_neg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double c_abs2(double2 a) { return fma(a.x, a.x, a.y * a.y); }
+
+// 2x2 on the amplitude pair (a0 = bit 0, a1 = bit 1).
+template <int SUB>
+__device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 m0, const double2 m1,
+                                        const double2 m2, const double2 m3) {
+    if (SUB == G1_H) {
+        const double f = m0.x;
+        const double sx = a0.x + a1.x, sy = a0.y + a1.y;
+        const double dx = a0.x - a1.x, dy = a0.y - a1.y;
+        a0 = make_double2(f * sx, f * sy);
+        a1 = make_double2(f * dx, f * dy);
+    } else if (SUB == G1_X) {
+        const double2 t = a0;
+        a0 = a1;
+        a1 = t;
+    } else if (SUB == G1_Y) {
+        const double2 t = a0;
+        a0 = make_double2(a1.y, -a1.x);   // -i * a1
+        a1 = make_double2(-t.y, t.x);     //  i * a0
+    } else if (SUB == G1_RX) {
+        const double c = m0.x, s = m0.y;
+        const double2 t = a0;
+        a0 = make_double2(fma(c, t.x, s * a1.y), fma(c, t.y, -s * a1.x));
+        a1 = make_double2(fma(s, t.y, c * a1.x), fma(-s, t.x, c * a1.y));
+    } else if (SUB == G1_RY) {
+        const double c = m0.x, s = m0.y;
+        const double2 t = a0;
+        a0 = make_double2(fma(c, t.x, -s * a1.x), fma(c, t.y, -s * a1.y));
+        a1 = make_double2(fma(s, t.x, c * a1.x), fma(s, t.y, c * a1.y));
+    } else {
+        const double2 t = a0;
+        double2 r0 = c_mul(m0, t), r1 = c_mul(m2, t);
+        r0.x = fma(m1.x, a1.x, r0.x); r0.x = fma(-m1.y, a1.y, r0.x);
+        r0.y = fma(m1.x, a1.y, r0.y); r0.y = fma(m1.y, a1.x, r0.y);
+        r1.x = fma(m3.x, a1.x, r1.x); r1.x = fma(-m3.y, a1.y, r1.x);
+        r1.y = fma(m3.x, a1.y, r1.y); r1.y = fma(m3.y, a1.x, r1.y);
+        a0 = r0;
+        a1 = r1;
+    }
+}
+
+// New value of this lane's amplitude x when its pair partner p sits in the
+// lane whose target bit differs; `bit` is this lane's target-bit value.
+template <int SUB>
+__device__ __forceinline__ double2 g1_lane_val(double2 x, double2 p, int bit, const double2 m0,
+                                               const double2 m1, const double2 m2, const double2 m3) {
+    if (SUB == G1_H) {
+        const double f = m0.x;
+        return bit ? make_double2(f * (p.x - x.x), f * (p.y - x.y))
+                   : make_double2(f * (x.x + p.x), f * (x.y + p.y));
+    } else if (SUB == G1_X) {
+        return p;
+    } else if (SUB == G1_Y) {
+        return bit ? make_double2(-p.y, p.x) : make_double2(p.y, -p.x);
+    } else if (SUB == G1_RX) {
+        const double c = m0.x, s = m0.y;
+        return make_double2(fma(c, x.x, s * p.y), fma(c, x.y, -s * p.x));
+    } else if (SUB == G1_RY) {
+        const double c = m0.x, s = bit ? m0.y : -m0.y;
+        return make_double2(fma(c, x.x, s * p.x), fma(c, x.y, s * p.y));
+    } else {
+        const double2 cx = bit ? m3 : m0, cp = bit ? m2 : m1;
+        double2 r = c_mul(cx, x);
+        r.x = fma(cp.x, p.x, r.x); r.x = fma(-cp.y, p.y, r.x);
+        r.y = fma(cp.x, p.y, r.y); r.y = fma(cp.y, p.x, r.y);
+        return r;
+    }
+}
+
+template <int K, int SUB>
+__device__ __forceinline__ void g1_reg(double2 (&a)[REGS], uint32_t creg, const double2* m) {
+    const double2 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
+#pragma unroll
+    for (int v = 0; v < REGS; ++v) {
+        if (v & (1 << K)) continue;
+        if ((v & creg) != creg) continue;
+        g1_pair<SUB>(a[v], a[v | (1 << K)], m0, m1, m2, m3);
+    }
+}
+
+template <int SUB>
+__device__ __forceinline__ void g1_reg_dispatch(int k, double2 (&a)[REGS], uint32_t creg, const double2* m) {
+    switch (k) {
+        case 0: g1_reg<0, SUB>(a, creg, m); break;
+        case 1: g1_reg<1, SUB>(a, creg, m); break;
+        case 2: g1_reg<2, SUB>(a, creg, m); break;
+        default: g1_reg<3, SUB>(a, creg, m); break;
+    }
+}
+
+template <int SUB>
+__device__ __forceinline__ void g1_lane(double2 (&a)[REGS], int lane, int b, bool tp, uint32_t creg,
+                                        const double2* m) {
+    const double2 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
+    const int bit = (lane >> b) & 1;
+    const int xm = 1 << b;
+#pragma unroll
+    for (int v = 0; v < REGS; ++v) {
+        if ((v & creg) != creg) continue;  // uniform across the warp
+        double2 p;
+        p.x = __shfl_xor_sync(0xffffffffu, a[v].x, xm);
+        p.y = __shfl_xor_sync(0xffffffffu, a[v].y, xm);
+        if (tp) a[v] = g1_lane_val<SUB>(a[v], p, bit, m0, m1, m2, m3);
+    }
+}
+
+// ------------------------------------------------------------ the pass kernel
+static_assert(REG_BITS == 4, "g1_reg_dispatch covers 4 register bits");
+
+__global__ void __launch_bounds__(PASS_THREADS, 2)
+k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
+       double* __restrict__ partials) {
+    extern __shared__ double2 tile[];
+    __shared__ double red[PASS_THREADS / 32];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+
+    // Global index of this CTA's tile origin: blockIdx.x deposited into the
+    // qubits outside the tile.
+    uint64_t g0 = 0;
+    {
+        const uint64_t b = blockIdx.x;
+        const int nout = (int)P.n - TILE_BITS;
+        for (int k = 0; k < nout; ++k) g0 |= ((b >> k) & 1ull) << P.outer_qubits[k];
+    }
+    int rs[REG_BITS], ws[WARP_BITS];
+#pragma unroll
+    for (int k = 0; k < REG_BITS; ++k) rs[k] = P.reg_slot0[k];
+#pragma unroll
+    for (int k = 0; k < WARP_BITS; ++k) ws[k] = P.warp_slot0[k];
+
+    uint64_t tb, rst[REG_BITS];
+    auto set_global_map = [&]() {
+        tb = g0 + (uint64_t)lane;
+#pragma unroll
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((wid >> k) & 1) tb += 1ull << P.slot_qubit[ws[k]];
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = 1ull << P.slot_qubit[rs[k]];
+    };
+    auto gidx = [&](int v) -> uint64_t {
+        uint64_t g = tb;
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k)
+            if ((v >> k) & 1) g += rst[k];
+        return g;
+    };
+    set_global_map();
+
+    const double nrm = *norm2_in;
+    const bool valid = nrm > 1e-12;
+    const double scale = valid ? 1.0 / sqrt(nrm) : 0.0;
+
+    double2 a[REGS];
+    if (valid) {
+#pragma unroll
+        for (int v = 0; v < REGS; ++v) {
+            const double2 x = __ldcs(amps + gidx(v));
+            a[v] = make_double2(x.x * scale, x.y * scale);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < REGS; ++v) a[v] = make_double2(gidx(v) == 0 ? 1.0 : 0.0, 0.0);
+    }
+
+    double2 pend = make_double2(1.0, 0.0);
+    bool dirty = false;
+    auto flush = [&]() {
+#pragma unroll
+        for (int v = 0; v < REGS; ++v) a[v] = c_mul(a[v], pend);
+        pend = make_double2(1.0, 0.0);
+        dirty = false;
+    };
+
+    const uint32_t nops = P.nops;
+    for (uint32_t oi = 0; oi < nops; ++oi) {
+        const PassOp& op = P.ops[oi];
+        const uint32_t kind = op.kind;
+        if (kind == PK_XCHG) {
+            if (dirty) flush();
+            __syncthreads();
+            {
+                uint32_t wb = 0;
+#pragma unroll
+                for (int k = 0; k < WARP_BITS; ++k)
+                    if ((wid >> k) & 1) wb += 1u << ws[k];
+#pragma unroll
+                for (int v = 0; v < REGS; ++v) {
+                    uint32_t h = wb;
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k)
+                        if ((v >> k) & 1) h += 1u << rs[k];
+                    tile[(h << LANE_BITS) + lane] = a[v];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < REG_BITS; ++k) rs[k] = op.xreg[k];
+#pragma unroll
+            for (int k = 0; k < WARP_BITS; ++k) ws[k] = op.xwarp[k];
+            {
+                uint32_t wb = 0;
+#pragma unroll
+                for (int k = 0; k < WARP_BITS; ++k)
+                    if ((wid >> k) & 1) wb += 1u << ws[k];
+#pragma unroll
+                for (int v = 0; v < REGS; ++v) {
+                    uint32_t h = wb;
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k)
+                        if ((v >> k) & 1) h += 1u << rs[k];
+                    a[v] = tile[(h << LANE_BITS) + lane];
+                }
+            }
+            set_global_map();
+            continue;
+        }
+        const bool tp = ((g0 & op.cond_outer) == op.cond_outer) &&
+                        (((uint32_t)lane & op.cond_lane) == op.cond_lane) &&
+                        (((uint32_t)wid & op.cond_warp) == op.cond_warp);
+        const uint32_t creg = op.cond_reg;
+        const double2* m = &P.coef[op.coef];
+        if (kind == PK_G1_REG) {
+            if (!tp) continue;
+            switch (op.sub) {
+                case G1_H: g1_reg_dispatch<G1_H>(op.t0, a, creg, m); break;
+                case G1_X: g1_reg_dispatch<G1_X>(op.t0, a, creg, m); break;
+                case G1_Y: g1_reg_dispatch<G1_Y>(op.t0, a, creg, m); break;
+                case G1_RX: g1_reg_dispatch<G1_RX>(op.t0, a, creg, m); break;
+                case G1_RY: g1_reg_dispatch<G1_RY>(op.t0, a, creg, m); break;
+                default: g1_reg_dispatch<G1_GEN>(op.t0, a, creg, m); break;
+            }
+        } else if (kind == PK_G1_LANE) {
+            if (dirty) flush();
+            switch (op.sub) {
+                case G1_H: g1_lane<G1_H>(a, lane, op.t0, tp, creg, m); break;
+                case G1_X: g1_lane<G1_X>(a, lane, op.t0, tp, creg, m); break;
+                case G1_Y: g1_lane<G1_Y>(a, lane, op.t0, tp, creg, m); break;
+                case G1_RX: g1_lane<G1_RX>(a, lane, op.t0, tp, creg, m); break;
+                case G1_RY: g1_lane<G1_RY>(a, lane, op.t0, tp, creg, m); break;
+                default: g1_lane<G1_GEN>(a, lane, op.t0, tp, creg, m); break;
+            }
+        } else {  // PK_DIAG
+            const uint32_t sl = op.sub & 7u;
+            const bool neg = (op.sub & 0x80u) != 0;
+            const int t0 = op.t0;
+            int sel = 0;
+            if (sl == SEL_LANE) sel = (lane >> t0) & 1;
+            else if (sl == SEL_WARP) sel = (wid >> t0) & 1;
+            else if (sl == SEL_OUTER) sel = (int)((g0 >> t0) & 1ull);
+            if (op.reg_free) {
+                dirty = true;
+                if (tp) pend = neg ? c_neg(pend) : c_mul(pend, m[sel]);
+            } else if (tp) {
+                if (sl == SEL_REG) {
+                    const double2 d0 = m[0], d1 = m[1];
+#pragma unroll
+                    for (int v = 0; v < REGS; ++v) {
+                        if ((v & creg) != creg) continue;
+                        a[v] = c_mul(a[v], ((v >> t0) & 1) ? d1 : d0);
+                    }
+                } else if (neg) {
+#pragma unroll
+                    for (int v = 0; v < REGS; ++v)
+                        if ((v & creg) == creg) a[v] = c_neg(a[v]);
+                } else {
+                    const double2 d = m[sel];
+#pragma unroll
+                    for (int v = 0; v < REGS; ++v)
+                        if ((v & creg) == creg) a[v] = c_mul(a[v], d);
+                }
+            }
+        }
+    }
+    if (dirty) flush();
+
+    double ss = 0.0;
+#pragma unroll
+    for (int v = 0; v < REGS; ++v) {
+        __stcs(amps + gidx(v), a[v]);
+        ss += c_abs2(a[v]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if (lane == 0) red[wid] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < PASS_THREADS / 32; ++w) t += red[w];
+        partials[blockIdx.x] = t;
+    }
+}
+
+// ------------------------------------------------------- per-gate kernels
+// Element-indexed grid-stride loops over [0, len) so that any slice length
+// works, as the reference's `j < len` checks allow (vectorization.rs:920-935).
+__device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+
+template <int SUB>
+__global__ void k_gate_g1(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+    const uint64_t bit = 1ull << g.t;
+    const double2 m0 = g.m[0], m1 = g.m[1], m2 = g.m[2], m3 = g.m[3];
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        if (i & bit) continue;
+        const uint64_t j = i | bit;
+        if (j >= len || (i & g.cmask) != g.cmask) continue;
+        double2 x = a[i], y = a[j];
+        g1_pair<SUB>(x, y, m0, m1, m2, m3);
+        a[i] = x;
+        a[j] = y;
+    }
+}
+
+__global__ void k_gate_diag(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+    const bool neg = (g.sub & 0x80u) != 0;
+    const bool has_sel = g.t < 64;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        if ((i & g.cmask) != g.cmask) continue;
+        if (neg) {
+            a[i] = c_neg(a[i]);
+        } else {
+            const bool s = has_sel && ((i >> g.t) & 1ull);
+            a[i] = c_mul(a[i], s ? g.m[1] : g.m[0]);
+        }
+    }
+}
+
+__global__ void k_gate_swap(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+    const uint64_t m1 = 1ull << g.t, m2 = 1ull << g.t2;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        if ((i & (m1 | m2)) != 0 || (i & g.cmask) != g.cmask) continue;
+        const uint64_t x = i | m2, y = i | m1;
+        if (x < len && y < len) {
+            const double2 t = a[x];
+            a[x] = a[y];
+            a[y] = t;
+        }
+    }
+}
+
+__global__ void k_gate_u2(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+    const uint64_t ml = 1ull << g.t, mh = 1ull << g.t2;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        if ((i & (ml | mh)) != 0) continue;
+        const uint64_t idx[4] = {i, i | ml, i | mh, i | ml | mh};
+        if (idx[3] >= len) continue;
+        double2 x[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) x[k] = a[idx[k]];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            double2 acc = c_mul(g.m[4 * r], x[0]);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                const double2 c = g.m[4 * r + k];
+                acc.x = fma(c.x, x[k].x, acc.x); acc.x = fma(-c.y, x[k].y, acc.x);
+                acc.y = fma(c.x, x[k].y, acc.y); acc.y = fma(c.y, x[k].x, acc.y);
+            }
+            a[idx[r]] = acc;
+        }
+    }
+}
+
+__global__ void k_reset_all(double2* __restrict__ a, uint64_t len) {
+    for (uint64_t i = gtid(); i < len; i += gstride()) a[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+}
+
+// --------------------------------------------------------------- reductions
+template <int NB>
+__device__ __forceinline__ void block_store_partials(double (&v)[NB], double* __restrict__ out, uint32_t stride) {
+    __shared__ double sh[NB][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        double x = v[b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[b][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < NB) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += sh[threadIdx.x][k];
+        out[(uint64_t)threadIdx.x * stride + blockIdx.x] = t;
+    }
+}
+
+// sum |a|^2 (scaled by s^2) per block
+__global__ void k_norm_partials(const double2* __restrict__ a, uint64_t len, double* __restrict__ partials) {
+    double v[1] = {0.0};
+    for (uint64_t i = gtid(); i < len; i += gstride()) v[0] += c_abs2(a[i]);
+    block_store_partials<1>(v, partials, gridDim.x);
+}
+
+// P(bit q = 0), P(bit q = 1) of the stored vector (unscaled) per block
+__global__ void k_p01_partials(const double2* __restrict__ a, uint64_t len, uint32_t q, double* __restrict__ partials) {
+    double v[2] = {0.0, 0.0};
+    const uint64_t m = 1ull << q;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        const double p = c_abs2(a[i]);
+        if (i & m) v[1] += p;
+        else v[0] += p;
+    }
+    block_store_partials<2>(v, partials, gridDim.x);
+}
+
+// Z-string sums for up to 8 masks per launch
+struct Masks8 {
+    uint64_t m[8];
+};
+
+__global__ void k_expz_partials(const double2* __restrict__ a, uint64_t len, const Masks8 mk, uint32_t k,
+                                double* __restrict__ partials) {
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t masks[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) masks[j] = (j < (int)k) ? mk.m[j] : 0ull;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        const double p = c_abs2(a[i]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] += (__popcll(i & masks[j]) & 1) ? -p : p;
+    }
+    block_store_partials<8>(v, partials, gridDim.x);
+}
+
+// Final reduction: out[s] = sum_k partials[s*count + k] in a fixed order (one
+// block per set), then optional scaling by 1/norm2 and status bookkeeping.
+__global__ void k_reduce(const double* __restrict__ partials, uint32_t count, double* __restrict__ out,
+                         const double* __restrict__ divide_by, uint32_t* __restrict__ status) {
+    __shared__ double sh[32];
+    const double* p = partials + (uint64_t)blockIdx.x * count;
+    double x = 0.0;
+    for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) x += p[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+        if (divide_by) {
+            const double d = *divide_by;
+            t = (d > 1e-12) ? t / d : 0.0;
+        }
+        out[blockIdx.x] = t;
+        if (status) {
+            if (t != t) atomicOr(&status[0], 1u);
+            if (!(t > 1e-12)) atomicAdd(&status[2], 1u);
+        }
+    }
+}
+
+// Collapse for measure / reset_qubit: keep bit q == outcome scaled by `f`
+// (already including the pending 1/||psi||), zero the other branch, and leave
+// norm partials of the result.
+__global__ void k_collapse(double2* __restrict__ a, uint64_t len, uint32_t q, uint32_t outcome, double f,
+                           double* __restrict__ partials) {
+    double v[1] = {0.0};
+    const uint64_t m = 1ull << q;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        const bool set = (i & m) != 0;
+        double2 x;
+        if (set != (outcome != 0)) x = make_double2(0.0, 0.0);
+        else {
+            x = a[i];
+            x = make_double2(x.x * f, x.y * f);
+        }
+        a[i] = x;
+        v[0] += c_abs2(x);
+    }
+    block_store_partials<1>(v, partials, gridDim.x);
+}
+
+// Materialise the pending normalisation in place (or reset to |0..0>).
+__global__ void k_materialize(double2* __restrict__ a, uint64_t len, const double* __restrict__ norm2_in,
+                              double* __restrict__ partials) {
+    double v[1] = {0.0};
+    const double nrm = *norm2_in;
+    const bool valid = nrm > 1e-12;
+    const double s = valid ? 1.0 / sqrt(nrm) : 0.0;
+    for (uint64_t i = gtid(); i < len; i += gstride()) {
+        double2 x;
+        if (valid) {
+            x = a[i];
+            x = make_double2(x.x * s, x.y * s);
+        } else {
+            x = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+        }
+        a[i] = x;
+        v[0] += c_abs2(x);
+    }
+    block_store_partials<1>(v, partials, gridDim.x);
+}
+
+__global__ void k_set_scalar(double* p, double v) { *p = v; }
+
+// Probabilities of [off, off+cnt) scaled by 1/norm2 (|0..0> when invalid).
+__global__ void k_probs(const double2* __restrict__ a, uint64_t off, uint64_t cnt, const double* __restrict__ norm2_in,
+                        double* __restrict__ out) {
+    const double nrm = *norm2_in;
+    const bool valid = nrm > 1e-12;
+    const double inv = valid ? 1.0 / nrm : 0.0;
+    for (uint64_t i = gtid(); i < cnt; i += gstride()) {
+        const uint64_t g = off + i;
+        out[i] = valid ? c_abs2(a[g]) * inv : (g == 0 ? 1.0 : 0.0);
+    }
+}
+
+// --------------------------------------------------- marginal tree & shots
+// Level k (1 <= k <= n-1) holds h_k[p] = sum_{i mod 2^k == p} |a_i|^2 for
+// p < 2^k at offset 2^k - 2 of `tree`. Level n-1 comes from the amplitudes.
+__global__ void k_tree_leaf(const double2* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
+                            double* __restrict__ lvl) {
+    const uint64_t half = 1ull << (n - 1);
+    const double nrm = *norm2_in;
+    const bool valid = nrm > 1e-12;
+    const double inv = valid ? 1.0 / nrm : 0.0;
+    for (uint64_t p = gtid(); p < half; p += gstride()) {
+        lvl[p] = valid ? (c_abs2(a[p]) + c_abs2(a[p + half])) * inv : (p == 0 ? 1.0 : 0.0);
+    }
+}
+
+__global__ void k_tree_up(const double* __restrict__ hi, double* __restrict__ lo, uint64_t cnt) {
+    for (uint64_t p = gtid(); p < cnt; p += gstride()) lo[p] = hi[p] + hi[p + cnt];
+}
+
+// One thread per shot. mode 0: the measure_all order of the reference — qubit
+// q measured with uniform u[shot*n + q] as `u < P0`, where P0 is the
+// conditional probability given the earlier outcomes; a branch with
+// probability <= 1e-12 zeroes the state, which normalize() then resets to
+// |0..0>, so every later outcome is 0 (quantum_state.rs:424-455, 888-907).
+// mode 1: inverse CDF with one uniform per shot, walking the same tree.
+__global__ void k_sample(const double2* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
+                         const double* __restrict__ tree, const double* __restrict__ u, uint64_t shots, int mode,
+                         unsigned long long* __restrict__ out) {
+    const double nrm = *norm2_in;
+    const bool valid = nrm > 1e-12;
+    const double inv = valid ? 1.0 / nrm : 0.0;
+    auto h = [&](uint32_t k, uint64_t p) -> double {
+        if (k == n) return valid ? c_abs2(a[p]) * inv : (p == 0 ? 1.0 : 0.0);
+        if (k == 0) {
+            if (n == 1) return valid ? (c_abs2(a[0]) + c_abs2(a[1])) * inv : 1.0;
+            return tree[0] + tree[1];
+        }
+        return tree[((1ull << k) - 2) + p];
+    };
+    for (uint64_t s = gtid(); s < shots; s += gstride()) {
+        uint64_t pre = 0;
+        if (mode == 0) {
+            bool dead = false;
+            for (uint32_t q = 0; q < n; ++q) {
+                const double uq = u[s * n + q];
+                if (dead) continue;  // |0..0>: P0 = 1 and u < 1
+                const double tot = h(q, pre);
+                const double p0 = h(q + 1, pre) / tot;
+                const double p1 = h(q + 1, pre | (1ull << q)) / tot;
+                const uint32_t b = (uq < p0) ? 0u : 1u;
+                const double pb = b ? p1 : p0;
+                pre |= (uint64_t)b << q;
+                if (!(pb > 1e-12)) dead = true;
+            }
+        } else {
+            double t = u[s] * h(0, 0);
+            for (uint32_t q = 0; q < n; ++q) {
+                const double left = h(q + 1, pre);
+                if (t < left) continue;
+                t -= left;
+                pre |= 1ull << q;
+            }
+        }
+        out[s] = pre;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+static int grid_for(uint64_t work, int threads, int max_blocks) {
+    uint64_t b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > (uint64_t)max_blocks) b = max_blocks;
+    return (int)b;
+}
+
+cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                        cudaStream_t st) {
+    const int smem = (1 << TILE_BITS) * (int)sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(k_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = 1u << (P.n - TILE_BITS);
+    k_pass<<<blocks, PASS_THREADS, smem, st>>>(amps, P, norm2_in, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st) {
+    const int threads = 256;
+    const int blocks = grid_for(len, threads, 148 * 16);
+    switch (g.kind) {
+        case GG_G1:
+            switch (g.sub) {
+                case G1_H: k_gate_g1<G1_H><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_X: k_gate_g1<G1_X><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_Y: k_gate_g1<G1_Y><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_RX: k_gate_g1<G1_RX><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_RY: k_gate_g1<G1_RY><<<blocks, threads, 0, st>>>(a, len, g); break;
+                default: k_gate_g1<G1_GEN><<<blocks, threads, 0, st>>>(a, len, g); break;
+            }
+            break;
+        case GG_DIAG: k_gate_diag<<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_SWAP: k_gate_swap<<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_U2: k_gate_u2<<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_RESET_ALL: k_reset_all<<<blocks, threads, 0, st>>>(a, len); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// Partial-sum grid: fixed per length so that reductions are deterministic.
+int reduce_blocks(uint64_t len) { return grid_for(len, 256, 148 * 8); }
+
+cudaError_t launch_norm(const double2* a, uint64_t len, double* partials, double* out, uint32_t* status,
+                        cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    k_norm_partials<<<nb, 256, 0, st>>>(a, len, partials);
+    k_reduce<<<1, 1024, 0, st>>>(partials, nb, out, nullptr, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_p01(const double2* a, uint64_t len, uint32_t q, double* partials, double* out2,
+                       const double* norm2, cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    k_p01_partials<<<nb, 256, 0, st>>>(a, len, q, partials);
+    k_reduce<<<2, 1024, 0, st>>>(partials, nb, out2, norm2, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expz(const double2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
+                        double* out, const double* norm2, cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    Masks8 mk{};
+    for (uint32_t j = 0; j < k && j < 8; ++j) mk.m[j] = masks[j];
+    k_expz_partials<<<nb, 256, 0, st>>>(a, len, mk, k, partials);
+    k_reduce<<<k, 1024, 0, st>>>(partials, nb, out, norm2, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_partials(const double* partials, uint32_t count, double* out, uint32_t* status,
+                                   cudaStream_t st) {
+    k_reduce<<<1, 1024, 0, st>>>(partials, count, out, nullptr, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collapse(double2* a, uint64_t len, uint32_t q, uint32_t outcome, double f, double* partials,
+                            double* norm2_out, uint32_t* status, cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    k_collapse<<<nb, 256, 0, st>>>(a, len, q, outcome, f, partials);
+    k_reduce<<<1, 1024, 0, st>>>(partials, nb, norm2_out, nullptr, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_materialize(double2* a, uint64_t len, double* norm2, double* partials, uint32_t* status,
+                               cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    k_materialize<<<nb, 256, 0, st>>>(a, len, norm2, partials);
+    k_reduce<<<1, 1024, 0, st>>>(partials, nb, norm2, nullptr, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_scalar(double* p, double v, cudaStream_t st) {
+    k_set_scalar<<<1, 1, 0, st>>>(p, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const double* norm2, double* out,
+                         cudaStream_t st) {
+    k_probs<<<grid_for(cnt, 256, 148 * 16), 256, 0, st>>>(a, off, cnt, norm2, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st) {
+    if (n < 2) return cudaSuccess;
+    double* leaf = tree + ((1ull << (n - 1)) - 2);
+    k_tree_leaf<<<grid_for(1ull << (n - 1), 256, 148 * 16), 256, 0, st>>>(a, n, norm2, leaf);
+    for (uint32_t k = n - 2; k >= 1; --k) {
+        const uint64_t cnt = 1ull << k;
+        k_tree_up<<<grid_for(cnt, 256, 148 * 16), 256, 0, st>>>(tree + ((2ull << k) - 2), tree + (cnt - 2), cnt);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
+                          uint64_t shots, int mode, unsigned long long* out, cudaStream_t st) {
+    k_sample<<<grid_for(shots, 128, 148 * 16), 128, 0, st>>>(a, n, norm2, tree, u, shots, mode, out);
+    return cudaGetLastError();
+}
+
+}  // namespace qoa

@@ -1,0 +1,34 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/qoa_cuda.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+import qoa_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "qoa_cuda.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(qoa_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_boundary():
+    names = declared()
+    for must in ("qoa_create", "qoa_apply", "qoa_measure", "qoa_sample", "qoa_get_state", "qoa_set_state",
+                 "qoa_vec_apply_hadamard", "qoa_vec_apply_controlled_phase_rotation"):
+        assert must in names
+    assert sum(n.startswith("qoa_vec_apply_") for n in names) == 17
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(qoa_b200.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_strerror_is_callable_without_gpu():
+    assert qoa_b200.lib.qoa_strerror(0) == b"ok"
+    assert b"range" in qoa_b200.lib.qoa_strerror(1)
