@@ -21,7 +21,8 @@ from . import circuits  # noqa: F401  (seeded circuit generators)
 from .circuits import OP_DTYPE, Op, ops_to_array
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libqoa_cuda.so")
+# QOA_B200_LIB points at an alternative build of the same library (A/B timing).
+LIB_PATH = os.environ.get("QOA_B200_LIB") or os.path.join(_HERE, "libqoa_cuda.so")
 
 QOA_OK, QOA_E_RANGE, QOA_E_ARG, QOA_E_OPCODE, QOA_E_CUDA, QOA_E_OOM, QOA_E_STATE, QOA_E_NOGPU = range(8)
 QOA_PREC_F64 = 0

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -89,7 +90,12 @@ struct Gate {
 inline double2 d2(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
 inline double2 from_polar(double r, double t) { return d2(r * std::cos(t), r * std::sin(t)); }
 
-bool is_pass_gate(const Gate& g) { return g.kind == K_G1 || g.kind == K_DIAG; }
+// Tile passes take every diagonal gate and the 2x2 gates; a controlled 2x2
+// must be X or Y (CNOT, Toffoli, CY), which is all the instruction set makes.
+bool is_pass_gate(const Gate& g) {
+    if (g.kind == K_DIAG) return true;
+    return g.kind == K_G1 && (g.cmask == 0 || g.sub == G1_X || g.sub == G1_Y);
+}
 bool is_barrier(const Gate& g) { return g.kind >= K_MEASURE; }
 
 // Algorithmic bytes of one per-gate application, S = 2^n * 16.
@@ -493,7 +499,7 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
         uint64_t tile = 0x1Full;  // lane qubits
         int nslots = 0;
         uint64_t bN = 0, bD = 0;  // qubits blocked by waiting gates (non-diagonal / diagonal action)
-        int budget_ops = MAX_PASS_OPS - 24;  // leave room for exchanges
+        int budget_ops = MAX_PASS_OPS / 3;  // room for the exchanges and flushes
         int budget_coef = MAX_PASS_COEF - 8;
         for (size_t i = first; i < N; ++i) {
             if (done[i]) continue;
@@ -503,7 +509,7 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
             if (ok) {
                 const uint64_t need = g.nmask & ~tile;
                 const int k = __builtin_popcountll(need);
-                const int nc = g.kind == K_G1 ? 4 : 2;
+                const int nc = g.kind == K_G1 ? 4 : 2;  // a selector diagonal becomes two phase ops
                 if (nslots + k > HIGH_SLOTS || budget_ops < 1 || budget_coef < nc) ok = false;
                 else {
                     tile |= need;
@@ -532,12 +538,23 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
     return steps;
 }
 
-// Builds the kernel op stream of a pass: picks which slots sit in registers
-// (Belady: keep the slots needed soonest) and translates every gate's qubits
-// into lane / register / warp / outer positions of the mapping in force.
+// Builds the kernel op stream of a pass. The tile's TILE_BITS index bits
+// (tile bit t < 5 = qubit t, tile bit 5 + s = high slot s) are assigned to
+// lane / register / warp roles; every 2x2 gate must act on a register bit, so
+// an exchange through shared memory re-assigns roles when its target is not
+// one (Belady: keep the bits needed soonest). The load and the store need the
+// lanes on tile bits 0..4 (coalesced), so a pass that moved them ends with an
+// exchange back. Gates are rewritten into cheaper equivalents up to a scalar:
+//   H  -> (a0+a1, a0-a1): the 1/sqrt2 is restored by the pass renormalisation;
+//   RZ -> e^{-i t/2} * diag(1, e^{i t}): the global phase joins P.phase;
+//   Z, CZ -> phase -1.
+// Diagonal factors that are constant over a thread's registers accumulate in
+// a per-thread pending factor, flushed only before an exchange that moves
+// amplitudes between threads whose factors may differ.
 int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParams& P) {
     memset(&P, 0, sizeof P);
     P.n = n;
+    P.phase = d2(1.0, 0.0);
     int slot_of[64];
     for (int q = 0; q < 64; ++q) slot_of[q] = -1;
     for (int s = 0; s < HIGH_SLOTS; ++s) {
@@ -547,138 +564,203 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     int no = 0;
     for (uint32_t q = LANE_BITS; q < n; ++q)
         if (slot_of[q] < 0) P.outer_qubits[no++] = (uint8_t)q;
+    auto tbit = [&](int q) -> int {
+        if (q < LANE_BITS) return q;
+        return slot_of[q] < 0 ? -1 : LANE_BITS + slot_of[q];
+    };
 
-    // next-use table over the gate sequence (register demand only)
+    // register demand per gate (tile bit of each 2x2 target)
     const int ng = (int)st.gates.size();
-    std::vector<int> need_slot(ng, -1);
+    std::vector<int> need(ng, -1);
     for (int i = 0; i < ng; ++i) {
         const Gate& g = G[st.gates[i]];
-        if (g.kind == K_G1 && g.t >= LANE_BITS) need_slot[i] = slot_of[g.t];
+        if (g.kind == K_G1) need[i] = tbit(g.t);
     }
-    auto next_use = [&](int from, int slot) {
+    auto next_use = [&](int from, int t) {
         for (int i = from; i < ng; ++i)
-            if (need_slot[i] == slot) return i;
+            if (need[i] == t) return i;
         return 1 << 30;
     };
-    auto choose_regs = [&](int from, int must, int (&rs)[REG_BITS], const int (&cur)[REG_BITS], bool have_cur) {
-        // candidates ordered by next use; `must` first
-        std::vector<std::pair<int, int>> c;
-        for (int s = 0; s < HIGH_SLOTS; ++s) c.push_back({s == must ? -1 : next_use(from, s), s});
-        std::sort(c.begin(), c.end());
-        int chosen[REG_BITS];
-        for (int k = 0; k < REG_BITS; ++k) chosen[k] = c[k].second;
-        // keep register positions of slots that stay
-        bool used[REG_BITS] = {false, false, false, false};
-        bool placed[REG_BITS] = {false, false, false, false};
-        int res[REG_BITS] = {-1, -1, -1, -1};
-        if (have_cur) {
-            for (int k = 0; k < REG_BITS; ++k)
-                for (int j = 0; j < REG_BITS; ++j)
-                    if (!placed[j] && chosen[j] == cur[k]) { res[k] = chosen[j]; placed[j] = true; used[k] = true; }
-        }
-        for (int j = 0; j < REG_BITS; ++j) {
-            if (placed[j]) continue;
-            for (int k = 0; k < REG_BITS; ++k)
-                if (!used[k]) { res[k] = chosen[j]; used[k] = true; break; }
-        }
-        for (int k = 0; k < REG_BITS; ++k) rs[k] = res[k];
-    };
-    auto warps_from = [&](const int (&rs)[REG_BITS], int (&ws)[WARP_BITS], const int (&curw)[WARP_BITS], bool have) {
-        bool inreg[HIGH_SLOTS] = {};
-        for (int k = 0; k < REG_BITS; ++k) inreg[rs[k]] = true;
-        std::vector<int> rest;
-        for (int s = 0; s < HIGH_SLOTS; ++s)
-            if (!inreg[s]) rest.push_back(s);
-        // keep warp positions of slots that stay in warps
-        int res[WARP_BITS] = {-1, -1, -1};
-        std::vector<char> taken(HIGH_SLOTS, 0);
-        if (have)
-            for (int k = 0; k < WARP_BITS; ++k)
-                if (!inreg[curw[k]]) { res[k] = curw[k]; taken[curw[k]] = 1; }
-        size_t ri = 0;
-        for (int k = 0; k < WARP_BITS; ++k) {
-            if (res[k] >= 0) continue;
-            while (ri < rest.size() && taken[rest[ri]]) ++ri;
-            res[k] = rest[ri];
-            taken[rest[ri]] = 1;
-        }
-        for (int k = 0; k < WARP_BITS; ++k) ws[k] = res[k];
-    };
 
-    int rs[REG_BITS], ws[WARP_BITS];
+    TileMap m;  // mapping in force
+    // initial mapping: lanes on tile bits 0..4; registers = the four high
+    // tile bits needed soonest; warps = the other two
     {
-        int dummy_r[REG_BITS] = {0, 0, 0, 0};
-        int dummy_w[WARP_BITS] = {0, 0, 0};
-        choose_regs(0, -1, rs, dummy_r, false);
-        warps_from(rs, ws, dummy_w, false);
+        for (int i = 0; i < LANE_BITS; ++i) m.lane[i] = (uint8_t)i;
+        std::vector<std::pair<int, int>> c;
+        for (int t = LANE_BITS; t < TILE_BITS; ++t) c.push_back({next_use(0, t), t});
+        std::sort(c.begin(), c.end());
+        for (int k = 0; k < REG_BITS; ++k) m.reg[k] = (uint8_t)c[k].second;
+        for (int k = 0; k < WARP_BITS; ++k) m.warp[k] = (uint8_t)c[REG_BITS + k].second;
     }
-    for (int k = 0; k < REG_BITS; ++k) P.reg_slot0[k] = (uint8_t)rs[k];
-    for (int k = 0; k < WARP_BITS; ++k) P.warp_slot0[k] = (uint8_t)ws[k];
+    P.map0 = m;
 
-    int nops = 0, ncoef = 0;
-    auto where = [&](int q, int& loc, int& idx) {
-        if (q < LANE_BITS) { loc = SEL_LANE; idx = q; return; }
-        const int s = slot_of[q];
-        if (s < 0) { loc = SEL_OUTER; idx = q; return; }
+    int nops = 0, ncoef = 0, nx = 0;
+    uint32_t dirty = 0;  // pending factor depends on lane / warp bits
+    auto new_op = [&]() -> PassOp* {
+        if (nops >= MAX_PASS_OPS) return nullptr;
+        PassOp* o = &P.ops[nops++];
+        memset(o, 0, sizeof *o);
+        return o;
+    };
+    // lane positions 0..2 carry a quarter-warp: give them tile bits with
+    // distinct residues mod 3 where the lane set allows (bank-conflict-free)
+    auto order_lanes = [&](TileMap& t) {
+        int best[LANE_BITS];
+        for (int i = 0; i < LANE_BITS; ++i) best[i] = t.lane[i];
+        int seen[3] = {-1, -1, -1};
+        std::vector<int> first, rest;
+        for (int i = 0; i < LANE_BITS; ++i) {
+            const int r = best[i] % 3;
+            if (seen[r] < 0) { seen[r] = best[i]; first.push_back(best[i]); }
+            else rest.push_back(best[i]);
+        }
+        int k = 0;
+        for (int x : first) t.lane[k++] = (uint8_t)x;
+        for (int x : rest) t.lane[k++] = (uint8_t)x;
+    };
+    auto exchange_to = [&](const TileMap& nm) -> bool {
+        if (dirty) {
+            PassOp* f = new_op();
+            if (!f) return false;
+            f->code = PC_FLUSH;
+            dirty = 0;
+        }
+        if (nx >= MAX_XCHG) return false;
+        PassOp* x = new_op();
+        if (!x) return false;
+        x->code = PC_XCHG;
+        x->coef = (uint16_t)nx;
+        P.xmap[nx++] = nm;
+        m = nm;
+        return true;
+    };
+    // bring tile bit `must` into the registers
+    auto make_reg = [&](int i, int must) -> bool {
+        std::vector<std::pair<int, int>> c;
+        for (int t = 0; t < TILE_BITS; ++t) c.push_back({t == must ? -1 : next_use(i, t), t});
+        std::sort(c.begin(), c.end());
+        bool want[TILE_BITS] = {};
+        for (int k = 0; k < REG_BITS; ++k) want[c[k].second] = true;
+        TileMap nm = m;
+        // outgoing register bits take the positions the incoming bits leave
+        std::vector<int> outgoing;
         for (int k = 0; k < REG_BITS; ++k)
-            if (rs[k] == s) { loc = SEL_REG; idx = k; return; }
-        for (int k = 0; k < WARP_BITS; ++k)
-            if (ws[k] == s) { loc = SEL_WARP; idx = k; return; }
-        loc = -1; idx = -1;
+            if (!want[m.reg[k]]) outgoing.push_back(m.reg[k]);
+        std::vector<int> incoming;
+        for (int t = 0; t < TILE_BITS; ++t) {
+            if (!want[t]) continue;
+            bool held = false;
+            for (int k = 0; k < REG_BITS; ++k) held |= m.reg[k] == t;
+            if (!held) incoming.push_back(t);
+        }
+        size_t oi = 0;
+        for (int t : incoming) {
+            const int o = outgoing[oi++];
+            for (int k = 0; k < REG_BITS; ++k)
+                if (nm.reg[k] == o) nm.reg[k] = (uint8_t)t;
+            for (int k = 0; k < LANE_BITS; ++k)
+                if (m.lane[k] == t) nm.lane[k] = (uint8_t)o;
+            for (int k = 0; k < WARP_BITS; ++k)
+                if (m.warp[k] == t) nm.warp[k] = (uint8_t)o;
+        }
+        order_lanes(nm);
+        return exchange_to(nm);
     };
     auto cond = [&](uint64_t mask, PassOp& op) {
         for (int q = 0; q < 64; ++q) {
             if (!((mask >> q) & 1)) continue;
-            int loc, idx;
-            where(q, loc, idx);
-            if (loc == SEL_LANE) op.cond_lane |= (uint8_t)(1u << idx);
-            else if (loc == SEL_REG) op.cond_reg |= (uint8_t)(1u << idx);
-            else if (loc == SEL_WARP) op.cond_warp |= (uint8_t)(1u << idx);
-            else op.cond_outer |= 1ull << q;
+            const int t = tbit(q);
+            if (t < 0) { op.cond_outer |= 1ull << q; continue; }
+            for (int k = 0; k < LANE_BITS; ++k)
+                if (m.lane[k] == t) op.cond_lane |= (uint8_t)(1u << k);
+            for (int k = 0; k < REG_BITS; ++k)
+                if (m.reg[k] == t) op.cond_reg |= (uint8_t)(1u << k);
+            for (int k = 0; k < WARP_BITS; ++k)
+                if (m.warp[k] == t) op.cond_warp |= (uint8_t)(1u << k);
         }
+        op.has_tp = (op.cond_lane || op.cond_warp || op.cond_outer) ? 1 : 0;
     };
+    auto phase_op = [&](uint64_t mask, double2 d) -> bool {
+        if (mask == 0) {  // global factor
+            P.phase = d2(P.phase.x * d.x - P.phase.y * d.y, P.phase.x * d.y + P.phase.y * d.x);
+            return true;
+        }
+        PassOp* o = new_op();
+        if (!o || ncoef >= MAX_PASS_COEF) return false;
+        cond(mask, *o);
+        o->coef = (uint16_t)ncoef;
+        P.coef[ncoef++] = d;
+        if (o->cond_reg == 0) {
+            o->code = PC_DIAG_T;
+            if (o->cond_lane || o->cond_warp) dirty = 1;
+        } else {
+            o->code = PC_DIAG_M;
+        }
+        return true;
+    };
+
     for (int i = 0; i < ng; ++i) {
         const Gate& g = G[st.gates[i]];
-        if (nops >= MAX_PASS_OPS - 1) return -1;
-        if (g.kind == K_G1 && g.t >= LANE_BITS) {
-            const int s = slot_of[g.t];
-            bool inreg = false;
-            for (int k = 0; k < REG_BITS; ++k) inreg |= rs[k] == s;
-            if (!inreg) {
-                int nrs[REG_BITS], nws[WARP_BITS];
-                choose_regs(i, s, nrs, rs, true);
-                warps_from(nrs, nws, ws, true);
-                PassOp& x = P.ops[nops++];
-                memset(&x, 0, sizeof x);
-                x.kind = PK_XCHG;
-                for (int k = 0; k < REG_BITS; ++k) { x.xreg[k] = (uint8_t)nrs[k]; rs[k] = nrs[k]; }
-                for (int k = 0; k < WARP_BITS; ++k) { x.xwarp[k] = (uint8_t)nws[k]; ws[k] = nws[k]; }
+        if (g.kind == K_G1) {
+            const int t = tbit(g.t);
+            int k = -1;
+            for (int j = 0; j < REG_BITS; ++j)
+                if (m.reg[j] == t) k = j;
+            if (k < 0) {
+                if (!make_reg(i, t)) return -1;
+                for (int j = 0; j < REG_BITS; ++j)
+                    if (m.reg[j] == t) k = j;
+            }
+            PassOp* o = new_op();
+            if (!o) return -1;
+            cond(g.cmask, *o);
+            o->k = (uint8_t)k;
+            const bool controlled = o->has_tp || o->cond_reg;
+            const int sub = g.sub == G1_H ? G1_HF : g.sub;
+            switch (sub) {
+                case G1_X: o->code = (uint8_t)(PC_XC + k); break;
+                case G1_Y: o->code = (uint8_t)(PC_YC + k); break;
+                case G1_HF: o->code = (uint8_t)(PC_HF + k); break;
+                case G1_RX: o->code = (uint8_t)(PC_RX + k); break;
+                case G1_RY: o->code = (uint8_t)(PC_RY + k); break;
+                default: o->code = (uint8_t)(PC_GEN + k); break;
+            }
+            if (controlled && sub != G1_X && sub != G1_Y) return -1;
+            if (ncoef + 4 > MAX_PASS_COEF) return -1;
+            o->coef = (uint16_t)ncoef;
+            for (int j = 0; j < 4; ++j) P.coef[ncoef++] = g.m[j];
+        } else {  // K_DIAG
+            if (g.neg) {
+                if (!phase_op(g.cmask, d2(-1, 0))) return -1;
+            } else if (g.t < 0) {
+                if (!phase_op(g.cmask, g.m[0])) return -1;
+            } else {
+                // (bit t ? d1 : d0) under cmask = d0 under cmask, then d1/d0 under cmask|t
+                const double2 d0 = g.m[0], d1 = g.m[1];
+                const double2 r = d2(d1.x * d0.x + d1.y * d0.y, d1.y * d0.x - d1.x * d0.y);  // d1 * conj(d0)
+                const double s2 = d0.x * d0.x + d0.y * d0.y;
+                if (!phase_op(g.cmask, d0)) return -1;
+                if (!phase_op(g.cmask | (1ull << g.t), d2(r.x / s2, r.y / s2))) return -1;
             }
         }
-        if (nops >= MAX_PASS_OPS) return -1;
-        PassOp& op = P.ops[nops++];
-        memset(&op, 0, sizeof op);
-        op.coef = (uint16_t)ncoef;
-        if (g.kind == K_G1) {
-            int loc, idx;
-            where(g.t, loc, idx);
-            op.kind = (loc == SEL_LANE) ? PK_G1_LANE : PK_G1_REG;
-            op.sub = (uint8_t)g.sub;
-            op.t0 = (uint8_t)idx;
-            cond(g.cmask, op);
-            for (int k = 0; k < 4; ++k) P.coef[ncoef++] = g.m[k];
-        } else {  // K_DIAG
-            op.kind = PK_DIAG;
-            int loc = SEL_NONE, idx = 0;
-            if (g.t >= 0) where(g.t, loc, idx);
-            op.sub = (uint8_t)(loc | (g.neg ? 0x80 : 0));
-            op.t0 = (uint8_t)idx;
-            cond(g.cmask, op);
-            op.reg_free = (uint8_t)((loc != SEL_REG && op.cond_reg == 0) ? 1 : 0);
-            P.coef[ncoef++] = g.m[0];
-            P.coef[ncoef++] = g.m[1];
-        }
-        if (ncoef > MAX_PASS_COEF) return -1;
+    }
+    // lanes back on tile bits 0..4 for the coalesced store
+    bool canonical = true;
+    for (int i = 0; i < LANE_BITS; ++i) canonical &= m.lane[i] == i;
+    if (!canonical) {
+        TileMap nm;
+        for (int i = 0; i < LANE_BITS; ++i) nm.lane[i] = (uint8_t)i;
+        std::vector<int> high;
+        for (int k = 0; k < REG_BITS; ++k)
+            if (m.reg[k] >= LANE_BITS) high.push_back(m.reg[k]);
+        for (int k = 0; k < WARP_BITS; ++k)
+            if (m.warp[k] >= LANE_BITS) high.push_back(m.warp[k]);
+        for (int k = 0; k < LANE_BITS; ++k)
+            if (m.lane[k] >= LANE_BITS) high.push_back(m.lane[k]);
+        for (int k = 0; k < REG_BITS; ++k) nm.reg[k] = (uint8_t)high[k];
+        for (int k = 0; k < WARP_BITS; ++k) nm.warp[k] = (uint8_t)high[REG_BITS + k];
+        if (!exchange_to(nm)) return -1;
     }
     P.nops = (uint32_t)nops;
     P.ncoef = (uint32_t)ncoef;
@@ -1231,6 +1313,15 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
             static thread_local PassParams P;
             if (build_pass(G, steps[si], ex.n, P) != 0)
                 return set_err(nullptr, QOA_E_ARG, "pass %zu does not fit one launch", si);
+            if (getenv("QOA_PLAN_STATS")) {  // op mix of each pass, for tuning
+                int cnt[PC_NCODES] = {};
+                for (uint32_t o = 0; o < P.nops; ++o) cnt[P.ops[o].code < PC_NCODES ? P.ops[o].code : 0]++;
+                int g1 = 0;
+                for (int c = PC_HF; c < PC_NCODES; ++c) g1 += cnt[c];
+                fprintf(stderr, "pass %zu: gates %zu ops %u g1 %d diag_t %d diag_m %d xchg %d flush %d\n", si,
+                        steps[si].gates.size(), P.nops, g1, cnt[PC_DIAG_T], cnt[PC_DIAG_M], cnt[PC_XCHG],
+                        cnt[PC_FLUSH]);
+            }
         }
     }
     for (size_t gi = 0; gi < G.size(); ++gi) {

@@ -27,7 +27,8 @@ __device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
 __device__ __forceinline__ double2 c_neg(double2 a) { return make_double2(-a.x, -a.y); }
 __device__ __forceinline__ double c_abs2(double2 a) { return fma(a.x, a.x, a.y * a.y); }
 
-// 2x2 on the amplitude pair (a0 = bit 0, a1 = bit 1).
+// 2x2 on the amplitude pair (a0 = bit 0, a1 = bit 1). G1_H is the exact
+// Hadamard (per-gate kernels); G1_HF drops its 1/sqrt2 (tile passes).
 template <int SUB>
 __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 m0, const double2 m1,
                                         const double2 m2, const double2 m3) {
@@ -37,6 +38,10 @@ __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 
         const double dx = a0.x - a1.x, dy = a0.y - a1.y;
         a0 = make_double2(f * sx, f * sy);
         a1 = make_double2(f * dx, f * dy);
+    } else if (SUB == G1_HF) {
+        const double2 t = a0;
+        a0 = make_double2(t.x + a1.x, t.y + a1.y);
+        a1 = make_double2(t.x - a1.x, t.y - a1.y);
     } else if (SUB == G1_X) {
         const double2 t = a0;
         a0 = a1;
@@ -67,75 +72,46 @@ __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 
     }
 }
 
-// New value of this lane's amplitude x when its pair partner p sits in the
-// lane whose target bit differs; `bit` is this lane's target-bit value.
-template <int SUB>
-__device__ __forceinline__ double2 g1_lane_val(double2 x, double2 p, int bit, const double2 m0,
-                                               const double2 m1, const double2 m2, const double2 m3) {
-    if (SUB == G1_H) {
-        const double f = m0.x;
-        return bit ? make_double2(f * (p.x - x.x), f * (p.y - x.y))
-                   : make_double2(f * (x.x + p.x), f * (x.y + p.y));
-    } else if (SUB == G1_X) {
-        return p;
-    } else if (SUB == G1_Y) {
-        return bit ? make_double2(-p.y, p.x) : make_double2(p.y, -p.x);
-    } else if (SUB == G1_RX) {
-        const double c = m0.x, s = m0.y;
-        return make_double2(fma(c, x.x, s * p.y), fma(c, x.y, -s * p.x));
-    } else if (SUB == G1_RY) {
-        const double c = m0.x, s = bit ? m0.y : -m0.y;
-        return make_double2(fma(c, x.x, s * p.x), fma(c, x.y, s * p.y));
-    } else {
-        const double2 cx = bit ? m3 : m0, cp = bit ? m2 : m1;
-        double2 r = c_mul(cx, x);
-        r.x = fma(cp.x, p.x, r.x); r.x = fma(-cp.y, p.y, r.x);
-        r.y = fma(cp.x, p.y, r.y); r.y = fma(cp.y, p.x, r.y);
-        return r;
-    }
-}
-
-template <int K, int SUB>
-__device__ __forceinline__ void g1_reg(double2 (&a)[REGS], uint32_t creg, const double2* m) {
-    const double2 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
+// ------------------------------------------------- tile pass building blocks
+template <int SUB, int K>
+__device__ __forceinline__ void g1r(double2 (&a)[REGS], const double2* __restrict__ m) {
+    double2 m0 = make_double2(0, 0), m1 = m0, m2 = m0, m3 = m0;
+    if (SUB == G1_RX || SUB == G1_RY || SUB == G1_GEN) m0 = m[0];
+    if (SUB == G1_GEN) { m1 = m[1]; m2 = m[2]; m3 = m[3]; }
 #pragma unroll
-    for (int v = 0; v < REGS; ++v) {
-        if (v & (1 << K)) continue;
-        if ((v & creg) != creg) continue;
-        g1_pair<SUB>(a[v], a[v | (1 << K)], m0, m1, m2, m3);
-    }
+    for (int v = 0; v < REGS; ++v)
+        if (!(v & (1 << K))) g1_pair<SUB>(a[v], a[v | (1 << K)], m0, m1, m2, m3);
 }
 
-template <int SUB>
-__device__ __forceinline__ void g1_reg_dispatch(int k, double2 (&a)[REGS], uint32_t creg, const double2* m) {
-    switch (k) {
-        case 0: g1_reg<0, SUB>(a, creg, m); break;
-        case 1: g1_reg<1, SUB>(a, creg, m); break;
-        case 2: g1_reg<2, SUB>(a, creg, m); break;
-        default: g1_reg<3, SUB>(a, creg, m); break;
-    }
-}
-
-template <int SUB>
-__device__ __forceinline__ void g1_lane(double2 (&a)[REGS], int lane, int b, bool tp, uint32_t creg,
-                                        const double2* m) {
-    const double2 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
-    const int bit = (lane >> b) & 1;
-    const int xm = 1 << b;
+// X / Y where every condition bit is set (tp: lane / warp / outer part)
+template <int SUB, int K>
+__device__ __forceinline__ void g1rc(double2 (&a)[REGS], bool tp, uint32_t creg) {
+    if (!tp) return;
+    const double2 z = make_double2(0, 0);
 #pragma unroll
-    for (int v = 0; v < REGS; ++v) {
-        if ((v & creg) != creg) continue;  // uniform across the warp
-        double2 p;
-        p.x = __shfl_xor_sync(0xffffffffu, a[v].x, xm);
-        p.y = __shfl_xor_sync(0xffffffffu, a[v].y, xm);
-        if (tp) a[v] = g1_lane_val<SUB>(a[v], p, bit, m0, m1, m2, m3);
-    }
+    for (int v = 0; v < REGS; ++v)
+        if (!(v & (1 << K)) && (v & creg) == creg) g1_pair<SUB>(a[v], a[v | (1 << K)], z, z, z, z);
+}
+
+__device__ __forceinline__ void diag_m(double2 (&a)[REGS], bool tp, uint32_t creg, double2 d) {
+    if (!tp) return;
+#pragma unroll
+    for (int v = 0; v < REGS; ++v)
+        if ((v & creg) == creg) a[v] = c_mul(a[v], d);
+}
+
+// Shared-memory position of tile index j: the low three bits are XORed with
+// the three-bit folds of the higher bits, so any three tile bits with distinct
+// residues mod 3 spread a quarter-warp's 16-byte accesses over all banks.
+__device__ __forceinline__ uint32_t spos(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
+
+// Global index stride of tile bit t (t < 5: qubit t; else high slot t - 5).
+__device__ __forceinline__ uint64_t tstride(const PassParams& P, uint32_t t) {
+    return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
 }
 
 // ------------------------------------------------------------ the pass kernel
-static_assert(REG_BITS == 4, "g1_reg_dispatch covers 4 register bits");
-
-__global__ void __launch_bounds__(PASS_THREADS, 2)
+__global__ void __launch_bounds__(PASS_THREADS, 4)
 k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
        double* __restrict__ partials) {
     extern __shared__ double2 tile[];
@@ -151,162 +127,168 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((b >> k) & 1ull) << P.outer_qubits[k];
     }
-    int rs[REG_BITS], ws[WARP_BITS];
-#pragma unroll
-    for (int k = 0; k < REG_BITS; ++k) rs[k] = P.reg_slot0[k];
-#pragma unroll
-    for (int k = 0; k < WARP_BITS; ++k) ws[k] = P.warp_slot0[k];
 
-    uint64_t tb, rst[REG_BITS];
-    auto set_global_map = [&]() {
-        tb = g0 + (uint64_t)lane;
-#pragma unroll
-        for (int k = 0; k < WARP_BITS; ++k)
-            if ((wid >> k) & 1) tb += 1ull << P.slot_qubit[ws[k]];
-#pragma unroll
-        for (int k = 0; k < REG_BITS; ++k) rst[k] = 1ull << P.slot_qubit[rs[k]];
-    };
-    auto gidx = [&](int v) -> uint64_t {
-        uint64_t g = tb;
-#pragma unroll
-        for (int k = 0; k < REG_BITS; ++k)
-            if ((v >> k) & 1) g += rst[k];
-        return g;
-    };
-    set_global_map();
+    // op stream and coefficients -> shared memory (after the tile)
+    const uint32_t nops = P.nops;
+    uint4* sops = reinterpret_cast<uint4*>(tile + (1 << TILE_BITS));
+    double2* scoef = reinterpret_cast<double2*>(sops + nops);
+    {
+        const uint4* gops = reinterpret_cast<const uint4*>(P.ops);
+        for (uint32_t i = threadIdx.x; i < nops; i += PASS_THREADS) sops[i] = gops[i];
+        for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS) scoef[i] = P.coef[i];
+    }
 
     const double nrm = *norm2_in;
     const bool valid = nrm > 1e-12;
-    const double scale = valid ? 1.0 / sqrt(nrm) : 0.0;
+    // The input's 1/||psi|| and the pass's factored global phase are applied
+    // once, at the end, as part of the per-thread pending factor.
+    double2 pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;
 
+    // Load with the initial mapping: lanes are tile bits 0..4 = qubits 0..4,
+    // so each warp reads 512 contiguous bytes per register.
     double2 a[REGS];
-    if (valid) {
+    {
+        uint64_t tb = g0 + (uint64_t)lane;
+#pragma unroll
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((wid >> k) & 1) tb += tstride(P, P.map0.warp[k]);
+        uint64_t rst[REG_BITS];
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = tstride(P, P.map0.reg[k]);
 #pragma unroll
         for (int v = 0; v < REGS; ++v) {
-            const double2 x = __ldcs(amps + gidx(v));
-            a[v] = make_double2(x.x * scale, x.y * scale);
-        }
-    } else {
+            uint64_t g = tb;
 #pragma unroll
-        for (int v = 0; v < REGS; ++v) a[v] = make_double2(gidx(v) == 0 ? 1.0 : 0.0, 0.0);
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) g += rst[k];
+            a[v] = valid ? __ldcs(amps + g) : make_double2(g == 0 ? 1.0 : 0.0, 0.0);
+        }
     }
+    __syncthreads();  // op stream staged
 
-    double2 pend = make_double2(1.0, 0.0);
-    bool dirty = false;
-    auto flush = [&]() {
-#pragma unroll
-        for (int v = 0; v < REGS; ++v) a[v] = c_mul(a[v], pend);
-        pend = make_double2(1.0, 0.0);
-        dirty = false;
-    };
-
-    const uint32_t nops = P.nops;
+    const uint32_t* ow = reinterpret_cast<const uint32_t*>(sops);
+    int cur = -1;  // mapping in force: -1 = map0, else xmap index
+    uint32_t w = nops ? ow[0] : 0;
     for (uint32_t oi = 0; oi < nops; ++oi) {
-        const PassOp& op = P.ops[oi];
-        const uint32_t kind = op.kind;
-        if (kind == PK_XCHG) {
-            if (dirty) flush();
-            __syncthreads();
-            {
-                uint32_t wb = 0;
-#pragma unroll
-                for (int k = 0; k < WARP_BITS; ++k)
-                    if ((wid >> k) & 1) wb += 1u << ws[k];
-#pragma unroll
-                for (int v = 0; v < REGS; ++v) {
-                    uint32_t h = wb;
-#pragma unroll
-                    for (int k = 0; k < REG_BITS; ++k)
-                        if ((v >> k) & 1) h += 1u << rs[k];
-                    tile[(h << LANE_BITS) + lane] = a[v];
-                }
+        const uint32_t hot = w;
+        if (oi + 1 < nops) w = ow[4 * (oi + 1)];
+        const uint32_t code = hot & 0xffu;
+        const double2* m = scoef + (hot >> 16);
+        // condition of ops that take one: register mask and thread predicate
+        auto conds = [&](bool& tp) -> uint32_t {
+            const uint32_t cw = ow[4 * oi + 1];
+            tp = true;
+            if (cw >> 24) {
+                const unsigned long long co = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+                const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
             }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < REG_BITS; ++k) rs[k] = op.xreg[k];
-#pragma unroll
-            for (int k = 0; k < WARP_BITS; ++k) ws[k] = op.xwarp[k];
-            {
-                uint32_t wb = 0;
-#pragma unroll
-                for (int k = 0; k < WARP_BITS; ++k)
-                    if ((wid >> k) & 1) wb += 1u << ws[k];
-#pragma unroll
-                for (int v = 0; v < REGS; ++v) {
-                    uint32_t h = wb;
-#pragma unroll
-                    for (int k = 0; k < REG_BITS; ++k)
-                        if ((v >> k) & 1) h += 1u << rs[k];
-                    a[v] = tile[(h << LANE_BITS) + lane];
-                }
+            return cw & 0xffu;
+        };
+        switch (code) {
+#define QOA_K4(BASE, ...) \
+    case BASE + 0: { constexpr int K = 0; __VA_ARGS__; } break; \
+    case BASE + 1: { constexpr int K = 1; __VA_ARGS__; } break; \
+    case BASE + 2: { constexpr int K = 2; __VA_ARGS__; } break; \
+    case BASE + 3: { constexpr int K = 3; __VA_ARGS__; } break;
+            QOA_K4(PC_HF, g1r<G1_HF, K>(a, m))
+            QOA_K4(PC_RX, g1r<G1_RX, K>(a, m))
+            QOA_K4(PC_RY, g1r<G1_RY, K>(a, m))
+            QOA_K4(PC_GEN, g1r<G1_GEN, K>(a, m))
+            QOA_K4(PC_XC, bool tp; const uint32_t cr = conds(tp); g1rc<G1_X, K>(a, tp, cr))
+            QOA_K4(PC_YC, bool tp; const uint32_t cr = conds(tp); g1rc<G1_Y, K>(a, tp, cr))
+#undef QOA_K4
+            case PC_DIAG_T: {
+                bool tp;
+                conds(tp);
+                if (tp) pend = c_mul(pend, m[0]);
+                break;
             }
-            set_global_map();
-            continue;
-        }
-        const bool tp = ((g0 & op.cond_outer) == op.cond_outer) &&
-                        (((uint32_t)lane & op.cond_lane) == op.cond_lane) &&
-                        (((uint32_t)wid & op.cond_warp) == op.cond_warp);
-        const uint32_t creg = op.cond_reg;
-        const double2* m = &P.coef[op.coef];
-        if (kind == PK_G1_REG) {
-            if (!tp) continue;
-            switch (op.sub) {
-                case G1_H: g1_reg_dispatch<G1_H>(op.t0, a, creg, m); break;
-                case G1_X: g1_reg_dispatch<G1_X>(op.t0, a, creg, m); break;
-                case G1_Y: g1_reg_dispatch<G1_Y>(op.t0, a, creg, m); break;
-                case G1_RX: g1_reg_dispatch<G1_RX>(op.t0, a, creg, m); break;
-                case G1_RY: g1_reg_dispatch<G1_RY>(op.t0, a, creg, m); break;
-                default: g1_reg_dispatch<G1_GEN>(op.t0, a, creg, m); break;
+            case PC_DIAG_M: {
+                bool tp;
+                const uint32_t cr = conds(tp);
+                diag_m(a, tp, cr, m[0]);
+                break;
             }
-        } else if (kind == PK_G1_LANE) {
-            if (dirty) flush();
-            switch (op.sub) {
-                case G1_H: g1_lane<G1_H>(a, lane, op.t0, tp, creg, m); break;
-                case G1_X: g1_lane<G1_X>(a, lane, op.t0, tp, creg, m); break;
-                case G1_Y: g1_lane<G1_Y>(a, lane, op.t0, tp, creg, m); break;
-                case G1_RX: g1_lane<G1_RX>(a, lane, op.t0, tp, creg, m); break;
-                case G1_RY: g1_lane<G1_RY>(a, lane, op.t0, tp, creg, m); break;
-                default: g1_lane<G1_GEN>(a, lane, op.t0, tp, creg, m); break;
-            }
-        } else {  // PK_DIAG
-            const uint32_t sl = op.sub & 7u;
-            const bool neg = (op.sub & 0x80u) != 0;
-            const int t0 = op.t0;
-            int sel = 0;
-            if (sl == SEL_LANE) sel = (lane >> t0) & 1;
-            else if (sl == SEL_WARP) sel = (wid >> t0) & 1;
-            else if (sl == SEL_OUTER) sel = (int)((g0 >> t0) & 1ull);
-            if (op.reg_free) {
-                dirty = true;
-                if (tp) pend = neg ? c_neg(pend) : c_mul(pend, m[sel]);
-            } else if (tp) {
-                if (sl == SEL_REG) {
-                    const double2 d0 = m[0], d1 = m[1];
+            case PC_FLUSH:
+#pragma unroll
+                for (int v = 0; v < REGS; ++v) a[v] = c_mul(a[v], pend);
+                pend = make_double2(1.0, 0.0);
+                break;
+            case PC_XCHG: {
+                // write under the current mapping, read under the new one
+                const TileMap& mo = cur < 0 ? P.map0 : P.xmap[cur];
+                const int nxt = (int)(hot >> 16);
+                const TileMap& mn = P.xmap[nxt];
+                __syncthreads();
+                {
+                    uint32_t jb = 0;
+#pragma unroll
+                    for (int i = 0; i < LANE_BITS; ++i) jb |= ((uint32_t)(lane >> i) & 1u) << mo.lane[i];
+#pragma unroll
+                    for (int i = 0; i < WARP_BITS; ++i) jb |= ((uint32_t)(wid >> i) & 1u) << mo.warp[i];
+                    const uint32_t pb = spos(jb);
+                    uint32_t pr[REG_BITS];
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k) pr[k] = spos(1u << mo.reg[k]);
 #pragma unroll
                     for (int v = 0; v < REGS; ++v) {
-                        if ((v & creg) != creg) continue;
-                        a[v] = c_mul(a[v], ((v >> t0) & 1) ? d1 : d0);
+                        uint32_t p = pb;
+#pragma unroll
+                        for (int k = 0; k < REG_BITS; ++k)
+                            if ((v >> k) & 1) p ^= pr[k];
+                        tile[p] = a[v];
                     }
-                } else if (neg) {
-#pragma unroll
-                    for (int v = 0; v < REGS; ++v)
-                        if ((v & creg) == creg) a[v] = c_neg(a[v]);
-                } else {
-                    const double2 d = m[sel];
-#pragma unroll
-                    for (int v = 0; v < REGS; ++v)
-                        if ((v & creg) == creg) a[v] = c_mul(a[v], d);
                 }
+                __syncthreads();
+                {
+                    uint32_t jb = 0;
+#pragma unroll
+                    for (int i = 0; i < LANE_BITS; ++i) jb |= ((uint32_t)(lane >> i) & 1u) << mn.lane[i];
+#pragma unroll
+                    for (int i = 0; i < WARP_BITS; ++i) jb |= ((uint32_t)(wid >> i) & 1u) << mn.warp[i];
+                    const uint32_t pb = spos(jb);
+                    uint32_t pr[REG_BITS];
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k) pr[k] = spos(1u << mn.reg[k]);
+#pragma unroll
+                    for (int v = 0; v < REGS; ++v) {
+                        uint32_t p = pb;
+#pragma unroll
+                        for (int k = 0; k < REG_BITS; ++k)
+                            if ((v >> k) & 1) p ^= pr[k];
+                        a[v] = tile[p];
+                    }
+                }
+                cur = nxt;
+                break;
             }
+            default: break;
         }
     }
-    if (dirty) flush();
 
+    // final flush of the pending factor, store (the last mapping has lanes on
+    // tile bits 0..4 again), and norm partials
     double ss = 0.0;
+    {
+        const TileMap& mf = cur < 0 ? P.map0 : P.xmap[cur];
+        uint64_t tb = g0 + (uint64_t)lane;
 #pragma unroll
-    for (int v = 0; v < REGS; ++v) {
-        __stcs(amps + gidx(v), a[v]);
-        ss += c_abs2(a[v]);
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((wid >> k) & 1) tb += tstride(P, mf.warp[k]);
+        uint64_t rst[REG_BITS];
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = tstride(P, mf.reg[k]);
+#pragma unroll
+        for (int v = 0; v < REGS; ++v) {
+            uint64_t g = tb;
+#pragma unroll
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) g += rst[k];
+            const double2 x = c_mul(a[v], pend);
+            __stcs(amps + g, x);
+            ss += c_abs2(x);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
@@ -315,7 +297,7 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
     if (threadIdx.x == 0) {
         double t = 0.0;
 #pragma unroll
-        for (int w = 0; w < PASS_THREADS / 32; ++w) t += red[w];
+        for (int w2 = 0; w2 < PASS_THREADS / 32; ++w2) t += red[w2];
         partials[blockIdx.x] = t;
     }
 }
@@ -613,8 +595,9 @@ static int grid_for(uint64_t work, int threads, int max_blocks) {
 
 cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
                         cudaStream_t st) {
-    const int smem = (1 << TILE_BITS) * (int)sizeof(double2);
-    cudaError_t e = cudaFuncSetAttribute(k_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int smem = (1 << TILE_BITS) * (int)sizeof(double2) + (int)P.nops * 16 + (int)P.ncoef * 16;
+    cudaError_t e = cudaFuncSetAttribute(k_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (1 << TILE_BITS) * (int)sizeof(double2) + MAX_PASS_OPS * 16 + MAX_PASS_COEF * 16);
     if (e != cudaSuccess) return e;
     const unsigned blocks = 1u << (P.n - TILE_BITS);
     k_pass<<<blocks, PASS_THREADS, smem, st>>>(amps, P, norm2_in, partials);
@@ -628,6 +611,7 @@ cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t s
         case GG_G1:
             switch (g.sub) {
                 case G1_H: k_gate_g1<G1_H><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_HF: k_gate_g1<G1_HF><<<blocks, threads, 0, st>>>(a, len, g); break;
                 case G1_X: k_gate_g1<G1_X><<<blocks, threads, 0, st>>>(a, len, g); break;
                 case G1_Y: k_gate_g1<G1_Y><<<blocks, threads, 0, st>>>(a, len, g); break;
                 case G1_RX: k_gate_g1<G1_RX><<<blocks, threads, 0, st>>>(a, len, g); break;

@@ -24,62 +24,78 @@ namespace qoa {
 // ---------------------------------------------------------------------------
 constexpr int LANE_BITS = 5;
 constexpr int REG_BITS = 4;
-constexpr int WARP_BITS = 3;
+constexpr int WARP_BITS = 2;
 constexpr int HIGH_SLOTS = REG_BITS + WARP_BITS;          // high qubits per pass
-constexpr int TILE_BITS = LANE_BITS + HIGH_SLOTS;         // 12 -> 4096 amps, 64 KB
-constexpr int PASS_THREADS = 32 << WARP_BITS;              // 256
+constexpr int TILE_BITS = LANE_BITS + HIGH_SLOTS;         // 11 -> 2048 amps, 32 KB
+constexpr int PASS_THREADS = 32 << WARP_BITS;              // 128
 constexpr int REGS = 1 << REG_BITS;                        // 16 amps per thread
-constexpr int MAX_PASS_OPS = 320;
-constexpr int MAX_PASS_COEF = 640;                         // double2 coefficients
+constexpr int MAX_PASS_OPS = 640;
+constexpr int MAX_PASS_COEF = 768;                         // double2 coefficients
+constexpr int MAX_XCHG = 48;
 
-// Op kinds inside a pass.
-enum PassOpKind : uint8_t {
-    PK_G1_REG = 0,   // 2x2 on register bit t0
-    PK_G1_LANE = 1,  // 2x2 on lane bit t0 (qubit t0 < 5), via shuffles
-    PK_DIAG = 2,     // diagonal factor: (sel ? d1 : d0) where the condition holds
-    PK_XCHG = 3,     // shared-memory exchange to a new register/warp mapping
+// 2x2 forms. Coefficients at coef[c..]:
+//   G1_HF  (a0+a1, a0-a1): the Hadamard with its 1/sqrt2 left to the pass renormalisation
+//   G1_X   swap; G1_Y (-i a1, i a0)
+//   G1_RX  [[al, -i be], [-i be, al]]  al = coef.x, be = coef.y
+//   G1_RY  [[al, -be], [be, al]]
+//   G1_GEN general complex 2x2 (coef[c..c+3] = m00 m01 m10 m11)
+//   G1_H   exact Hadamard (per-gate kernels only)
+enum G1Sub : uint8_t { G1_HF = 0, G1_X = 1, G1_Y = 2, G1_RX = 3, G1_RY = 4, G1_GEN = 5, G1_NSUB = 6, G1_H = 7 };
+
+// Op codes of the pass interpreter (one flat jump table). Register-bit ops
+// come in four copies, one per register bit k, so every pair index is a
+// compile-time register name.
+enum PassCode : uint8_t {
+    PC_NOP = 0,
+    PC_XCHG = 1,      // shared-memory exchange to mapping `coef`
+    PC_FLUSH = 2,     // registers *= per-thread pending factor
+    PC_DIAG_T = 3,    // pending factor *= coef[c] where the thread condition holds
+    PC_DIAG_M = 4,    // registers with (v & cond_reg) == cond_reg *= coef[c] (thread condition too)
+    PC_HF = 8,        // +k
+    PC_RX = 12,       // +k
+    PC_RY = 16,       // +k
+    PC_GEN = 20,      // +k
+    PC_XC = 24,       // +k: X on register bit k where the conditions hold (CNOT, Toffoli, X)
+    PC_YC = 28,       // +k: Y likewise (CY, Y)
+    PC_NCODES = 32,
 };
 
-// 2x2 specialisations (sub field). Coefficients at coef[c..c+3] = m00 m01 m10 m11.
-enum G1Sub : uint8_t {
-    G1_GEN = 0,  // general complex 2x2
-    G1_H = 1,    // (a+b)*f, (a-b)*f with real f = coef[c].x
-    G1_X = 2,    // swap
-    G1_Y = 3,    // (-i a1, i a0)
-    G1_RX = 4,   // [[c, -is], [-is, c]] with c = coef[c].x, s = coef[c].y
-    G1_RY = 5,   // [[c, -s], [s, c]]
-};
-
-// Location of the selector bit of a PK_DIAG op.
-enum SelLoc : uint8_t { SEL_NONE = 0, SEL_REG = 1, SEL_LANE = 2, SEL_WARP = 3, SEL_OUTER = 4 };
-
-// One op of a pass. Conditions: every listed bit must be 1 (control masks of
-// CNOT / Toffoli / CY, and the CZ / CPHASE / phase-gate masks).
+// One op of a pass (16 bytes). The first 32-bit word (code, k, coef) is all
+// the interpreter loop reads; the condition words are read only by ops that
+// take conditions. Conditions: every listed bit must be 1 (controls of CNOT /
+// Toffoli / CY; masks of phase gates, CZ, CPHASE).
 struct PassOp {
-    uint8_t kind;
-    uint8_t sub;        // G1Sub, or SelLoc for PK_DIAG
-    uint8_t t0;         // register bit / lane bit / selector index
-    uint8_t reg_free;   // PK_DIAG: 1 when the factor is constant over a thread's registers
-    uint16_t coef;      // index into PassParams::coef
+    uint8_t code;
+    uint8_t k;          // register bit of the op
+    uint16_t coef;      // index into PassParams::coef; PC_XCHG: mapping index
     uint8_t cond_reg;   // register-bit mask
     uint8_t cond_lane;  // lane-bit mask
     uint8_t cond_warp;  // warp-bit mask
-    uint8_t xreg[REG_BITS];   // PK_XCHG: slot held by each register bit afterwards
-    uint8_t xwarp[WARP_BITS]; // PK_XCHG: slot held by each warp bit afterwards
-    uint64_t cond_outer;      // mask over global index bits outside the tile
+    uint8_t has_tp;     // any lane / warp / outer condition
+    uint64_t cond_outer;// mask over global index bits outside the tile
+};
+static_assert(sizeof(PassOp) == 16, "k_pass reads a PassOp as 32/64-bit words");
+
+// A register / lane / warp assignment of the tile's TILE_BITS index bits.
+// Tile bit t < 5 is qubit t; tile bit 5 + s is high slot s.
+struct TileMap {
+    uint8_t lane[LANE_BITS];
+    uint8_t reg[REG_BITS];
+    uint8_t warp[WARP_BITS];
 };
 
-// Everything a pass kernel launch needs, passed by value (__grid_constant__):
-// kernel parameters live in the constant bank, so every warp reads the op
-// stream with broadcast loads and concurrent launches never share it.
+// Everything a pass kernel launch needs, passed by value (__grid_constant__);
+// each CTA copies the op stream and coefficients into shared memory once.
 struct PassParams {
-    uint32_t n;                  // qubits
+    uint32_t n;                       // qubits
     uint32_t nops;
     uint32_t ncoef;
+    uint32_t pad_;
+    double2 phase;                    // global phase of the factored gates of this pass
     uint8_t slot_qubit[HIGH_SLOTS];   // global qubit of each high slot
-    uint8_t reg_slot0[REG_BITS];      // initial mapping: slot of each register bit
-    uint8_t warp_slot0[WARP_BITS];    // initial mapping: slot of each warp bit
     uint8_t outer_qubits[64];         // qubits outside the tile, ascending (n - TILE_BITS of them)
+    TileMap map0;                     // mapping at load (lanes = tile bits 0..4)
+    TileMap xmap[MAX_XCHG];           // mappings after each exchange
     PassOp ops[MAX_PASS_OPS];
     double2 coef[MAX_PASS_COEF];
 };

@@ -4,7 +4,7 @@ against the oracle without a GPU."""
 import numpy as np
 
 K_G1, K_DIAG, K_SWAP, K_U2 = 0, 1, 2, 3
-G1_GEN, G1_H, G1_X, G1_Y, G1_RX, G1_RY = range(6)
+G1_HF, G1_X, G1_Y, G1_RX, G1_RY, G1_GEN, G1_H = 0, 1, 2, 3, 4, 5, 7
 
 
 def g1_matrix(sub, m):
