@@ -198,6 +198,27 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
              int32_t* pass_of, int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits,
              double* gate_matrix, size_t* ngates, size_t* npasses);
 
+/* ---- allocation-free entry point ----------------------------------------- */
+/* No counterpart in the reference. <Z_mask> = sum_i (-1)^popcount(i & mask)
+ * |a_i|^2 over a state vector the CALLER owns in device memory (`d_amps`,
+ * `len` interleaved complex128 values, used as given, not renormalised), for
+ * k <= QOA_NOALLOC_MAX_MASKS masks; the k results go to the caller's device
+ * array `d_out`. Work is queued on the caller's cudaStream_t `stream` (NULL =
+ * legacy default stream) and the call returns without waiting.
+ * It calls no cudaMalloc, cudaFree or other allocating routine, for callers
+ * that cannot allow one: a host runtime that owns and accounts for every
+ * device buffer itself, or a latency-critical caller that cannot accept
+ * cudaMalloc's implicit synchronisation. Its scratch is one fixed static
+ * device array of 75,776 bytes that every device loading the library holds
+ * until exit. The first call on each device resolves that array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race: order
+ * them. More than QOA_NOALLOC_MAX_MASKS masks -> QOA_E_ARG (see
+ * qoa_last_error(NULL)). */
+#define QOA_NOALLOC_MAX_MASKS 8
+int qoa_expect_z_noalloc(const void* d_amps, size_t len, const uint64_t* masks, size_t k, double* d_out,
+                         void* stream);
+
 /* ---- (ii) slice-level shims: src/vectorization.rs pub fns ---------------- */
 /* `amps` points to `len` interleaved complex128 values in host memory. */
 int qoa_vec_apply_hadamard(double* amps, size_t len, double norm_re, double norm_im, size_t mask_bit); /* vectorization.rs:16 */

@@ -46,6 +46,19 @@ cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, con
 using namespace qoa;
 
 namespace {
+std::mutex g_err_mu;
+std::string g_err;  // errors before a handle exists
+}  // namespace
+
+namespace qoa {
+// Records an error for qoa_last_error(NULL) (entry points without a handle).
+void note_global_error(const char* msg) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = msg;
+}
+}  // namespace qoa
+
+namespace {
 
 // ---------------------------------------------------------------- Philox
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). Draw (seed; stream,
@@ -140,9 +153,6 @@ struct qoa_state_s {
 };
 
 namespace {
-
-std::mutex g_err_mu;
-std::string g_err;  // errors before a handle exists
 
 int set_err(qoa_state_t s, int code, const char* fmt, ...) {
     char buf[512];
