@@ -33,9 +33,16 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = {"workload": "random layered circuit, H layer + 20 layers", "n_qubits": 30, "gates": 930,
+WORKLOAD = {"workload": "random layered circuit, H layer + 20 layers", "n_qubits": 30, "depth": 20, "gates": 930,
             "state_bytes": 16 << 30, "dtype": "complex128", "cz_mask": "reference (index-as-mask)",
             "l2_policy": "inputs larger than L2 (16 GiB state)", "seed": 1}
+
+
+def set_workload(n: int, depth: int):
+    """Smaller instances of the same circuit family (profiling captures)."""
+    WORKLOAD.update(n_qubits=n, depth=depth, gates=n + depth * (n + n // 2), state_bytes=16 << n,
+                    workload=f"random layered circuit, H layer + {depth} layers",
+                    l2_policy="inputs larger than L2" if (16 << n) > (126 << 20) else "state fits in L2")
 
 
 def dist_env():
@@ -111,6 +118,19 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def pass_traffic_bytes(n: int):
+    """DRAM bytes per tile-pass launch at n qubits, scaled from the committed
+    ncu capture of the 26-qubit instance (traffic grows with the amplitudes)."""
+    p = os.path.join(ROOT, "profiles", "k_pass_layered26.md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_amplitude:"):
+                return float(line.split(":")[1]) * (1 << n)
+    except OSError:
+        pass
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -145,7 +165,7 @@ def run_reference(args):
     from qoa_b200 import circuits as C
     from oracle import pyoracle as po
     n = WORKLOAD["n_qubits"]
-    ops = C.ops_to_array(C.layered_h_workload(n, 20, WORKLOAD["seed"]))
+    ops = C.ops_to_array(C.layered_h_workload(n, WORKLOAD["depth"], WORKLOAD["seed"]))
     po.set_fast(False)
     st = po.OracleState(n, 1)
     per_step = args.ref_gates_per_step
@@ -170,8 +190,8 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD),
             "cpu_baseline": {"value": value, "unit": "gates/s", "cores": threads, "kind": "port",
-                             "sample": f"{per_step} gate(s) per step of the 930-gate circuit at n=30, in order, "
-                                       "faithful oracle: single-thread gate loop + all-core normalize"},
+                             "sample": f"{per_step} gate(s) per step of the {len(ops)}-gate circuit at n={n}, in "
+                                       "order, faithful oracle: single-thread gate loop + all-core normalize"},
             "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     st.close()
@@ -195,7 +215,7 @@ def run_ours(args):
     from qoa_b200 import circuits as C
 
     n = WORKLOAD["n_qubits"]
-    ops_list = C.layered_h_workload(n, 20, WORKLOAD["seed"])
+    ops_list = C.layered_h_workload(n, WORKLOAD["depth"], WORKLOAD["seed"])
     ops = C.ops_to_array(ops_list)
     G = len(ops)
 
@@ -245,7 +265,8 @@ def run_ours(args):
     avg_ms = float(pass_ms.mean()) if pass_ms.size else float("nan")
     achieved = float(pass_bytes.mean() / (avg_ms / 1e3) / 1e9) if pass_ms.size else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None, "traffic": pass_traffic_bytes(n),
+                "traffic_source": "ncu dram bytes of the 26-qubit instance, scaled per amplitude",
                 "kernel": "k_pass", "launches_per_step": int(pass_ms.size), "avg_launch_ms": avg_ms,
                 "algorithmic_bytes_per_launch": float(pass_bytes.mean()) if pass_ms.size else None,
                 "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
@@ -284,7 +305,7 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu:
         g, k, thr = cpu_gates_per_s(ops, n, args.cpu_gates, args.cpu_seconds)
         cpu = {"value": g, "unit": "gates/s", "cores": thr, "kind": "port",
-               "sample": f"first {k} gates of the same 930-gate circuit at n=30 (16 GiB), faithful oracle: "
+               "sample": f"first {k} gates of the same {G}-gate circuit at n={n}, faithful oracle: "
                          "single-thread gate loop + all-core normalize after each gate"}
 
     if rank == 0:
@@ -314,7 +335,11 @@ def main():
     ap.add_argument("--cpu-gates", type=int, default=12)
     ap.add_argument("--cpu-seconds", type=float, default=25.0)
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
+    ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
+    ap.add_argument("--depth", type=int, default=20)
     args = ap.parse_args()
+    if (args.qubits, args.depth) != (30, 20):
+        set_workload(args.qubits, args.depth)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

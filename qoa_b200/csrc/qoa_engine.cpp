@@ -613,6 +613,85 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         memset(o, 0, sizeof *o);
         return o;
     };
+    // Deferred diagonal factors (they commute with everything up to the next
+    // 2x2 on one of their register bits, or the next exchange):
+    //   tab[v]  product of the register-only phases, per register index v
+    //   tm      thread-only phases (lane / warp / outer conditions), emitted as
+    //           one PC_DIAG_TM group
+    double2 tab[REGS];
+    uint32_t tab_bits = 0;
+    int tab_count = 0;
+    PassOp tab_last;
+    double2 tab_last_d = d2(1, 0);
+    std::vector<std::pair<PassOp, double2>> tm;
+    std::vector<std::pair<PassOp, double2>> mx;  // register x thread phases
+    uint32_t mx_bits = 0;
+    auto tab_reset = [&]() {
+        for (int v = 0; v < REGS; ++v) tab[v] = d2(1, 0);
+        tab_bits = 0;
+        tab_count = 0;
+    };
+    tab_reset();
+    auto flush_tab = [&]() -> bool {
+        if (tab_count == 0) return true;
+        PassOp* o = new_op();
+        if (!o) return false;
+        if (tab_count == 1) {  // one phase: the masked form touches fewer registers
+            *o = tab_last;
+            if (ncoef >= MAX_PASS_COEF) return false;
+            o->coef = (uint16_t)ncoef;
+            P.coef[ncoef++] = tab_last_d;
+        } else {
+            if (ncoef + REGS > MAX_PASS_COEF) return false;
+            o->code = PC_DIAG_TAB;
+            o->coef = (uint16_t)ncoef;
+            for (int v = 0; v < REGS; ++v) P.coef[ncoef++] = tab[v];
+        }
+        tab_reset();
+        return true;
+    };
+    // a group header followed by its entry records (one dispatch)
+    auto emit_group = [&](std::vector<std::pair<PassOp, double2>>& list, uint8_t code) -> bool {
+        size_t at = 0;
+        while (at < list.size()) {
+            const size_t cnt = std::min<size_t>(255, list.size() - at);
+            PassOp* h = new_op();
+            if (!h) return false;
+            h->code = code;
+            h->k = (uint8_t)cnt;
+            for (size_t e = 0; e < cnt; ++e) {
+                PassOp* r = new_op();
+                if (!r || ncoef >= MAX_PASS_COEF) return false;
+                *r = list[at + e].first;
+                r->code = PC_NOP;
+                r->coef = (uint16_t)ncoef;
+                P.coef[ncoef++] = list[at + e].second;
+            }
+            at += cnt;
+        }
+        list.clear();
+        return true;
+    };
+    auto flush_tm = [&]() -> bool { return emit_group(tm, PC_DIAG_TM); };
+    auto flush_mx = [&]() -> bool {
+        mx_bits = 0;
+        if (mx.size() == 1) {  // a lone entry needs no group header
+            PassOp* e = new_op();
+            if (!e || ncoef >= MAX_PASS_COEF) return false;
+            *e = mx[0].first;
+            e->code = PC_DIAG_M;
+            e->coef = (uint16_t)ncoef;
+            P.coef[ncoef++] = mx[0].second;
+            mx.clear();
+            return true;
+        }
+        // runs of equal register masks share one register multiply in the kernel
+        std::stable_sort(mx.begin(), mx.end(), [](const std::pair<PassOp, double2>& x,
+                                                  const std::pair<PassOp, double2>& y) {
+            return x.first.cond_reg < y.first.cond_reg;
+        });
+        return emit_group(mx, PC_DIAG_MX);
+    };
     // lane positions 0..2 carry a quarter-warp: give them tile bits with
     // distinct residues mod 3 where the lane set allows (bank-conflict-free)
     auto order_lanes = [&](TileMap& t) {
@@ -630,6 +709,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         for (int x : rest) t.lane[k++] = (uint8_t)x;
     };
     auto exchange_to = [&](const TileMap& nm) -> bool {
+        if (!flush_tab() || !flush_mx() || !flush_tm()) return false;
         if (dirty) {
             PassOp* f = new_op();
             if (!f) return false;
@@ -696,17 +776,28 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             P.phase = d2(P.phase.x * d.x - P.phase.y * d.y, P.phase.x * d.y + P.phase.y * d.x);
             return true;
         }
-        PassOp* o = new_op();
-        if (!o || ncoef >= MAX_PASS_COEF) return false;
-        cond(mask, *o);
-        o->coef = (uint16_t)ncoef;
-        P.coef[ncoef++] = d;
-        if (o->cond_reg == 0) {
-            o->code = PC_DIAG_T;
-            if (o->cond_lane || o->cond_warp) dirty = 1;
-        } else {
-            o->code = PC_DIAG_M;
+        PassOp o;
+        memset(&o, 0, sizeof o);
+        cond(mask, o);
+        if (o.cond_reg == 0) {  // thread-only: joins the pending factor
+            o.code = PC_DIAG_T;
+            if (o.cond_lane || o.cond_warp) dirty = 1;
+            tm.push_back({o, d});
+            return true;
         }
+        if (!o.has_tp) {  // register-only: joins the table
+            for (int v = 0; v < REGS; ++v)
+                if (((uint32_t)v & o.cond_reg) == o.cond_reg)
+                    tab[v] = d2(tab[v].x * d.x - tab[v].y * d.y, tab[v].x * d.y + tab[v].y * d.x);
+            tab_bits |= o.cond_reg;
+            o.code = PC_DIAG_M;
+            tab_last = o;
+            tab_last_d = d;
+            ++tab_count;
+            return true;
+        }
+        mx.push_back({o, d});  // register and thread conditions together
+        mx_bits |= o.cond_reg;
         return true;
     };
 
@@ -722,6 +813,16 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
                 for (int j = 0; j < REG_BITS; ++j)
                     if (m.reg[j] == t) k = j;
             }
+            // deferred register phases on this bit or on a control bit must land first
+            uint32_t touch = 1u << k;
+            {
+                PassOp c;
+                memset(&c, 0, sizeof c);
+                cond(g.cmask, c);
+                touch |= c.cond_reg;
+            }
+            if ((tab_bits & touch) && !flush_tab()) return -1;
+            if ((mx_bits & touch) && !flush_mx()) return -1;
             PassOp* o = new_op();
             if (!o) return -1;
             cond(g.cmask, *o);
@@ -740,6 +841,16 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             if (ncoef + 4 > MAX_PASS_COEF) return -1;
             o->coef = (uint16_t)ncoef;
             for (int j = 0; j < 4; ++j) P.coef[ncoef++] = g.m[j];
+            if (sub == G1_RX || sub == G1_RY) {
+                // factor out the larger of |cos|, |sin|: its sign joins the
+                // global phase, its magnitude the renormalisation
+                const double c = g.m[0].x, sn = g.m[0].y;
+                const bool a_form = std::fabs(c) >= std::fabs(sn);
+                const double f = a_form ? c : sn;
+                P.coef[o->coef] = d2(a_form ? sn / c : c / sn, 0.0);
+                if (f < 0) P.phase = d2(-P.phase.x, -P.phase.y);
+                if (!a_form) o->code = (uint8_t)((sub == G1_RX ? PC_RXB : PC_RYB) + k);
+            }
         } else {  // K_DIAG
             if (g.neg) {
                 if (!phase_op(g.cmask, d2(-1, 0))) return -1;
@@ -755,6 +866,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             }
         }
     }
+    if (!flush_tab() || !flush_mx() || !flush_tm()) return -1;
     // lanes back on tile bits 0..4 for the coalesced store
     bool canonical = true;
     for (int i = 0; i < LANE_BITS; ++i) canonical &= m.lane[i] == i;
@@ -1328,9 +1440,10 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
                 for (uint32_t o = 0; o < P.nops; ++o) cnt[P.ops[o].code < PC_NCODES ? P.ops[o].code : 0]++;
                 int g1 = 0;
                 for (int c = PC_HF; c < PC_NCODES; ++c) g1 += cnt[c];
-                fprintf(stderr, "pass %zu: gates %zu ops %u g1 %d diag_t %d diag_m %d xchg %d flush %d\n", si,
-                        steps[si].gates.size(), P.nops, g1, cnt[PC_DIAG_T], cnt[PC_DIAG_M], cnt[PC_XCHG],
-                        cnt[PC_FLUSH]);
+                const int disp = (int)P.nops - cnt[PC_NOP];
+                fprintf(stderr, "pass %zu: gates %zu dispatches %d g1 %d tm %d mx %d (entries %d) tab %d diag_m %d xchg %d flush %d\n",
+                        si, steps[si].gates.size(), disp, g1, cnt[PC_DIAG_TM], cnt[PC_DIAG_MX], cnt[PC_NOP],
+                        cnt[PC_DIAG_TAB], cnt[PC_DIAG_M], cnt[PC_XCHG], cnt[PC_FLUSH]);
             }
         }
     }

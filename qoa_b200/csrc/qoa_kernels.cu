@@ -60,6 +60,26 @@ __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 
         const double2 t = a0;
         a0 = make_double2(fma(c, t.x, -s * a1.x), fma(c, t.y, -s * a1.y));
         a1 = make_double2(fma(s, t.x, c * a1.x), fma(s, t.y, c * a1.y));
+    } else if (SUB == G1_RXA) {
+        const double t = m0.x;
+        const double2 u = a0;
+        a0 = make_double2(fma(t, a1.y, u.x), fma(-t, a1.x, u.y));
+        a1 = make_double2(fma(t, u.y, a1.x), fma(-t, u.x, a1.y));
+    } else if (SUB == G1_RXB) {
+        const double r = m0.x;
+        const double2 u = a0;
+        a0 = make_double2(fma(r, u.x, a1.y), fma(r, u.y, -a1.x));
+        a1 = make_double2(fma(r, a1.x, u.y), fma(r, a1.y, -u.x));
+    } else if (SUB == G1_RYA) {
+        const double t = m0.x;
+        const double2 u = a0;
+        a0 = make_double2(fma(-t, a1.x, u.x), fma(-t, a1.y, u.y));
+        a1 = make_double2(fma(t, u.x, a1.x), fma(t, u.y, a1.y));
+    } else if (SUB == G1_RYB) {
+        const double r = m0.x;
+        const double2 u = a0;
+        a0 = make_double2(fma(r, u.x, -a1.x), fma(r, u.y, -a1.y));
+        a1 = make_double2(fma(r, a1.x, u.x), fma(r, a1.y, u.y));
     } else {
         const double2 t = a0;
         double2 r0 = c_mul(m0, t), r1 = c_mul(m2, t);
@@ -76,7 +96,7 @@ __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 
 template <int SUB, int K>
 __device__ __forceinline__ void g1r(double2 (&a)[REGS], const double2* __restrict__ m) {
     double2 m0 = make_double2(0, 0), m1 = m0, m2 = m0, m3 = m0;
-    if (SUB == G1_RX || SUB == G1_RY || SUB == G1_GEN) m0 = m[0];
+    if (SUB != G1_HF && SUB != G1_X && SUB != G1_Y) m0 = m[0];
     if (SUB == G1_GEN) { m1 = m[1]; m2 = m[2]; m3 = m[3]; }
 #pragma unroll
     for (int v = 0; v < REGS; ++v)
@@ -192,8 +212,10 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
     case BASE + 2: { constexpr int K = 2; __VA_ARGS__; } break; \
     case BASE + 3: { constexpr int K = 3; __VA_ARGS__; } break;
             QOA_K4(PC_HF, g1r<G1_HF, K>(a, m))
-            QOA_K4(PC_RX, g1r<G1_RX, K>(a, m))
-            QOA_K4(PC_RY, g1r<G1_RY, K>(a, m))
+            QOA_K4(PC_RX, g1r<G1_RXA, K>(a, m))
+            QOA_K4(PC_RY, g1r<G1_RYA, K>(a, m))
+            QOA_K4(PC_RXB, g1r<G1_RXB, K>(a, m))
+            QOA_K4(PC_RYB, g1r<G1_RYB, K>(a, m))
             QOA_K4(PC_GEN, g1r<G1_GEN, K>(a, m))
             QOA_K4(PC_XC, bool tp; const uint32_t cr = conds(tp); g1rc<G1_X, K>(a, tp, cr))
             QOA_K4(PC_YC, bool tp; const uint32_t cr = conds(tp); g1rc<G1_Y, K>(a, tp, cr))
@@ -208,6 +230,56 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
                 bool tp;
                 const uint32_t cr = conds(tp);
                 diag_m(a, tp, cr, m[0]);
+                break;
+            }
+            case PC_DIAG_MX: {
+                // entries sorted by register mask: each run of equal masks
+                // folds its thread-conditioned factors into one scalar, then
+                // multiplies the matching registers once
+                const uint32_t cnt = (hot >> 8) & 0xffu;
+                double2 f = make_double2(1.0, 0.0);
+                for (uint32_t e = 1; e <= cnt; ++e) {
+                    const uint4 rec = sops[oi + e];
+                    bool tp = true;
+                    const uint32_t cw = rec.y;
+                    if (cw >> 24) {
+                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
+                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
+                    }
+                    if (tp) f = c_mul(f, scoef[rec.x >> 16]);
+                    const bool last = (e == cnt) || ((sops[oi + e + 1].y & 0xffu) != (cw & 0xffu));
+                    if (last) {
+                        diag_m(a, true, cw & 0xffu, f);
+                        f = make_double2(1.0, 0.0);
+                    }
+                }
+                oi += cnt;
+                if (oi + 1 < nops) w = ow[4 * (oi + 1)];
+                break;
+            }
+            case PC_DIAG_TAB:
+#pragma unroll
+                for (int v = 0; v < REGS; ++v) a[v] = c_mul(a[v], m[v]);
+                break;
+            case PC_DIAG_TM: {
+                // entries oi+1 .. oi+cnt: independent factors, multiplied in
+                const uint32_t cnt = (hot >> 8) & 0xffu;
+                double2 f = make_double2(1.0, 0.0);
+                for (uint32_t e = 1; e <= cnt; ++e) {
+                    const uint4 rec = sops[oi + e];
+                    bool tp = true;
+                    const uint32_t cw = rec.y;
+                    if (cw >> 24) {
+                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
+                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
+                    }
+                    if (tp) f = c_mul(f, scoef[rec.x >> 16]);
+                }
+                pend = c_mul(pend, f);
+                oi += cnt;
+                if (oi + 1 < nops) w = ow[4 * (oi + 1)];
                 break;
             }
             case PC_FLUSH:

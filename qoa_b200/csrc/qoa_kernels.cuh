@@ -40,7 +40,13 @@ constexpr int MAX_XCHG = 48;
 //   G1_RY  [[al, -be], [be, al]]
 //   G1_GEN general complex 2x2 (coef[c..c+3] = m00 m01 m10 m11)
 //   G1_H   exact Hadamard (per-gate kernels only)
-enum G1Sub : uint8_t { G1_HF = 0, G1_X = 1, G1_Y = 2, G1_RX = 3, G1_RY = 4, G1_GEN = 5, G1_NSUB = 6, G1_H = 7 };
+enum G1Sub : uint8_t {
+    G1_HF = 0, G1_X = 1, G1_Y = 2, G1_RX = 3, G1_RY = 4, G1_GEN = 5, G1_NSUB = 6, G1_H = 7,
+    // rotations with the larger of |cos|, |sin| factored out (tile passes):
+    //   RXA [[1, -i t], [-i t, 1]]  RXB [[r, -i], [-i, r]]
+    //   RYA [[1, -t], [t, 1]]       RYB [[r, -1], [1, r]]     (t or r = coef.x)
+    G1_RXA = 8, G1_RXB = 9, G1_RYA = 10, G1_RYB = 11,
+};
 
 // Op codes of the pass interpreter (one flat jump table). Register-bit ops
 // come in four copies, one per register bit k, so every pair index is a
@@ -51,13 +57,18 @@ enum PassCode : uint8_t {
     PC_FLUSH = 2,     // registers *= per-thread pending factor
     PC_DIAG_T = 3,    // pending factor *= coef[c] where the thread condition holds
     PC_DIAG_M = 4,    // registers with (v & cond_reg) == cond_reg *= coef[c] (thread condition too)
+    PC_DIAG_TAB = 5,  // register v *= coef[c + v] (a product of register-only phases)
+    PC_DIAG_TM = 6,   // the next k ops are PC_DIAG_T entries: pending factor *= each (one dispatch)
+    PC_DIAG_MX = 7,   // the next k ops are PC_DIAG_M entries, applied in one dispatch
     PC_HF = 8,        // +k
     PC_RX = 12,       // +k
     PC_RY = 16,       // +k
     PC_GEN = 20,      // +k
     PC_XC = 24,       // +k: X on register bit k where the conditions hold (CNOT, Toffoli, X)
     PC_YC = 28,       // +k: Y likewise (CY, Y)
-    PC_NCODES = 32,
+    PC_RXB = 32,      // +k (PC_RX carries the A form)
+    PC_RYB = 36,      // +k (PC_RY carries the A form)
+    PC_NCODES = 40,
 };
 
 // One op of a pass (16 bytes). The first 32-bit word (code, k, coef) is all
