@@ -58,6 +58,10 @@ extern "C" {
 
 /* ---- precision -------------------------------------------------------- */
 #define QOA_PREC_F64  0  /* complex128 amplitudes: the plain (drop-in) method */
+/* complex64 amplitudes, gates fused on the host (FP64) into dense blocks of
+ * up to 5 qubits applied on the tensor cores (3xTF32, FP32 accumulation);
+ * norms and probabilities stay FP64. Needs n >= 11; unitary ops only. */
+#define QOA_PREC_F32  1
 
 /* ---- handle flags ------------------------------------------------------ */
 /* CZ / CPHASE condition mask. The reference's QuantumState passes the raw
@@ -165,7 +169,8 @@ int qoa_probabilities(qoa_state_t s, double* out);
 /* <Z_mask> = sum_i (-1)^popcount(i & mask) |a_i|^2 for k masks. */
 int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out);
 /* get_state_vector / set_state_vector (quantum_state.rs:1129-1145); set
- * renormalises. bytes must be 2^n * 16. */
+ * renormalises. bytes must be 2^n * 16 (complex128), or 2^n * 8 (complex64)
+ * for a QOA_PREC_F32 handle. */
 int qoa_get_state(qoa_state_t s, void* host, size_t bytes);
 int qoa_set_state(qoa_state_t s, const void* host, size_t bytes);
 /* seed_rng (quantum_state.rs:956): seeds the handle's Philox4x32-10 stream. */

@@ -26,6 +26,7 @@ LIB_PATH = os.environ.get("QOA_B200_LIB") or os.path.join(_HERE, "libqoa_cuda.so
 
 QOA_OK, QOA_E_RANGE, QOA_E_ARG, QOA_E_OPCODE, QOA_E_CUDA, QOA_E_OOM, QOA_E_STATE, QOA_E_NOGPU = range(8)
 QOA_PREC_F64 = 0
+QOA_PREC_F32 = 1
 QOA_FLAG_COMPAT_MASK_QUIRK = 0x1
 QOA_FLAG_PER_GATE = 0x2
 QOA_FLAG_PROFILE = 0x4
@@ -148,13 +149,18 @@ class QuantumState:
 
     def __init__(self, n_qubits: int, noise_config: Optional[NoiseConfig] = None, *,
                  compat_mask_quirk: bool = False, per_gate: bool = False, profile: bool = False,
-                 noise_gate_qubits_only: bool = False, seed: int = 0):
+                 noise_gate_qubits_only: bool = False, seed: int = 0, precision: str = "f64"):
         flags = ((QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0)
                  | (QOA_FLAG_PER_GATE if per_gate else 0)
                  | (QOA_FLAG_PROFILE if profile else 0)
                  | (QOA_FLAG_NOISE_GATE_QUBITS if noise_gate_qubits_only else 0))
+        if precision not in ("f64", "f32"):
+            raise ValueError("precision must be 'f64' or 'f32'")
+        self.precision = precision
+        self._dtype = np.complex64 if precision == "f32" else np.complex128
         h = ctypes.c_void_p()
-        _check(lib.qoa_create(max(int(n_qubits), 1), QOA_PREC_F64, flags, ctypes.byref(h)))
+        _check(lib.qoa_create(max(int(n_qubits), 1), QOA_PREC_F32 if precision == "f32" else QOA_PREC_F64, flags,
+                              ctypes.byref(h)))
         self._h = h
         self.flags = flags
         self.noise_config = noise_config
@@ -270,12 +276,12 @@ class QuantumState:
     def get_state_vector(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         n = self.n
         if out is None:
-            out = np.empty(1 << n, dtype=np.complex128)
+            out = np.empty(1 << n, dtype=self._dtype)
         _check(lib.qoa_get_state(self._h, _ptr(out), out.nbytes), self._h)
         return out
 
     def set_state_vector(self, amps: np.ndarray):
-        a = np.ascontiguousarray(np.asarray(amps, dtype=np.complex128))
+        a = np.ascontiguousarray(np.asarray(amps, dtype=self._dtype))
         _check(lib.qoa_set_state(self._h, _ptr(a), a.nbytes), self._h)
 
     def expect_z(self, masks: Iterable[int]) -> np.ndarray:

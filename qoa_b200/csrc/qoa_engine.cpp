@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <complex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -41,6 +42,15 @@ cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const dou
 cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st);
 cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
                           uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
+cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32Phase* phases,
+                            const double* norm2_in, double* partials, cudaStream_t st);
+cudaError_t launch_f32_reset(float2* a, uint64_t len, cudaStream_t st);
+cudaError_t launch_f32_norm(const float2* a, uint64_t len, double* partials, double* out, uint32_t* status,
+                            cudaStream_t st);
+cudaError_t launch_f32_materialize(float2* a, uint64_t len, double* norm2, double* partials, uint32_t* status,
+                                   cudaStream_t st);
+cudaError_t launch_f32_probs(const float2* a, uint64_t off, uint64_t cnt, const double* norm2, double* out,
+                             cudaStream_t st);
 }  // namespace qoa
 
 using namespace qoa;
@@ -130,6 +140,11 @@ double gate_bytes(const Gate& g, uint32_t n) {
 struct qoa_state_s {
     uint32_t n = 1;
     uint32_t flags = 0;
+    int precision = QOA_PREC_F64;
+    float* f32_mats = nullptr;       // FP32 passes: block matrices (device)
+    size_t f32_mats_cap = 0;
+    F32Phase* f32_phases = nullptr;  // FP32 passes: phase entries (device)
+    size_t f32_phases_cap = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     double2* amps = nullptr;
@@ -188,7 +203,7 @@ int alloc_state(qoa_state_t s, uint32_t n) {
     if (s->amps) { cudaFree(s->amps); s->amps = nullptr; }
     if (s->partials) { cudaFree(s->partials); s->partials = nullptr; }
     s->n = n;
-    CK(cudaMalloc(&s->amps, sizeof(double2) << n));
+    CK(cudaMalloc(&s->amps, (s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2)) << n));
     s->partials_cap = partials_needed(n);
     CK(cudaMalloc(&s->partials, s->partials_cap * sizeof(double)));
     return QOA_OK;
@@ -487,7 +502,15 @@ struct Step {
 // diagonally (controls, phases). Non-diagonal targets must be in the tile:
 // qubits 0..4 always are; up to HIGH_SLOTS higher qubits are claimed in the
 // order gates ask for them.
-std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate) {
+// FP32 passes fuse gates into dense blocks, so a non-diagonal gate needs all
+// of its qubits (controls included) in the tile, and SWAP / U2 can join too.
+bool is_pass_gate_f32(const Gate& g) { return g.kind <= K_U2; }
+uint64_t tile_need(const Gate& g, bool f32) {
+    if (!f32) return g.nmask;
+    return g.kind == K_DIAG ? 0 : (g.nmask | g.dmask);
+}
+
+std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false) {
     std::vector<Step> steps;
     const size_t N = G.size();
     std::vector<char> done(N, 0);
@@ -497,7 +520,7 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
         while (first < N && done[first]) ++first;
         if (first >= N) break;
         const Gate& g0 = G[first];
-        if (!tiles || !is_pass_gate(g0)) {
+        if (!tiles || !(f32 ? is_pass_gate_f32(g0) : is_pass_gate(g0))) {
             Step st;
             st.gates.push_back((int)first);
             done[first] = 1;
@@ -515,9 +538,9 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
             if (done[i]) continue;
             const Gate& g = G[i];
             if (is_barrier(g)) break;
-            bool ok = is_pass_gate(g) && !(g.nmask & (bN | bD)) && !(g.dmask & bN);
+            bool ok = (f32 ? is_pass_gate_f32(g) : is_pass_gate(g)) && !(g.nmask & (bN | bD)) && !(g.dmask & bN);
             if (ok) {
-                const uint64_t need = g.nmask & ~tile;
+                const uint64_t need = tile_need(g, f32) & ~tile;
                 const int k = __builtin_popcountll(need);
                 const int nc = g.kind == K_G1 ? 4 : 2;  // a selector diagonal becomes two phase ops
                 if (nslots + k > HIGH_SLOTS || budget_ops < 1 || budget_coef < nc) ok = false;
@@ -889,6 +912,242 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     return 0;
 }
 
+// ------------------------------------------------------- FP32 fused passes
+using cplx = std::complex<double>;
+
+// The exact 2x2 of a K_G1 gate (the forms of Expander).
+void g1_exact(const Gate& g, cplx (&m)[4]) {
+    switch (g.sub) {
+        case G1_H: {
+            const double f = g.m[0].x;
+            m[0] = f; m[1] = f; m[2] = f; m[3] = -f;
+            break;
+        }
+        case G1_X: m[0] = 0; m[1] = 1; m[2] = 1; m[3] = 0; break;
+        case G1_Y: m[0] = 0; m[1] = cplx(0, -1); m[2] = cplx(0, 1); m[3] = 0; break;
+        case G1_RX: {
+            const double c = g.m[0].x, sn = g.m[0].y;
+            m[0] = c; m[1] = cplx(0, -sn); m[2] = cplx(0, -sn); m[3] = c;
+            break;
+        }
+        case G1_RY: {
+            const double c = g.m[0].x, sn = g.m[0].y;
+            m[0] = c; m[1] = -sn; m[2] = sn; m[3] = c;
+            break;
+        }
+        default:
+            for (int k = 0; k < 4; ++k) m[k] = cplx(g.m[k].x, g.m[k].y);
+    }
+}
+
+// Applies gate g to a vector over the 5-qubit block space whose bit i is the
+// block's i-th qubit bq[i] (global qubit indices).
+void block_apply(const Gate& g, const int* bq, cplx* v) {
+    auto bit = [&](int q) -> uint32_t {
+        for (int i = 0; i < 5; ++i)
+            if (bq[i] == q) return 1u << i;
+        return 0;
+    };
+    auto bmask = [&](uint64_t m) -> uint32_t {
+        uint32_t r = 0;
+        for (int q = 0; q < 64; ++q)
+            if ((m >> q) & 1) r |= bit(q);
+        return r;
+    };
+    const uint32_t cm = bmask(g.cmask);
+    if (g.kind == K_G1) {
+        cplx m[4];
+        g1_exact(g, m);
+        const uint32_t tb = bit(g.t);
+        for (uint32_t r = 0; r < 32; ++r) {
+            if ((r & tb) || (r & cm) != cm) continue;
+            const cplx a0 = v[r], a1 = v[r | tb];
+            v[r] = m[0] * a0 + m[1] * a1;
+            v[r | tb] = m[2] * a0 + m[3] * a1;
+        }
+    } else if (g.kind == K_DIAG) {
+        const uint32_t sb = g.t >= 0 ? bit(g.t) : 0;
+        for (uint32_t r = 0; r < 32; ++r) {
+            if ((r & cm) != cm) continue;
+            if (g.neg) v[r] = -v[r];
+            else v[r] *= (sb && (r & sb)) ? cplx(g.m[1].x, g.m[1].y) : cplx(g.m[0].x, g.m[0].y);
+        }
+    } else if (g.kind == K_SWAP) {
+        const uint32_t b1 = bit(g.t), b2 = bit(g.t2);
+        for (uint32_t r = 0; r < 32; ++r) {
+            if ((r & (b1 | b2)) || (r & cm) != cm) continue;
+            std::swap(v[r | b2], v[r | b1]);
+        }
+    } else if (g.kind == K_U2) {
+        const uint32_t bl = bit(g.t), bh = bit(g.t2);
+        for (uint32_t r = 0; r < 32; ++r) {
+            if (r & (bl | bh)) continue;
+            const uint32_t idx[4] = {r, r | bl, r | bh, r | bl | bh};
+            cplx x[4], y[4];
+            for (int k = 0; k < 4; ++k) x[k] = v[idx[k]];
+            for (int row = 0; row < 4; ++row) {
+                y[row] = 0;
+                for (int k = 0; k < 4; ++k) y[row] += cplx(g.m[4 * row + k].x, g.m[4 * row + k].y) * x[k];
+            }
+            for (int k = 0; k < 4; ++k) v[idx[k]] = y[k];
+        }
+    }
+}
+
+uint64_t gate_qubits(const Gate& g) {
+    uint64_t m = g.nmask | g.dmask;
+    if (g.kind == K_DIAG && g.t >= 0) m |= 1ull << g.t;
+    return m;
+}
+
+// TF32 of x, rounded to nearest (ties away from zero), as mma consumes it.
+float tf32_round(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    if ((b & 0x7f800000u) != 0x7f800000u) {
+        b += 0x1000u;
+        b &= 0xffffe000u;
+    }
+    float r;
+    memcpy(&r, &b, 4);
+    return r;
+}
+
+// Fuses a pass's gates into dense blocks of <= 5 tile qubits (FP64 unitaries,
+// rounded for the tensor cores) and phase groups.
+int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32PassParams& P,
+                   std::vector<float>& mats, std::vector<F32Phase>& phases) {
+    memset(&P, 0, sizeof P);
+    P.n = n;
+    int slot_of[64];
+    for (int q = 0; q < 64; ++q) slot_of[q] = -1;
+    for (int s = 0; s < HIGH_SLOTS; ++s) {
+        P.slot_qubit[s] = (uint8_t)st.slots[s];
+        slot_of[st.slots[s]] = s;
+    }
+    int no = 0;
+    for (uint32_t q = LANE_BITS; q < n; ++q)
+        if (slot_of[q] < 0) P.outer_qubits[no++] = (uint8_t)q;
+    uint64_t tile = 0x1Full;
+    for (int s = 0; s < HIGH_SLOTS; ++s) tile |= 1ull << st.slots[s];
+    auto tbit = [&](int q) -> int { return q < LANE_BITS ? q : LANE_BITS + slot_of[q]; };
+
+    int nops = 0;
+    uint64_t B = 0;                 // qubits of the open block
+    std::vector<const Gate*> blk;   // its gates, in order
+    std::vector<const Gate*> pend;  // deferred diagonal gates
+    uint64_t pend_q = 0;
+
+    auto close_block = [&]() -> bool {
+        if (blk.empty()) return true;
+        if (nops >= MAX_F32_OPS) return false;
+        // block qubits: B padded to 5 with other tile qubits, ascending tile bit
+        std::vector<std::pair<int, int>> bq;
+        for (int q = 0; q < 64; ++q)
+            if ((B >> q) & 1) bq.push_back({tbit(q), q});
+        for (int q = 0; q < 64 && bq.size() < 5; ++q)
+            if (((tile >> q) & 1) && !((B >> q) & 1)) bq.push_back({tbit(q), q});
+        std::sort(bq.begin(), bq.end());
+        int qs[5];
+        uint32_t bm = 0;
+        for (int i = 0; i < 5; ++i) { qs[i] = bq[i].second; bm |= 1u << bq[i].first; }
+        cplx U[32][32];
+        for (int c = 0; c < 32; ++c) {
+            cplx v[32];
+            for (int r = 0; r < 32; ++r) v[r] = (r == c) ? 1.0 : 0.0;
+            for (const Gate* g : blk) block_apply(*g, qs, v);
+            for (int r = 0; r < 32; ++r) U[r][c] = v[r];
+        }
+        // real embedding [[Ur, -Ui], [Ui, Ur]], split into TF32 hi / lo
+        const size_t base = mats.size();
+        mats.resize(base + 8192);
+        for (int r = 0; r < 64; ++r)
+            for (int c = 0; c < 64; ++c) {
+                const cplx u = U[r & 31][c & 31];
+                double x;
+                if (r < 32) x = (c < 32) ? u.real() : -u.imag();
+                else x = (c < 32) ? u.imag() : u.real();
+                const float h = tf32_round((float)x);
+                const float l = tf32_round((float)(x - (double)h));
+                mats[base + r * 64 + c] = h;
+                mats[base + 4096 + r * 64 + c] = l;
+            }
+        F32Op& op = P.ops[nops++];
+        op.kind = 0;
+        op.bmask = bm;
+        op.index = (uint32_t)(base / 8192);
+        blk.clear();
+        B = 0;
+        return true;
+    };
+    // one phase entry per factor: d where every bit of `mask` is set
+    auto phase_entry = [&](uint64_t mask, cplx d, std::vector<F32Phase>& one, std::vector<F32Phase>& multi) {
+        F32Phase e;
+        memset(&e, 0, sizeof e);
+        for (int q = 0; q < 64; ++q) {
+            if (!((mask >> q) & 1)) continue;
+            if ((tile >> q) & 1) e.tile |= 1u << tbit(q);
+            else e.outer |= 1ull << q;
+        }
+        e.re = d.real();
+        e.im = d.imag();
+        (__builtin_popcount(e.tile) <= 1 ? one : multi).push_back(e);
+    };
+    auto flush_pend = [&]() -> bool {
+        if (pend.empty()) return true;
+        std::vector<F32Phase> one, multi;
+        for (const Gate* g : pend) {
+            if (g->neg) phase_entry(g->cmask, -1.0, one, multi);
+            else if (g->t < 0) phase_entry(g->cmask, cplx(g->m[0].x, g->m[0].y), one, multi);
+            else {
+                const cplx d0(g->m[0].x, g->m[0].y), d1(g->m[1].x, g->m[1].y);
+                phase_entry(g->cmask, d0, one, multi);
+                phase_entry(g->cmask | (1ull << g->t), d1 / d0, one, multi);
+            }
+        }
+        for (int k = 0; k < 2; ++k) {
+            std::vector<F32Phase>& list = k == 0 ? one : multi;
+            if (list.empty()) continue;
+            if (nops >= MAX_F32_OPS) return false;
+            F32Op& op = P.ops[nops++];
+            op.kind = (uint32_t)(k + 1);
+            op.index = (uint32_t)phases.size();
+            op.count = (uint32_t)list.size();
+            phases.insert(phases.end(), list.begin(), list.end());
+        }
+        pend.clear();
+        pend_q = 0;
+        return true;
+    };
+
+    for (int gi : st.gates) {
+        const Gate& g = G[gi];
+        const uint64_t Q = gate_qubits(g);
+        if (g.kind == K_DIAG) {
+            if (!blk.empty() && (Q & ~tile) == 0 && __builtin_popcountll(B | Q) <= 5) {
+                blk.push_back(&g);
+                B |= Q;
+            } else {
+                pend.push_back(&g);
+                pend_q |= Q;
+            }
+            continue;
+        }
+        // non-diagonal: every qubit is a tile qubit (the scheduler claimed them)
+        if (pend_q & g.nmask) {
+            if (!close_block() || !flush_pend()) return -1;
+        }
+        if (__builtin_popcountll(B | Q) > 5) {
+            if (!close_block()) return -1;
+        }
+        blk.push_back(&g);
+        B |= Q;
+    }
+    if (!close_block() || !flush_pend()) return -1;
+    P.nops = (uint32_t)nops;
+    return 0;
+}
+
 // ------------------------------------------------------------- execution
 GGate to_ggate(const Gate& g) {
     GGate k;
@@ -952,6 +1211,12 @@ int read_p01(qoa_state_t s, uint32_t q, double& p0, double& p1, double& norm2) {
 }
 
 int do_reset_all(qoa_state_t s) {
+    if (s->precision == QOA_PREC_F32) {
+        CK(launch_f32_reset((float2*)s->amps, state_len(s), s->stream));
+        CK(launch_set_scalar(s->scal, 1.0, s->stream));
+        s->launches += 2;
+        return QOA_OK;
+    }
     GGate k;
     memset(&k, 0, sizeof k);
     k.kind = GG_RESET_ALL;
@@ -1006,7 +1271,56 @@ double next_meas_uniform(qoa_state_t s) {
     return uniform01(s->seed, s->noise_stream ^ kMeasStreamXor, s->meas_draws++, 0);
 }
 
+// FP32 precision form: every step must be a fused pass; all passes of the op
+// list are built first and their block matrices and phases uploaded at once.
+int execute_f32(qoa_state_t s, std::vector<Gate>& G) {
+    for (const Gate& g : G)
+        if (g.kind > K_U2)
+            return set_err(s, QOA_E_OPCODE, "the FP32 precision form takes unitary ops only");
+    if (s->n < (uint32_t)TILE_BITS) return set_err(s, QOA_E_ARG, "the FP32 precision form needs n >= %d", TILE_BITS);
+    std::vector<Step> steps = schedule(G, s->n, false, true);
+    std::vector<F32PassParams> passes(steps.size());
+    std::vector<float> mats;
+    std::vector<F32Phase> phases;
+    for (size_t i = 0; i < steps.size(); ++i) {
+        if (!steps[i].pass) return set_err(s, QOA_E_OPCODE, "gate outside an FP32 pass");
+        if (build_f32_pass(G, steps[i], s->n, passes[i], mats, phases) != 0)
+            return set_err(s, QOA_E_ARG, "FP32 pass %zu does not fit one launch", i);
+    }
+    if (mats.size() > s->f32_mats_cap) {
+        CK(cudaStreamSynchronize(s->stream));
+        if (s->f32_mats) cudaFree(s->f32_mats);
+        s->f32_mats = nullptr;
+        CK(cudaMalloc(&s->f32_mats, mats.size() * sizeof(float)));
+        s->f32_mats_cap = mats.size();
+    }
+    if (phases.size() > s->f32_phases_cap) {
+        CK(cudaStreamSynchronize(s->stream));
+        if (s->f32_phases) cudaFree(s->f32_phases);
+        s->f32_phases = nullptr;
+        CK(cudaMalloc(&s->f32_phases, phases.size() * sizeof(F32Phase)));
+        s->f32_phases_cap = phases.size();
+    }
+    if (!mats.empty())
+        CK(cudaMemcpyAsync(s->f32_mats, mats.data(), mats.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    if (!phases.empty())
+        CK(cudaMemcpyAsync(s->f32_phases, phases.data(), phases.size() * sizeof(F32Phase), cudaMemcpyHostToDevice,
+                           s->stream));
+    for (const F32PassParams& P : passes) {
+        {
+            Timer tm(s, 2.0 * std::ldexp(8.0, (int)s->n), 2);
+            CK(launch_f32_pass((float2*)s->amps, P, s->f32_mats, s->f32_phases, s->scal, s->partials, s->stream));
+        }
+        CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
+        s->launches += 2;
+    }
+    // the vectors above live until the copies are done
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
 int execute(qoa_state_t s, std::vector<Gate>& G) {
+    if (s->precision == QOA_PREC_F32) return execute_f32(s, G);
     const bool per_gate = (s->flags & QOA_FLAG_PER_GATE) != 0;
     // Split at QINIT (changes n) and run each segment through the scheduler.
     size_t i = 0;
@@ -1146,13 +1460,17 @@ int qoa_create(uint32_t n, int precision, uint32_t flags, qoa_state_t* out) {
     qoa_state_t s = nullptr;
     if (!out) return set_err(nullptr, QOA_E_ARG, "null out");
     *out = nullptr;
-    if (precision != QOA_PREC_F64) return set_err(nullptr, QOA_E_ARG, "unsupported precision %d", precision);
+    if (precision != QOA_PREC_F64 && precision != QOA_PREC_F32)
+        return set_err(nullptr, QOA_E_ARG, "unsupported precision %d", precision);
+    if (precision == QOA_PREC_F32 && n < (uint32_t)TILE_BITS)
+        return set_err(nullptr, QOA_E_ARG, "the FP32 precision form needs n >= %d", TILE_BITS);
     if (n < 1) n = 1;
     if (n > 40) return set_err(nullptr, QOA_E_ARG, "n=%u qubits exceeds the engine limit", n);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(nullptr, QOA_E_NOGPU, "no CUDA device");
     s = new qoa_state_s();
     s->flags = flags;
+    s->precision = precision;
     cudaGetDevice(&s->device);
     auto fail = [&](int rc) {
         std::string m = s->err;
@@ -1181,6 +1499,8 @@ int qoa_destroy(qoa_state_t s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& r : s->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     if (s->amps) cudaFree(s->amps);
+    if (s->f32_mats) cudaFree(s->f32_mats);
+    if (s->f32_phases) cudaFree(s->f32_phases);
     if (s->partials) cudaFree(s->partials);
     if (s->scal) cudaFree(s->scal);
     if (s->status) cudaFree(s->status);
@@ -1224,6 +1544,7 @@ int qoa_apply(qoa_state_t s, const qoa_op* ops, size_t nops) {
 int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome) {
     int rc = check_handle(s);
     if (rc) return rc;
+    if (s->precision == QOA_PREC_F32) return set_err(s, QOA_E_ARG, "not available for an FP32 handle");
     if (q >= s->n) return set_err(s, QOA_E_RANGE, "qubit index %u out of bounds", q);
     if (u < 0) u = next_meas_uniform(s);
     rc = do_measure(s, q, u, outcome);
@@ -1238,6 +1559,7 @@ int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome) {
 int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t* out) {
     int rc = check_handle(s);
     if (rc) return rc;
+    if (s->precision == QOA_PREC_F32) return set_err(s, QOA_E_ARG, "not available for an FP32 handle");
     if (!u || !out || (mode != 0 && mode != 1)) return set_err(s, QOA_E_ARG, "bad sample arguments");
     if (shots == 0) return QOA_OK;
     const uint32_t n = s->n;
@@ -1271,7 +1593,10 @@ int qoa_probabilities(qoa_state_t s, double* out) {
     CK(cudaMallocAsync(&d, chunk * sizeof(double), s->stream));
     for (uint64_t off = 0; off < len; off += chunk) {
         const uint64_t cnt = std::min(chunk, len - off);
-        CK(launch_probs(s->amps, off, cnt, s->scal, d, s->stream));
+        if (s->precision == QOA_PREC_F32)
+            CK(launch_f32_probs((const float2*)s->amps, off, cnt, s->scal, d, s->stream));
+        else
+            CK(launch_probs(s->amps, off, cnt, s->scal, d, s->stream));
         s->launches++;
         CK(cudaMemcpyAsync(out + off, d, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     }
@@ -1283,6 +1608,7 @@ int qoa_probabilities(qoa_state_t s, double* out) {
 int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out) {
     int rc = check_handle(s);
     if (rc) return rc;
+    if (s->precision == QOA_PREC_F32) return set_err(s, QOA_E_ARG, "not available for an FP32 handle");
     if ((!masks || !out) && k) return set_err(s, QOA_E_ARG, "null argument");
     for (size_t i = 0; i < k; i += 8) {
         const uint32_t kk = (uint32_t)std::min<size_t>(8, k - i);
@@ -1298,9 +1624,13 @@ int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out) {
 int qoa_get_state(qoa_state_t s, void* host, size_t bytes) {
     int rc = check_handle(s);
     if (rc) return rc;
-    if (!host || bytes != state_len(s) * sizeof(double2))
-        return set_err(s, QOA_E_ARG, "get_state needs %llu bytes", (unsigned long long)(state_len(s) * sizeof(double2)));
-    CK(launch_materialize(s->amps, state_len(s), s->scal, s->partials, s->status, s->stream));
+    const size_t esz = s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2);
+    if (!host || bytes != state_len(s) * esz)
+        return set_err(s, QOA_E_ARG, "get_state needs %llu bytes", (unsigned long long)(state_len(s) * esz));
+    if (s->precision == QOA_PREC_F32)
+        CK(launch_f32_materialize((float2*)s->amps, state_len(s), s->scal, s->partials, s->status, s->stream));
+    else
+        CK(launch_materialize(s->amps, state_len(s), s->scal, s->partials, s->status, s->stream));
     s->launches += 2;
     CK(cudaMemcpyAsync(host, s->amps, bytes, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -1310,10 +1640,14 @@ int qoa_get_state(qoa_state_t s, void* host, size_t bytes) {
 int qoa_set_state(qoa_state_t s, const void* host, size_t bytes) {
     int rc = check_handle(s);
     if (rc) return rc;
-    if (!host || bytes != state_len(s) * sizeof(double2))
-        return set_err(s, QOA_E_ARG, "set_state needs %llu bytes", (unsigned long long)(state_len(s) * sizeof(double2)));
+    const size_t esz = s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2);
+    if (!host || bytes != state_len(s) * esz)
+        return set_err(s, QOA_E_ARG, "set_state needs %llu bytes", (unsigned long long)(state_len(s) * esz));
     CK(cudaMemcpyAsync(s->amps, host, bytes, cudaMemcpyHostToDevice, s->stream));
-    CK(launch_norm(s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
+    if (s->precision == QOA_PREC_F32)
+        CK(launch_f32_norm((const float2*)s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
+    else
+        CK(launch_norm(s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
     s->launches += 2;
     // set_state_vector normalises at once (quantum_state.rs:1143): a zero or
     // NaN vector becomes |0..0> before any gate sees it.

@@ -112,6 +112,35 @@ struct PassParams {
 };
 
 // ---------------------------------------------------------------------------
+// FP32-fused precision passes (qoa_f32.cu)
+// ---------------------------------------------------------------------------
+constexpr int MAX_F32_OPS = 256;
+
+struct F32Op {
+    uint32_t kind;   // 0 = dense block, 1 = phases with <= 1 tile bit, 2 = phases with >= 2 tile bits
+    uint32_t bmask;  // kind 0: the 5 tile bits the block acts on
+    uint32_t index;  // kind 0: matrix index; kind 1/2: first phase entry
+    uint32_t count;  // kind 1/2: number of phase entries
+};
+
+// Multiply by (re, im) where the global index has every bit of `outer` and
+// the tile index every bit of `tile`.
+struct F32Phase {
+    uint64_t outer;
+    uint32_t tile;
+    uint32_t pad_;
+    double re, im;
+};
+
+struct F32PassParams {
+    uint32_t n;
+    uint32_t nops;
+    uint8_t slot_qubit[HIGH_SLOTS];
+    uint8_t outer_qubits[64];
+    F32Op ops[MAX_F32_OPS];
+};
+
+// ---------------------------------------------------------------------------
 // Per-gate kernels over global memory (fallback / per-gate mode / shims).
 // ---------------------------------------------------------------------------
 enum GGKind : uint8_t {

@@ -1,0 +1,86 @@
+"""FP32-fused precision form: complex64 state, gates fused on the host into
+dense blocks of up to 5 qubits applied on the tensor cores (3xTF32, FP32
+accumulation). Checked against the FP64 oracle (relative L2 and infidelity)
+and, for the QFT, against sqrt(N) * IDFT."""
+import math
+
+import numpy as np
+import pytest
+
+import qoa_b200 as qb
+from qoa_b200 import circuits as C
+from oracle import pyoracle as po
+from tests.test_plan import mixed_circuit
+
+F32_REL_L2 = 1e-5      # FP32 arithmetic over a few fused passes
+F32_INFIDELITY = 1e-6  # 1 - |<psi_ref|psi>|^2
+
+
+def fidelity_err(a, b):
+    a = a.astype(np.complex128) / np.linalg.norm(a)
+    b = b.astype(np.complex128) / np.linalg.norm(b)
+    return 1.0 - abs(np.vdot(b, a)) ** 2
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a.astype(np.complex128) - b) / np.linalg.norm(b))
+
+
+def f32_run(n, ops, init=None):
+    with qb.QuantumState(n, precision="f32") as st:
+        if init is not None:
+            st.set_state_vector(init.astype(np.complex64))
+        st.execute(C.ops_to_array(ops))
+        return st.get_state_vector()
+
+
+def oracle_run(n, ops, init=None):
+    po.set_fast(True)
+    o = po.OracleState(n, 0)
+    if init is not None:
+        o.set_state(init)
+    o.apply(C.ops_to_array(ops))
+    return o.state()
+
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    return v / np.linalg.norm(v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [11, 12, 14, 17])
+def test_f32_layered_matches_oracle(n):
+    ops = C.random_layered(n, 6, 300 + n, initial_h=True)
+    got, ref = f32_run(n, ops), oracle_run(n, ops)
+    assert got.dtype == np.complex64
+    assert rel_l2(got, ref) < F32_REL_L2
+    assert fidelity_err(got, ref) < F32_INFIDELITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [12, 15])
+def test_f32_mixed_gate_kinds(n):
+    ops = mixed_circuit(n, 150, 11 * n)
+    got, ref = f32_run(n, ops), oracle_run(n, ops)
+    assert rel_l2(got, ref) < F32_REL_L2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [11, 14, 18])
+def test_f32_qft_matches_inverse_dft(n):
+    init = random_state(n, 4)
+    got = f32_run(n, C.qft(n), init=init)
+    ref = np.fft.ifft(init) * math.sqrt(1 << n)
+    assert rel_l2(got, ref) < F32_REL_L2
+    assert fidelity_err(got, ref) < F32_INFIDELITY
+
+
+@pytest.mark.gpu
+def test_f32_rejects_non_unitary_ops_and_small_n():
+    with pytest.raises(qb.QoaError):
+        qb.QuantumState(8, precision="f32")
+    with qb.QuantumState(12, precision="f32") as st:
+        with pytest.raises(qb.QoaError):
+            st.execute(C.ops_to_array([C.Op(C.MEASURE, [0])]))
