@@ -323,6 +323,75 @@ def run_ours(args):
     return 0
 
 
+def run_qft(args):
+    """Precision form: QFT (H + CPHASE(pi/2^k) ladder + swap network) on a seeded
+    Gaussian state. FP32-fused (complex64, <=5-qubit blocks on the tensor cores)
+    at n = args.qft_qubits for throughput; FP64 plain and FP32-fused both at
+    n - 1 for gates/s side by side and for relative L2 / 1 - F between them."""
+    import torch
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+
+    n = args.qft_qubits
+    dev = torch.device("cuda", 0)
+
+    def timed(st, ops, steps, warmup, kind):
+        stream = torch.cuda.ExternalStream(st.stream_ptr(), device=dev)
+        for _ in range(warmup):
+            st.execute(ops)
+        st.sync()
+        st.launch_times()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            st.execute(ops)
+        e1.record(stream)
+        st.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        lm, lb, lk = st.launch_times()
+        sel = lk == kind
+        passes = int(sel.sum() // steps)
+        bw = float(lb[sel].sum() / (lm[sel].sum() / 1e3) / 1e9) if sel.any() else None
+        return ms, passes, bw, float(lm[sel].mean()) if sel.any() else None
+
+    out = {"metric": "QFT gates/s, FP32-fused vs FP64 plain", "unit": "gates/s", "impl": "qoa_b200",
+           "data": "synthetic (seeded Gaussian input state)", "higher_is_better": True, "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup}
+    ops_n = C.ops_to_array(C.qft(n))
+    with qb.QuantumState(n, precision="f32", profile=True) as st:
+        st.set_random_state(2)
+        ms, passes, bw, avg = timed(st, ops_n, args.steps, args.warmup, 2)
+    peak, src = measured_peaks()
+    out.update(value=len(ops_n) / (ms / 1e3), dtype="complex64 (3xTF32 tensor cores, FP32 accumulate)",
+               config={"workload": f"QFT n={n}", "gates": len(ops_n), "state_bytes": 8 << n},
+               ms_per_step=ms, fp32_passes=passes,
+               roofline={"bound": "hbm", "achieved": bw, "peak": peak, "unit": "GB/s",
+                         "frac": bw / peak if bw else None, "kernel": "k_f32_pass", "avg_launch_ms": avg,
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})"})
+    m = n - 1
+    ops_m = C.ops_to_array(C.qft(m))
+    with qb.QuantumState(m, profile=True) as s64:
+        s64.set_random_state(2)
+        ms64, p64, bw64, _ = timed(s64, ops_m, args.steps, args.warmup, 0)
+    with qb.QuantumState(m, precision="f32", profile=True) as s32:
+        s32.set_random_state(2)
+        ms32, p32, bw32, _ = timed(s32, ops_m, args.steps, args.warmup, 2)
+    # accuracy: one QFT from the same input on both precisions
+    with qb.QuantumState(m) as a, qb.QuantumState(m, precision="f32") as b:
+        a.set_random_state(2)
+        b.set_random_state(2)
+        a.execute(ops_m)
+        b.execute(ops_m)
+        rel, infid = b.compare(a)
+    out.update(at_n_minus_1={"n": m, "fp64_gates_s": len(ops_m) / (ms64 / 1e3),
+                             "fp32_gates_s": len(ops_m) / (ms32 / 1e3), "fp32_over_fp64": ms64 / ms32,
+                             "fp64_ms": ms64, "fp32_ms": ms32, "fp64_pass_launches": p64, "fp32_passes": p32,
+                             "fp32_rel_l2_vs_fp64": rel, "fp32_infidelity_vs_fp64": infid})
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,7 +406,11 @@ def main():
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
     ap.add_argument("--depth", type=int, default=20)
+    ap.add_argument("--workload", default="layered", choices=["layered", "qft"])
+    ap.add_argument("--qft-qubits", type=int, default=33)
     args = ap.parse_args()
+    if args.workload == "qft":
+        return run_qft(args)
     if (args.qubits, args.depth) != (30, 20):
         set_workload(args.qubits, args.depth)
     if args.impl == "reference":

@@ -173,6 +173,13 @@ int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out);
  * for a QOA_PREC_F32 handle. */
 int qoa_get_state(qoa_state_t s, void* host, size_t bytes);
 int qoa_set_state(qoa_state_t s, const void* host, size_t bytes);
+/* No reference counterpart: a seeded Gaussian state (re, im of every
+ * amplitude i.i.d. N(0,1), Philox4x32-10 + Box-Muller), normalised. Handles of
+ * either precision seeded alike hold the same state (complex64 = rounded). */
+int qoa_set_random_state(qoa_state_t s, uint64_t seed);
+/* No reference counterpart: relative L2 distance and 1 - |<a|b>|^2 of the
+ * normalised states of two handles of equal size (either precision). */
+int qoa_compare(qoa_state_t a, qoa_state_t b, double* rel_l2, double* infidelity);
 /* seed_rng (quantum_state.rs:956): seeds the handle's Philox4x32-10 stream. */
 int qoa_seed(qoa_state_t s, uint64_t seed);
 /* NoiseConfig (quantum_state.rs:15-24): mode 0 Ideal, 1 Fixed(p), 2 Random. */
@@ -193,6 +200,37 @@ int qoa_launch_count(qoa_state_t s, uint64_t* count);
 int qoa_launch_times(qoa_state_t s, double* ms, double* bytes, int* kind, size_t cap, size_t* n);
 const char* qoa_last_error(qoa_state_t s);
 const char* qoa_strerror(int code);
+
+/* ---- batching form (no reference counterpart) ---------------------------- */
+/* Many circuits run together: circuits of up to tune.small_max_n qubits (at
+ * most 12 for complex128, 13 for complex64) run whole-state in shared memory
+ * in one persistent launch; larger ones run as tile passes on views into one
+ * packed arena, spread over tune.streams streams. The first qoa_batch_run
+ * runs eagerly, then captures the whole batch into a CUDA graph; later runs
+ * replay it. Results: <Z_mask> of each circuit's final state for the masks
+ * given at qoa_batch_add, in order of addition. Unitary ops only. */
+typedef struct qoa_batch_s* qoa_batch_t;
+typedef struct qoa_batch_tuning {
+    uint32_t small_max_n;       /* shared-memory kernel up to this many qubits */
+    uint32_t small_threads;     /* threads per CTA of that kernel (multiple of 32) */
+    uint32_t small_ctas_per_sm; /* its persistent grid = SMs x this */
+    uint32_t streams;           /* streams the larger circuits spread over */
+    uint32_t pass_gate_budget;  /* max gates per tile pass (fusion width); 0 = default */
+} qoa_batch_tuning;
+int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out);
+int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, const uint64_t* zmasks, size_t nmasks,
+                  uint32_t* id);
+int qoa_batch_set_tuning(qoa_batch_t b, const qoa_batch_tuning* t);
+int qoa_batch_get_tuning(qoa_batch_t b, qoa_batch_tuning* t);
+int qoa_batch_run(qoa_batch_t b);
+/* Replays the captured graph on the batch's stream without waiting. */
+int qoa_batch_launch(qoa_batch_t b);
+/* The stream the batch runs on (its graph launches and joins there). */
+int qoa_batch_stream(qoa_batch_t b, void** stream);
+int qoa_batch_results(qoa_batch_t b, double* out, size_t count);
+int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t* large, uint32_t* graph_ready);
+const char* qoa_batch_last_error(qoa_batch_t b);
+int qoa_batch_destroy(qoa_batch_t b);
 
 /* ---- plan introspection (host only, no GPU needed) ---------------------- */
 /* Runs the pass scheduler on an op list for an n-qubit state and writes, for

@@ -44,6 +44,15 @@ class QoaStatus(ctypes.Structure):
                 ("zero_norm_resets", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("small_max_n", ctypes.c_uint32), ("small_threads", ctypes.c_uint32),
+                ("small_ctas_per_sm", ctypes.c_uint32), ("streams", ctypes.c_uint32),
+                ("pass_gate_budget", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"qoa_b200: {LIB_PATH} is missing; build it with `make -C qoa_b200` "
@@ -65,6 +74,8 @@ def _load() -> ctypes.CDLL:
         "qoa_get_state": (i32, [vp, vp, sz]),
         "qoa_set_state": (i32, [vp, vp, sz]),
         "qoa_seed": (i32, [vp, u64]),
+        "qoa_set_random_state": (i32, [vp, u64]),
+        "qoa_compare": (i32, [vp, vp, P(dbl), P(dbl)]),
         "qoa_set_noise": (i32, [vp, i32, dbl]),
         "qoa_set_trajectory": (i32, [vp, u64]),
         "qoa_status": (i32, [vp, P(QoaStatus)]),
@@ -74,6 +85,17 @@ def _load() -> ctypes.CDLL:
         "qoa_launch_times": (i32, [vp, vp, vp, vp, sz, P(sz)]),
         "qoa_last_error": (ctypes.c_char_p, [vp]),
         "qoa_strerror": (ctypes.c_char_p, [i32]),
+        "qoa_batch_create": (i32, [i32, u32, P(vp)]),
+        "qoa_batch_add": (i32, [vp, u32, vp, sz, vp, sz, P(u32)]),
+        "qoa_batch_set_tuning": (i32, [vp, P(BatchTuning)]),
+        "qoa_batch_get_tuning": (i32, [vp, P(BatchTuning)]),
+        "qoa_batch_run": (i32, [vp]),
+        "qoa_batch_results": (i32, [vp, vp, sz]),
+        "qoa_batch_launch": (i32, [vp]),
+        "qoa_batch_stream": (i32, [vp, P(vp)]),
+        "qoa_batch_info": (i32, [vp, P(u32), P(u32), P(u32), P(u32)]),
+        "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
+        "qoa_batch_destroy": (i32, [vp]),
         "qoa_plan": (i32, [u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, P(sz), P(sz)]),
         "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
         "qoa_vec_apply_x": (i32, [vp, sz, sz]),
@@ -284,6 +306,16 @@ class QuantumState:
         a = np.ascontiguousarray(np.asarray(amps, dtype=self._dtype))
         _check(lib.qoa_set_state(self._h, _ptr(a), a.nbytes), self._h)
 
+    def set_random_state(self, seed: int):
+        """Seeded Gaussian state (re, im i.i.d. N(0,1)), normalised, made on the device."""
+        _check(lib.qoa_set_random_state(self._h, int(seed)), self._h)
+
+    def compare(self, other: "QuantumState"):
+        """(relative L2, 1 - fidelity) of the two normalised states."""
+        r, f = ctypes.c_double(), ctypes.c_double()
+        _check(lib.qoa_compare(self._h, other._h, ctypes.byref(r), ctypes.byref(f)), self._h)
+        return r.value, f.value
+
     def expect_z(self, masks: Iterable[int]) -> np.ndarray:
         m = np.ascontiguousarray(np.asarray(list(masks), dtype=np.uint64))
         out = np.empty(len(m), dtype=np.float64)
@@ -361,3 +393,92 @@ def vec_call(name: str, amps: np.ndarray, *args) -> int:
         raise TypeError("amps must be a C-contiguous complex128 array")
     f = getattr(lib, "qoa_vec_apply_" + name)
     return _check(f(_ptr(amps), amps.size, *args))
+
+
+class Batch:
+    """Many circuits run together (qoa_batch_*): each circuit starts in
+    |0..0>, applies its unitary op list and yields <Z_mask> of its final
+    normalised state for each mask given. Small circuits run whole-state in
+    shared memory in one persistent launch; larger ones run as tile passes on
+    views into one packed arena. The first run() captures the batch into a
+    CUDA graph that later runs replay."""
+
+    def __init__(self, precision: str = "f64", compat_mask_quirk: bool = False):
+        if precision not in ("f64", "f32"):
+            raise ValueError("precision must be 'f64' or 'f32'")
+        self.precision = precision
+        h = ctypes.c_void_p()
+        flags = QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0
+        rc = lib.qoa_batch_create(QOA_PREC_F32 if precision == "f32" else QOA_PREC_F64, flags, ctypes.byref(h))
+        if rc != QOA_OK:
+            raise QoaError(rc, (lib.qoa_last_error(None) or b"").decode())
+        self._h = h
+        self._nresults = 0
+        self._keep = []
+
+    def _check(self, rc: int):
+        if rc != QOA_OK:
+            raise QoaError(rc, (lib.qoa_batch_last_error(self._h) or b"").decode())
+
+    def add(self, n: int, ops, zmasks: Sequence[int]) -> int:
+        arr = ops if isinstance(ops, np.ndarray) else ops_to_array(ops)
+        arr = np.ascontiguousarray(arr)
+        m = np.ascontiguousarray(np.asarray(list(zmasks), dtype=np.uint64))
+        cid = ctypes.c_uint32()
+        self._check(lib.qoa_batch_add(self._h, n, _ptr(arr) if len(arr) else None, len(arr),
+                                      _ptr(m) if len(m) else None, len(m), ctypes.byref(cid)))
+        self._nresults += len(m)
+        return cid.value
+
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        self._check(lib.qoa_batch_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = BatchTuning()
+        self._check(lib.qoa_batch_get_tuning(self._h, ctypes.byref(t)))
+        for k, v in kw.items():
+            if not hasattr(t, k):
+                raise KeyError(k)
+            setattr(t, k, int(v))
+        self._check(lib.qoa_batch_set_tuning(self._h, ctypes.byref(t)))
+
+    def run(self):
+        self._check(lib.qoa_batch_run(self._h))
+
+    def launch(self):
+        """Replays the captured graph without waiting (after a first run())."""
+        self._check(lib.qoa_batch_launch(self._h))
+
+    def stream_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(lib.qoa_batch_stream(self._h, ctypes.byref(p)))
+        return p.value or 0
+
+    def results(self) -> np.ndarray:
+        out = np.zeros(self._nresults, dtype=np.float64)
+        self._check(lib.qoa_batch_results(self._h, _ptr(out) if len(out) else None, len(out)))
+        return out
+
+    def info(self) -> dict:
+        v = [ctypes.c_uint32() for _ in range(4)]
+        self._check(lib.qoa_batch_info(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("circuits", "small", "large", "graph_ready"), (x.value for x in v)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.qoa_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

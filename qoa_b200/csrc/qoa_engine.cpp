@@ -42,7 +42,8 @@ cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const dou
 cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st);
 cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
                           uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
-cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32Phase* phases,
+cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32PhaseOp* pops,
+                            const F32Angle* angles, const F32Phase* phases, const float2* tables,
                             const double* norm2_in, double* partials, cudaStream_t st);
 cudaError_t launch_f32_reset(float2* a, uint64_t len, cudaStream_t st);
 cudaError_t launch_f32_norm(const float2* a, uint64_t len, double* partials, double* out, uint32_t* status,
@@ -51,6 +52,14 @@ cudaError_t launch_f32_materialize(float2* a, uint64_t len, double* norm2, doubl
                                    cudaStream_t st);
 cudaError_t launch_f32_probs(const float2* a, uint64_t off, uint64_t cnt, const double* norm2, double* out,
                              cudaStream_t st);
+cudaError_t launch_random_state(void* a, bool f32, uint64_t len, uint64_t seed, cudaStream_t st);
+cudaError_t launch_f32_expz(const float2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
+                            double* out, const double* norm2, cudaStream_t st);
+cudaError_t launch_small_batch(bool f32, const SmallCircuit* circs, uint32_t count, const SmallOp* ops,
+                               const uint64_t* masks, double* out, unsigned int* counter, int max_n, int threads,
+                               int ctas_per_sm, cudaStream_t st);
+cudaError_t launch_compare(const void* a, bool af32, const void* b, bool bf32, uint64_t len, const double* na,
+                           const double* nb, double* partials, double* out3, cudaStream_t st);
 }  // namespace qoa
 
 using namespace qoa;
@@ -141,8 +150,12 @@ struct qoa_state_s {
     uint32_t n = 1;
     uint32_t flags = 0;
     int precision = QOA_PREC_F64;
-    float* f32_mats = nullptr;       // FP32 passes: block matrices (device)
+    void* f32_mats = nullptr;        // FP32 passes: upload arena (device bytes)
     size_t f32_mats_cap = 0;
+    std::vector<F32PassParams> f32_passes;  // prepared FP32 passes
+    size_t f32_off[5] = {0, 0, 0, 0, 0};    // arena sections: mats, pops, angles, phases, tables
+    bool view = false;               // batch view: amps / scal / status / partials / stream not owned
+    int pass_budget = 0;             // max gates per tile pass (0: the default)
     F32Phase* f32_phases = nullptr;  // FP32 passes: phase entries (device)
     size_t f32_phases_cap = 0;
     int device = 0;
@@ -510,7 +523,8 @@ uint64_t tile_need(const Gate& g, bool f32) {
     return g.kind == K_DIAG ? 0 : (g.nmask | g.dmask);
 }
 
-std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false) {
+std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false,
+                           int gate_budget = 0) {
     std::vector<Step> steps;
     const size_t N = G.size();
     std::vector<char> done(N, 0);
@@ -533,6 +547,7 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
         int nslots = 0;
         uint64_t bN = 0, bD = 0;  // qubits blocked by waiting gates (non-diagonal / diagonal action)
         int budget_ops = MAX_PASS_OPS / 3;  // room for the exchanges and flushes
+        if (gate_budget > 0 && gate_budget < budget_ops) budget_ops = gate_budget;
         int budget_coef = MAX_PASS_COEF - 8;
         for (size_t i = first; i < N; ++i) {
             if (done[i]) continue;
@@ -1015,8 +1030,16 @@ float tf32_round(float x) {
 
 // Fuses a pass's gates into dense blocks of <= 5 tile qubits (FP64 unitaries,
 // rounded for the tensor cores) and phase groups.
-int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32PassParams& P,
-                   std::vector<float>& mats, std::vector<F32Phase>& phases) {
+struct F32Upload {
+    std::vector<float> mats;
+    std::vector<F32PhaseOp> pops;
+    std::vector<F32Angle> angles;
+    std::vector<F32Phase> phases;
+    std::vector<float2> tables;
+};
+
+int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32PassParams& P, F32Upload& up) {
+    std::vector<float>& mats = up.mats;
     memset(&P, 0, sizeof P);
     P.n = n;
     int slot_of[64];
@@ -1080,41 +1103,72 @@ int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32Pa
         B = 0;
         return true;
     };
-    // one phase entry per factor: d where every bit of `mask` is set
-    auto phase_entry = [&](uint64_t mask, cplx d, std::vector<F32Phase>& one, std::vector<F32Phase>& multi) {
-        F32Phase e;
-        memset(&e, 0, sizeof e);
-        for (int q = 0; q < 64; ++q) {
-            if (!((mask >> q) & 1)) continue;
-            if ((tile >> q) & 1) e.tile |= 1u << tbit(q);
-            else e.outer |= 1ull << q;
-        }
-        e.re = d.real();
-        e.im = d.imag();
-        (__builtin_popcount(e.tile) <= 1 ? one : multi).push_back(e);
-    };
+    // pending diagonal gates -> one phase group: unit factors d = e^{i theta}
+    // where every bit of a mask is set, split by how they depend on the CTA
     auto flush_pend = [&]() -> bool {
         if (pend.empty()) return true;
-        std::vector<F32Phase> one, multi;
+        if (nops >= MAX_F32_OPS) return false;
+        std::vector<std::vector<F32Angle>> lists(TILE_BITS + 1);
+        std::vector<cplx> table;
+        std::vector<F32Phase> multi;
+        auto entry = [&](uint64_t mask, cplx d) {
+            uint32_t tl = 0;
+            uint64_t outer = 0;
+            for (int q = 0; q < 64; ++q) {
+                if (!((mask >> q) & 1)) continue;
+                if ((tile >> q) & 1) tl |= 1u << tbit(q);
+                else outer |= 1ull << q;
+            }
+            if (outer == 0) {  // the same in every CTA: into the tile table
+                if (table.empty()) table.assign(1u << TILE_BITS, cplx(1.0, 0.0));
+                for (uint32_t j = 0; j < (1u << TILE_BITS); ++j)
+                    if ((j & tl) == tl) table[j] *= d;
+            } else if (__builtin_popcount(tl) <= 1) {
+                const int t = tl ? __builtin_ctz(tl) : TILE_BITS;
+                lists[t].push_back(F32Angle{outer, std::atan2(d.imag(), d.real())});
+            } else {
+                F32Phase e;
+                memset(&e, 0, sizeof e);
+                e.outer = outer;
+                e.tile = tl;
+                e.re = d.real();
+                e.im = d.imag();
+                multi.push_back(e);
+            }
+        };
         for (const Gate* g : pend) {
-            if (g->neg) phase_entry(g->cmask, -1.0, one, multi);
-            else if (g->t < 0) phase_entry(g->cmask, cplx(g->m[0].x, g->m[0].y), one, multi);
+            if (g->neg) entry(g->cmask, -1.0);
+            else if (g->t < 0) entry(g->cmask, cplx(g->m[0].x, g->m[0].y));
             else {
                 const cplx d0(g->m[0].x, g->m[0].y), d1(g->m[1].x, g->m[1].y);
-                phase_entry(g->cmask, d0, one, multi);
-                phase_entry(g->cmask | (1ull << g->t), d1 / d0, one, multi);
+                entry(g->cmask, d0);
+                entry(g->cmask | (1ull << g->t), d1 / d0);
             }
         }
-        for (int k = 0; k < 2; ++k) {
-            std::vector<F32Phase>& list = k == 0 ? one : multi;
-            if (list.empty()) continue;
-            if (nops >= MAX_F32_OPS) return false;
-            F32Op& op = P.ops[nops++];
-            op.kind = (uint32_t)(k + 1);
-            op.index = (uint32_t)phases.size();
-            op.count = (uint32_t)list.size();
-            phases.insert(phases.end(), list.begin(), list.end());
+        F32PhaseOp po;
+        memset(&po, 0, sizeof po);
+        po.table = -1;
+        for (int t = 0; t <= TILE_BITS; ++t) {
+            po.bit_start[t] = (uint32_t)up.angles.size();
+            up.angles.insert(up.angles.end(), lists[t].begin(), lists[t].end());
         }
+        po.bit_start[TILE_BITS + 1] = (uint32_t)up.angles.size();
+        if (!table.empty()) {
+            po.table = (int32_t)(up.tables.size() >> TILE_BITS);
+            for (const cplx& c : table) {
+                float2 f;
+                f.x = (float)c.real();
+                f.y = (float)c.imag();
+                up.tables.push_back(f);
+            }
+        }
+        po.multi_start = (uint32_t)up.phases.size();
+        po.multi_count = (uint32_t)multi.size();
+        up.phases.insert(up.phases.end(), multi.begin(), multi.end());
+        F32Op& op = P.ops[nops++];
+        op.kind = 1;
+        op.index = (uint32_t)up.pops.size();
+        up.pops.push_back(po);
         pend.clear();
         pend_q = 0;
         return true;
@@ -1271,52 +1325,68 @@ double next_meas_uniform(qoa_state_t s) {
     return uniform01(s->seed, s->noise_stream ^ kMeasStreamXor, s->meas_draws++, 0);
 }
 
-// FP32 precision form: every step must be a fused pass; all passes of the op
-// list are built first and their block matrices and phases uploaded at once.
-int execute_f32(qoa_state_t s, std::vector<Gate>& G) {
+// FP32 precision form: every step must be a fused pass. Prepare builds all
+// passes of an op list and uploads their block matrices and phases at once
+// (synchronously); launch only enqueues kernels, so it can be captured.
+int f32_prepare(qoa_state_t s, std::vector<Gate>& G) {
     for (const Gate& g : G)
         if (g.kind > K_U2)
             return set_err(s, QOA_E_OPCODE, "the FP32 precision form takes unitary ops only");
     if (s->n < (uint32_t)TILE_BITS) return set_err(s, QOA_E_ARG, "the FP32 precision form needs n >= %d", TILE_BITS);
-    std::vector<Step> steps = schedule(G, s->n, false, true);
-    std::vector<F32PassParams> passes(steps.size());
-    std::vector<float> mats;
-    std::vector<F32Phase> phases;
+    std::vector<Step> steps = schedule(G, s->n, false, true, s->pass_budget);
+    s->f32_passes.assign(steps.size(), F32PassParams());
+    F32Upload up;
     for (size_t i = 0; i < steps.size(); ++i) {
         if (!steps[i].pass) return set_err(s, QOA_E_OPCODE, "gate outside an FP32 pass");
-        if (build_f32_pass(G, steps[i], s->n, passes[i], mats, phases) != 0)
+        if (build_f32_pass(G, steps[i], s->n, s->f32_passes[i], up) != 0)
             return set_err(s, QOA_E_ARG, "FP32 pass %zu does not fit one launch", i);
     }
-    if (mats.size() > s->f32_mats_cap) {
-        CK(cudaStreamSynchronize(s->stream));
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t* o = s->f32_off;
+    o[0] = 0;
+    o[1] = al(o[0] + up.mats.size() * sizeof(float));
+    o[2] = al(o[1] + up.pops.size() * sizeof(F32PhaseOp));
+    o[3] = al(o[2] + up.angles.size() * sizeof(F32Angle));
+    o[4] = al(o[3] + up.phases.size() * sizeof(F32Phase));
+    const size_t total = al(o[4] + up.tables.size() * sizeof(float2)) + 256;
+    std::vector<unsigned char> host(total, 0);
+    auto put = [&](size_t off, const void* src, size_t bytes) { if (bytes) memcpy(host.data() + off, src, bytes); };
+    put(o[0], up.mats.data(), up.mats.size() * sizeof(float));
+    put(o[1], up.pops.data(), up.pops.size() * sizeof(F32PhaseOp));
+    put(o[2], up.angles.data(), up.angles.size() * sizeof(F32Angle));
+    put(o[3], up.phases.data(), up.phases.size() * sizeof(F32Phase));
+    put(o[4], up.tables.data(), up.tables.size() * sizeof(float2));
+    CK(cudaStreamSynchronize(s->stream));
+    if (total > s->f32_mats_cap) {
         if (s->f32_mats) cudaFree(s->f32_mats);
         s->f32_mats = nullptr;
-        CK(cudaMalloc(&s->f32_mats, mats.size() * sizeof(float)));
-        s->f32_mats_cap = mats.size();
+        CK(cudaMalloc(&s->f32_mats, total));
+        s->f32_mats_cap = total;
     }
-    if (phases.size() > s->f32_phases_cap) {
-        CK(cudaStreamSynchronize(s->stream));
-        if (s->f32_phases) cudaFree(s->f32_phases);
-        s->f32_phases = nullptr;
-        CK(cudaMalloc(&s->f32_phases, phases.size() * sizeof(F32Phase)));
-        s->f32_phases_cap = phases.size();
-    }
-    if (!mats.empty())
-        CK(cudaMemcpyAsync(s->f32_mats, mats.data(), mats.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    if (!phases.empty())
-        CK(cudaMemcpyAsync(s->f32_phases, phases.data(), phases.size() * sizeof(F32Phase), cudaMemcpyHostToDevice,
-                           s->stream));
-    for (const F32PassParams& P : passes) {
+    CK(cudaMemcpy(s->f32_mats, host.data(), total, cudaMemcpyHostToDevice));
+    return QOA_OK;
+}
+
+int f32_launch(qoa_state_t s) {
+    unsigned char* dev = (unsigned char*)s->f32_mats;
+    const size_t* o = s->f32_off;
+    for (const F32PassParams& P : s->f32_passes) {
         {
             Timer tm(s, 2.0 * std::ldexp(8.0, (int)s->n), 2);
-            CK(launch_f32_pass((float2*)s->amps, P, s->f32_mats, s->f32_phases, s->scal, s->partials, s->stream));
+            CK(launch_f32_pass((float2*)s->amps, P, (const float*)(dev + o[0]), (const F32PhaseOp*)(dev + o[1]),
+                               (const F32Angle*)(dev + o[2]), (const F32Phase*)(dev + o[3]),
+                               (const float2*)(dev + o[4]), s->scal, s->partials, s->stream));
         }
         CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
         s->launches += 2;
     }
-    // the vectors above live until the copies are done
-    CK(cudaStreamSynchronize(s->stream));
     return QOA_OK;
+}
+
+int execute_f32(qoa_state_t s, std::vector<Gate>& G) {
+    int rc = f32_prepare(s, G);
+    if (rc) return rc;
+    return f32_launch(s);
 }
 
 int execute(qoa_state_t s, std::vector<Gate>& G) {
@@ -1328,7 +1398,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         size_t j = i;
         while (j < G.size() && G[j].kind != K_QINIT) ++j;
         std::vector<Gate> seg(G.begin() + i, G.begin() + j);
-        std::vector<Step> steps = schedule(seg, s->n, per_gate);
+        std::vector<Step> steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
         for (const Step& st : steps) {
             int rc;
             if (st.pass) rc = run_pass(s, seg, st);
@@ -1433,6 +1503,241 @@ inline bool shim_bit_ok(size_t b) { return b < 64; }
 
 }  // namespace
 
+// ================================================================ batching
+// Many circuits in one go. Circuits small enough for a CTA's shared memory run
+// in one persistent launch (k_small_batch); the others run as tile passes on
+// views into one packed arena, spread over a pool of streams. The first run
+// captures all of it (small launch, every large circuit's reset / passes /
+// expectation values, fork and join over the streams) into a CUDA graph;
+// later runs replay the graph.
+struct qoa_batch_s {
+    int precision = QOA_PREC_F64;
+    uint32_t flags = 0;
+    int device = 0;
+    qoa_batch_tuning tune{};
+    struct Circ {
+        uint32_t n;
+        std::vector<Gate> gates;
+        std::vector<uint64_t> masks;
+        uint32_t out_start;
+        bool small;
+    };
+    std::vector<Circ> circs;
+    uint32_t nresults = 0;
+    bool prepared = false;
+    // device
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    void* arena = nullptr;
+    SmallCircuit* d_small = nullptr;
+    SmallOp* d_ops = nullptr;
+    uint64_t* d_masks = nullptr;
+    double* d_out = nullptr;
+    unsigned int* d_counter = nullptr;
+    uint32_t nsmall = 0;
+    uint32_t small_max_n_used = 0;
+    std::vector<qoa_state_t> views;       // per large circuit
+    std::vector<int> view_circ;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int bset_err(qoa_batch_t b, int code, const char* msg) {
+    if (b) b->err = msg;
+    note_global_error(msg);
+    return code;
+}
+
+#define BCK(call)                                                                   \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) return bset_err(b, QOA_E_CUDA, cudaGetErrorString(e_)); \
+    } while (0)
+
+bool small_ok(const Gate& g) { return g.kind == K_G1 || g.kind == K_DIAG || g.kind == K_SWAP; }
+
+SmallOp to_small(const Gate& g) {
+    SmallOp o;
+    memset(&o, 0, sizeof o);
+    o.cmask = (uint32_t)g.cmask;
+    if (g.kind == K_G1) {
+        o.kind = SK_G1;
+        o.t = (uint8_t)g.t;
+        cplx m[4];
+        g1_exact(g, m);
+        for (int k = 0; k < 4; ++k) o.m[k] = d2(m[k].real(), m[k].imag());
+    } else if (g.kind == K_DIAG) {
+        o.kind = SK_DIAG;
+        o.t = g.t >= 0 ? (uint8_t)g.t : 255;
+        if (g.neg) o.m[0] = o.m[1] = d2(-1, 0);
+        else {
+            o.m[0] = g.m[0];
+            o.m[1] = g.t >= 0 ? g.m[1] : g.m[0];
+        }
+    } else {
+        o.kind = SK_SWAP;
+        o.t = (uint8_t)g.t;
+        o.t2 = (uint8_t)g.t2;
+    }
+    return o;
+}
+
+void batch_free_device(qoa_batch_t b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    for (qoa_state_t v : b->views) qoa_destroy(v);
+    b->views.clear();
+    b->view_circ.clear();
+    for (void* p : {(void*)b->arena, (void*)b->d_small, (void*)b->d_ops, (void*)b->d_masks, (void*)b->d_out,
+                    (void*)b->d_counter})
+        if (p) cudaFree(p);
+    b->arena = nullptr; b->d_small = nullptr; b->d_ops = nullptr; b->d_masks = nullptr; b->d_out = nullptr;
+    b->d_counter = nullptr;
+    b->prepared = false;
+}
+
+int batch_prepare(qoa_batch_t b) {
+    const bool f32 = b->precision == QOA_PREC_F32;
+    const uint32_t cap = f32 ? SMALL_MAX_F32 : SMALL_MAX_F64;
+    const uint32_t smax = std::min<uint32_t>(b->tune.small_max_n, cap);
+    // small circuits
+    std::vector<SmallCircuit> sc;
+    std::vector<SmallOp> sops;
+    std::vector<uint64_t> masks;
+    uint32_t maxn = 1;
+    for (auto& c : b->circs) {
+        c.small = c.n <= smax || (f32 && c.n < (uint32_t)TILE_BITS);
+        for (const Gate& g : c.gates) c.small = c.small && small_ok(g);
+        if (!c.small && (c.n < (uint32_t)TILE_BITS && f32))
+            return bset_err(b, QOA_E_ARG, "circuit below the FP32 tile size with a gate the small kernel lacks");
+        if (!c.small) continue;
+        if (c.n > cap) return bset_err(b, QOA_E_ARG, "circuit too large for the shared-memory kernel");
+        SmallCircuit d;
+        d.n = c.n;
+        d.op_start = (uint32_t)sops.size();
+        for (const Gate& g : c.gates) sops.push_back(to_small(g));
+        d.op_count = (uint32_t)c.gates.size();
+        d.mask_start = (uint32_t)masks.size();
+        masks.insert(masks.end(), c.masks.begin(), c.masks.end());
+        d.mask_count = (uint32_t)c.masks.size();
+        d.out_start = c.out_start;
+        sc.push_back(d);
+        maxn = std::max(maxn, c.n);
+    }
+    b->nsmall = (uint32_t)sc.size();
+    b->small_max_n_used = maxn;
+    BCK(cudaMalloc(&b->d_out, std::max<size_t>(1, b->nresults) * sizeof(double)));
+    BCK(cudaMalloc(&b->d_counter, sizeof(unsigned int)));
+    if (!sc.empty()) {
+        BCK(cudaMalloc(&b->d_small, sc.size() * sizeof(SmallCircuit)));
+        BCK(cudaMalloc(&b->d_ops, std::max<size_t>(1, sops.size()) * sizeof(SmallOp)));
+        BCK(cudaMalloc(&b->d_masks, std::max<size_t>(1, masks.size()) * sizeof(uint64_t)));
+        BCK(cudaMemcpy(b->d_small, sc.data(), sc.size() * sizeof(SmallCircuit), cudaMemcpyHostToDevice));
+        if (!sops.empty()) BCK(cudaMemcpy(b->d_ops, sops.data(), sops.size() * sizeof(SmallOp), cudaMemcpyHostToDevice));
+        if (!masks.empty())
+            BCK(cudaMemcpy(b->d_masks, masks.data(), masks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    }
+    // streams
+    const uint32_t ns = std::max<uint32_t>(1, b->tune.streams);
+    while (b->streams.size() < ns) {
+        cudaStream_t st;
+        BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        b->streams.push_back(st);
+        cudaEvent_t ev;
+        BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->events.push_back(ev);
+    }
+    // arena for the large circuits: state, partials, scalars, status
+    const size_t esz = f32 ? sizeof(float2) : sizeof(double2);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t total = 0;
+    std::vector<size_t> off;
+    for (size_t i = 0; i < b->circs.size(); ++i) {
+        const auto& c = b->circs[i];
+        if (c.small) continue;
+        off.push_back(total);
+        total = al(total + (esz << c.n));
+        total = al(total + partials_needed(c.n) * sizeof(double));
+        total = al(total + 16 * sizeof(double));
+        total = al(total + 4 * sizeof(uint32_t));
+    }
+    if (total) BCK(cudaMalloc(&b->arena, total));
+    size_t k = 0;
+    for (size_t i = 0; i < b->circs.size(); ++i) {
+        auto& c = b->circs[i];
+        if (c.small) continue;
+        unsigned char* base = (unsigned char*)b->arena + off[k];
+        qoa_state_t v = new qoa_state_s();
+        v->view = true;
+        v->n = c.n;
+        v->flags = b->flags & QOA_FLAG_COMPAT_MASK_QUIRK;
+        v->precision = b->precision;
+        v->device = b->device;
+        v->pass_budget = (int)b->tune.pass_gate_budget;
+        v->stream = b->streams[k % ns];
+        size_t o = 0;
+        v->amps = (double2*)(base + o);
+        o = al(o + (esz << c.n));
+        v->partials = (double*)(base + o);
+        v->partials_cap = partials_needed(c.n);
+        o = al(o + v->partials_cap * sizeof(double));
+        v->scal = (double*)(base + o);
+        o = al(o + 16 * sizeof(double));
+        v->status = (uint32_t*)(base + o);
+        BCK(cudaMemset(v->status, 0, 4 * sizeof(uint32_t)));
+        if (f32) {
+            int rc = f32_prepare(v, c.gates);
+            if (rc) { std::string m = v->err; qoa_destroy(v); return bset_err(b, rc, m.c_str()); }
+        }
+        b->views.push_back(v);
+        b->view_circ.push_back((int)i);
+        ++k;
+    }
+    b->prepared = true;
+    return QOA_OK;
+}
+
+// Enqueues one full batch on stream 0 (forking to the pool and joining).
+int batch_enqueue(qoa_batch_t b) {
+    const bool f32 = b->precision == QOA_PREC_F32;
+    cudaStream_t s0 = b->streams[0];
+    const uint32_t ns = (uint32_t)b->streams.size();
+    BCK(cudaEventRecord(b->events[0], s0));
+    for (uint32_t i = 1; i < ns; ++i) BCK(cudaStreamWaitEvent(b->streams[i], b->events[0], 0));
+    for (size_t k = 0; k < b->views.size(); ++k) {
+        qoa_state_t v = b->views[k];
+        auto& c = b->circs[b->view_circ[k]];
+        int rc = do_reset_all(v);
+        if (!rc) rc = f32 ? f32_launch(v) : execute(v, c.gates);
+        if (rc) return bset_err(b, rc, v->err.c_str());
+        for (size_t m = 0; m < c.masks.size(); m += 8) {
+            const uint32_t kk = (uint32_t)std::min<size_t>(8, c.masks.size() - m);
+            cudaError_t e = f32 ? launch_f32_expz((const float2*)v->amps, state_len(v), c.masks.data() + m, kk,
+                                                  v->partials, b->d_out + c.out_start + m, v->scal, v->stream)
+                                : launch_expz(v->amps, state_len(v), c.masks.data() + m, kk, v->partials,
+                                              b->d_out + c.out_start + m, v->scal, v->stream);
+            BCK(e);
+        }
+    }
+    if (b->nsmall) {
+        BCK(launch_small_batch(f32, b->d_small, b->nsmall, b->d_ops, b->d_masks, b->d_out, b->d_counter,
+                               (int)b->small_max_n_used, (int)b->tune.small_threads, (int)b->tune.small_ctas_per_sm,
+                               s0));
+    }
+    for (uint32_t i = 1; i < ns; ++i) {
+        BCK(cudaEventRecord(b->events[i], b->streams[i]));
+        BCK(cudaStreamWaitEvent(s0, b->events[i], 0));
+    }
+    return QOA_OK;
+}
+
+}  // namespace
+
 // ==================================================================== C ABI
 extern "C" {
 
@@ -1497,6 +1802,11 @@ int qoa_destroy(qoa_state_t s) {
     if (!s) return QOA_OK;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->view) {  // batch view: only its own FP32 arena
+        if (s->f32_mats) cudaFree(s->f32_mats);
+        delete s;
+        return QOA_OK;
+    }
     for (auto& r : s->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     if (s->amps) cudaFree(s->amps);
     if (s->f32_mats) cudaFree(s->f32_mats);
@@ -1660,6 +1970,35 @@ int qoa_set_state(qoa_state_t s, const void* host, size_t bytes) {
     return QOA_OK;
 }
 
+int qoa_set_random_state(qoa_state_t s, uint64_t seed) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    const bool f32 = s->precision == QOA_PREC_F32;
+    CK(launch_random_state(s->amps, f32, state_len(s), seed, s->stream));
+    if (f32) CK(launch_f32_norm((const float2*)s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
+    else CK(launch_norm(s->amps, state_len(s), s->partials, s->scal, nullptr, s->stream));
+    s->launches += 3;
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+
+int qoa_compare(qoa_state_t a, qoa_state_t b, double* rel_l2, double* infidelity) {
+    qoa_state_t s = a;  // error reporting
+    int rc = check_handle(a);
+    if (rc) return rc;
+    if (!b || a->n != b->n || a->device != b->device) return set_err(a, QOA_E_ARG, "states differ in size or device");
+    CK(cudaStreamSynchronize(b->stream));
+    CK(launch_compare(a->amps, a->precision == QOA_PREC_F32, b->amps, b->precision == QOA_PREC_F32, state_len(a),
+                      a->scal, b->scal, a->partials, a->scal + 8, a->stream));
+    a->launches += 2;
+    double h[3];
+    CK(cudaMemcpyAsync(h, a->scal + 8, sizeof h, cudaMemcpyDeviceToHost, a->stream));
+    CK(cudaStreamSynchronize(a->stream));
+    if (rel_l2) *rel_l2 = std::sqrt(std::max(h[0], 0.0));
+    if (infidelity) *infidelity = 1.0 - (h[1] * h[1] + h[2] * h[2]);
+    return QOA_OK;
+}
+
 int qoa_seed(qoa_state_t s, uint64_t seed) {
     if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
     s->seed = seed;
@@ -1742,7 +2081,6 @@ int qoa_launch_times(qoa_state_t s, double* ms, double* bytes, int* kind, size_t
 int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t cap, int32_t* pass_of,
              int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits, double* gate_matrix, size_t* ngates,
              size_t* npasses) {
-    qoa_state_t s = nullptr;
     if ((!ops && nops) || !ngates || !npasses) return set_err(nullptr, QOA_E_ARG, "null argument");
     Expander ex;
     ex.n = std::max<uint32_t>(n, 1);
@@ -1796,6 +2134,150 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
                 gate_matrix[32 * gi + 2 * k + 1] = g.m[k].y;
             }
     }
+    return QOA_OK;
+}
+
+
+// ---- batching form ------------------------------------------------------------
+int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out) {
+    if (!out) return set_err(nullptr, QOA_E_ARG, "null out");
+    *out = nullptr;
+    if (precision != QOA_PREC_F64 && precision != QOA_PREC_F32)
+        return set_err(nullptr, QOA_E_ARG, "unsupported precision %d", precision);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(nullptr, QOA_E_NOGPU, "no CUDA device");
+    qoa_batch_t b = new qoa_batch_s();
+    b->precision = precision;
+    b->flags = flags;
+    cudaGetDevice(&b->device);
+    b->tune.small_max_n = precision == QOA_PREC_F32 ? SMALL_MAX_F32 : SMALL_MAX_F64;
+    b->tune.small_threads = 256;
+    b->tune.small_ctas_per_sm = 2;
+    b->tune.streams = 8;
+    b->tune.pass_gate_budget = 0;
+    *out = b;
+    return QOA_OK;
+}
+
+int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, const uint64_t* zmasks, size_t nmasks,
+                  uint32_t* id) {
+    if (!b || (!ops && nops) || (!zmasks && nmasks)) return bset_err(b, QOA_E_ARG, "null argument");
+    if (b->prepared) return bset_err(b, QOA_E_ARG, "batch already ran; create a new batch to add circuits");
+    if (n < 1 || n > 40) return bset_err(b, QOA_E_ARG, "bad qubit count");
+    Expander ex;
+    ex.n = n;
+    ex.flags = b->flags;
+    ex.s = nullptr;
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    if (ex.first_err != QOA_OK) return bset_err(b, ex.first_err, ex.err.c_str());
+    for (const Gate& g : ex.out)
+        if (g.kind > K_U2) return bset_err(b, QOA_E_OPCODE, "batched circuits take unitary ops only");
+    qoa_batch_s::Circ c;
+    c.n = n;
+    c.gates = std::move(ex.out);
+    c.masks.assign(zmasks, zmasks + nmasks);
+    c.out_start = b->nresults;
+    c.small = false;
+    b->nresults += (uint32_t)nmasks;
+    if (id) *id = (uint32_t)b->circs.size();
+    b->circs.push_back(std::move(c));
+    return QOA_OK;
+}
+
+int qoa_batch_set_tuning(qoa_batch_t b, const qoa_batch_tuning* t) {
+    if (!b || !t) return bset_err(b, QOA_E_ARG, "null argument");
+    if (t->small_threads < 32 || t->small_threads > 1024 || (t->small_threads & 31) || t->small_ctas_per_sm < 1 ||
+        t->streams < 1 || t->streams > 64)
+        return bset_err(b, QOA_E_ARG, "bad tuning values");
+    if (b->prepared) {
+        cudaSetDevice(b->device);
+        for (cudaStream_t st : b->streams) cudaStreamSynchronize(st);
+        batch_free_device(b);
+    }
+    b->tune = *t;
+    return QOA_OK;
+}
+
+int qoa_batch_get_tuning(qoa_batch_t b, qoa_batch_tuning* t) {
+    if (!b || !t) return bset_err(b, QOA_E_ARG, "null argument");
+    *t = b->tune;
+    return QOA_OK;
+}
+
+int qoa_batch_run(qoa_batch_t b) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, QOA_E_CUDA, "cudaSetDevice failed");
+    if (!b->prepared) {
+        int rc = batch_prepare(b);
+        if (rc) return rc;
+    }
+    if (!b->exec) {
+        // make every kernel attribute the captured launches need first
+        int rc = batch_enqueue(b);  // eager run (also the warm-up)
+        if (rc) return rc;
+        BCK(cudaStreamSynchronize(b->streams[0]));
+        BCK(cudaStreamBeginCapture(b->streams[0], cudaStreamCaptureModeThreadLocal));
+        rc = batch_enqueue(b);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->streams[0], &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        BCK(e);
+        b->graph = g;
+        BCK(cudaGraphInstantiate(&b->exec, g, 0));
+        return QOA_OK;
+    }
+    BCK(cudaGraphLaunch(b->exec, b->streams[0]));
+    BCK(cudaStreamSynchronize(b->streams[0]));
+    return QOA_OK;
+}
+
+int qoa_batch_launch(qoa_batch_t b) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    if (!b->exec) return bset_err(b, QOA_E_ARG, "qoa_batch_launch replays the graph that the first qoa_batch_run makes");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, QOA_E_CUDA, "cudaSetDevice failed");
+    BCK(cudaGraphLaunch(b->exec, b->streams[0]));
+    return QOA_OK;
+}
+
+int qoa_batch_stream(qoa_batch_t b, void** stream) {
+    if (!b || !stream) return bset_err(b, QOA_E_ARG, "null argument");
+    if (b->streams.empty()) return bset_err(b, QOA_E_ARG, "the batch has not run yet");
+    *stream = (void*)b->streams[0];
+    return QOA_OK;
+}
+
+int qoa_batch_results(qoa_batch_t b, double* out, size_t count) {
+    if (!b || (!out && count)) return bset_err(b, QOA_E_ARG, "null argument");
+    if (count != b->nresults) return bset_err(b, QOA_E_ARG, "count must equal the number of masks added");
+    if (!b->prepared) return bset_err(b, QOA_E_ARG, "run the batch first");
+    cudaSetDevice(b->device);
+    BCK(cudaStreamSynchronize(b->streams[0]));
+    if (count) BCK(cudaMemcpy(out, b->d_out, count * sizeof(double), cudaMemcpyDeviceToHost));
+    return QOA_OK;
+}
+
+int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t* large, uint32_t* graph_ready) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    if (circuits) *circuits = (uint32_t)b->circs.size();
+    if (small) *small = b->nsmall;
+    if (large) *large = (uint32_t)b->views.size();
+    if (graph_ready) *graph_ready = b->exec ? 1u : 0u;
+    return QOA_OK;
+}
+
+const char* qoa_batch_last_error(qoa_batch_t b) { return b ? b->err.c_str() : qoa_last_error(nullptr); }
+
+int qoa_batch_destroy(qoa_batch_t b) {
+    if (!b) return QOA_OK;
+    cudaSetDevice(b->device);
+    for (cudaStream_t st : b->streams) cudaStreamSynchronize(st);
+    batch_free_device(b);
+    for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+    for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
+    delete b;
     return QOA_OK;
 }
 

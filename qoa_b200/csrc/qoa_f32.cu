@@ -114,18 +114,24 @@ __device__ void f32_block(const float2* __restrict__ src, float2* __restrict__ d
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(F32_THREADS, 4)
-k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, const float* __restrict__ mats,
-           const F32Phase* __restrict__ phases, const double* __restrict__ norm2_in, double* __restrict__ partials) {
+// One CTA's tile of one FP32 pass: `blk` numbers the tile, `nrm` is the
+// input's squared norm (<= 1e-12: input |0..0>, not read), `partial_out`
+// (optional) receives the tile's squared norm after the pass.
+__device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F32PassParams& P,
+                                              const float* __restrict__ mats, const F32PhaseOp* __restrict__ pops,
+                                              const F32Angle* __restrict__ angles,
+                                              const F32Phase* __restrict__ phases, const float2* __restrict__ tables,
+                                              const double nrm, const uint64_t blk, double* __restrict__ partial_out) {
     __shared__ float2 buf[2][F32_TILE];
     __shared__ int ro[32], co[64];
     __shared__ float2 tlo[32], thi[64];
+    __shared__ double alpha[TILE_BITS + 1];
     __shared__ double red[F32_THREADS / 32];
     const int tid = threadIdx.x;
 
     uint64_t g0 = 0;
     {
-        const uint64_t b = blockIdx.x;
+        const uint64_t b = blk;
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((b >> k) & 1ull) << P.outer_qubits[k];
     }
@@ -136,7 +142,6 @@ k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, c
             if ((j >> (LANE_BITS + s)) & 1u) g += 1ull << P.slot_qubit[s];
         return g;
     };
-    const double nrm = *norm2_in;
     const bool valid = nrm > 1e-12;
     const float scale = valid ? (float)(1.0 / sqrt(nrm)) : 0.f;
 #pragma unroll 4
@@ -156,71 +161,54 @@ k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, c
             const float* a = mats + (size_t)op.index * 8192;
             f32_block(buf[cur], buf[cur ^ 1], op.bmask, a, a + 4096, ro, co);
             cur ^= 1;
-        } else if (op.kind == 1) {
-            // phases whose tile part is at most one bit: per CTA, a factor per
-            // tile bit (their outer-qubit condition is constant over the CTA),
-            // combined into tables over the 5 lane bits and the 6 high bits
-            if (tid < 64) {
-                double ar[TILE_BITS], ai[TILE_BITS];
-                double sr = 1.0, si = 0.0;
-                for (int t = 0; t < TILE_BITS; ++t) { ar[t] = 1.0; ai[t] = 0.0; }
-                for (uint32_t e = 0; e < op.count; ++e) {
-                    const F32Phase ph = phases[op.index + e];
-                    if ((g0 & ph.outer) != ph.outer) continue;
-                    const double pr = ph.re, pi = ph.im;
-                    if (ph.tile == 0) {
-                        const double t = sr * pr - si * pi;
-                        si = sr * pi + si * pr;
-                        sr = t;
-                    } else {
-                        const int t = __ffs(ph.tile) - 1;
-                        const double u = ar[t] * pr - ai[t] * pi;
-                        ai[t] = ar[t] * pi + ai[t] * pr;
-                        ar[t] = u;
-                    }
+        } else {
+            const F32PhaseOp po = pops[op.index];
+            // per-CTA angle of each tile bit (and of the scalar part)
+            if (tid <= TILE_BITS) {
+                double th = 0.0;
+                for (uint32_t e = po.bit_start[tid]; e < po.bit_start[tid + 1]; ++e) {
+                    const F32Angle an = angles[e];
+                    if ((g0 & an.outer) == an.outer) th += an.theta;
                 }
-                if (tid < 32) {
-                    double xr = sr, xi = si;
-                    for (int t = 0; t < LANE_BITS; ++t)
-                        if ((tid >> t) & 1) {
-                            const double u = xr * ar[t] - xi * ai[t];
-                            xi = xr * ai[t] + xi * ar[t];
-                            xr = u;
-                        }
-                    tlo[tid] = make_float2((float)xr, (float)xi);
-                }
-                double xr = 1.0, xi = 0.0;
-                for (int t = 0; t < HIGH_SLOTS; ++t)
-                    if ((tid >> t) & 1) {
-                        const double u = xr * ar[LANE_BITS + t] - xi * ai[LANE_BITS + t];
-                        xi = xr * ai[LANE_BITS + t] + xi * ar[LANE_BITS + t];
-                        xr = u;
-                    }
-                thi[tid] = make_float2((float)xr, (float)xi);
+                alpha[tid] = th;
             }
             __syncthreads();
+            if (tid < 32) {
+                double th = alpha[TILE_BITS];
+                for (int t = 0; t < LANE_BITS; ++t)
+                    if ((tid >> t) & 1) th += alpha[t];
+                double sn, cs;
+                sincos(th, &sn, &cs);
+                tlo[tid] = make_float2((float)cs, (float)sn);
+            }
+            if (tid < 64) {
+                double th = 0.0;
+                for (int t = 0; t < HIGH_SLOTS; ++t)
+                    if ((tid >> t) & 1) th += alpha[LANE_BITS + t];
+                double sn, cs;
+                sincos(th, &sn, &cs);
+                thi[tid] = make_float2((float)cs, (float)sn);
+            }
+            __syncthreads();
+            const float2* tab = po.table >= 0 ? tables + (size_t)po.table * F32_TILE : nullptr;
             float2* s = buf[cur];
             for (int i = 0; i < F32_PER_THREAD; ++i) {
                 const uint32_t j = (uint32_t)(tid + F32_THREADS * i);
                 const float2 l = tlo[j & 31u], h = thi[j >> LANE_BITS];
-                const float2 f = make_float2(l.x * h.x - l.y * h.y, l.x * h.y + l.y * h.x);
+                float2 f = make_float2(l.x * h.x - l.y * h.y, l.x * h.y + l.y * h.x);
+                if (tab) {
+                    const float2 u = __ldg(tab + j);
+                    f = make_float2(f.x * u.x - f.y * u.y, f.x * u.y + f.y * u.x);
+                }
+                for (uint32_t e = 0; e < po.multi_count; ++e) {
+                    const F32Phase ph = phases[po.multi_start + e];
+                    if ((g0 & ph.outer) == ph.outer && (j & ph.tile) == ph.tile) {
+                        const float pr = (float)ph.re, pi = (float)ph.im;
+                        f = make_float2(f.x * pr - f.y * pi, f.x * pi + f.y * pr);
+                    }
+                }
                 const float2 x = s[j];
                 s[j] = make_float2(x.x * f.x - x.y * f.y, x.x * f.y + x.y * f.x);
-            }
-            __syncthreads();
-        } else {
-            // phases with two or more tile bits in their mask: per amplitude
-            float2* s = buf[cur];
-            for (uint32_t e = 0; e < op.count; ++e) {
-                const F32Phase ph = phases[op.index + e];
-                if ((g0 & ph.outer) != ph.outer) continue;
-                const float pr = (float)ph.re, pi = (float)ph.im;
-                for (int i = 0; i < F32_PER_THREAD; ++i) {
-                    const uint32_t j = (uint32_t)(tid + F32_THREADS * i);
-                    if ((j & ph.tile) != ph.tile) continue;
-                    const float2 x = s[j];
-                    s[j] = make_float2(x.x * pr - x.y * pi, x.x * pi + x.y * pr);
-                }
             }
             __syncthreads();
         }
@@ -233,6 +221,7 @@ k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, c
         __stcs(amps + gidx(j), x);
         ss += (double)x.x * x.x + (double)x.y * x.y;
     }
+    if (!partial_out) return;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
     if ((tid & 31) == 0) red[tid >> 5] = ss;
@@ -240,14 +229,51 @@ k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, c
     if (tid == 0) {
         double t = 0.0;
         for (int w2 = 0; w2 < F32_THREADS / 32; ++w2) t += red[w2];
-        partials[blockIdx.x] = t;
+        *partial_out = t;
     }
 }
 
-cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32Phase* phases,
+__global__ void __launch_bounds__(F32_THREADS, 4)
+k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, const float* __restrict__ mats,
+           const F32PhaseOp* __restrict__ pops, const F32Angle* __restrict__ angles,
+           const F32Phase* __restrict__ phases, const float2* __restrict__ tables, const double* __restrict__ norm2_in,
+           double* __restrict__ partials) {
+    f32_pass_tile(amps, P, mats, pops, angles, phases, tables, *norm2_in, blockIdx.x, partials + blockIdx.x);
+}
+
+// Arena form: one launch runs one pass of each of many circuits (see
+// k_pass_arena); every circuit's block matrices, phase groups, angle lists
+// and tables lie in one shared upload, so the base pointers are common.
+__global__ void __launch_bounds__(F32_THREADS, 4)
+k_f32_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ tile_start,
+                 const float* __restrict__ mats, const F32PhaseOp* __restrict__ pops,
+                 const F32Angle* __restrict__ angles, const F32Phase* __restrict__ phases,
+                 const float2* __restrict__ tables) {
+    const uint32_t b = blockIdx.x;
+    uint32_t lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const ArenaJob J = jobs[lo];
+    f32_pass_tile(reinterpret_cast<float2*>(J.amps), *reinterpret_cast<const F32PassParams*>(J.params), mats, pops,
+                  angles, phases, tables, J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr);
+}
+
+cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                                  const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
+                                  const F32Phase* phases, const float2* tables, cudaStream_t st) {
+    if (!njobs || !tiles) return cudaSuccess;
+    k_f32_pass_arena<<<tiles, F32_THREADS, 0, st>>>(jobs, njobs, tile_start, mats, pops, angles, phases, tables);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32PhaseOp* pops,
+                            const F32Angle* angles, const F32Phase* phases, const float2* tables,
                             const double* norm2_in, double* partials, cudaStream_t st) {
     const unsigned blocks = 1u << (P.n - TILE_BITS);
-    k_f32_pass<<<blocks, F32_THREADS, 0, st>>>(amps, P, mats, phases, norm2_in, partials);
+    k_f32_pass<<<blocks, F32_THREADS, 0, st>>>(amps, P, mats, pops, angles, phases, tables, norm2_in, partials);
     return cudaGetLastError();
 }
 
@@ -304,7 +330,45 @@ __global__ void k_f32_probs(const float2* __restrict__ a, uint64_t off, uint64_t
     }
 }
 
+__global__ void k_f32_expz_partials(const float2* __restrict__ a, uint64_t len, const ExpzMasks mk, uint32_t k,
+                                    double* __restrict__ partials) {
+    __shared__ double sh[8][32];
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float2 x = a[i];
+        const double p = (double)x.x * x.x + (double)x.y * x.y;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] += (__popcll(i & mk.m[j]) & 1) ? -p : p;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        double x = v[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[j][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < k) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += sh[threadIdx.x][q];
+        partials[(uint64_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+}
+
 int reduce_blocks(uint64_t len);
+cudaError_t launch_reduce_div(const double* partials, uint32_t count, uint32_t sets, double* out, const double* divide_by,
+                              cudaStream_t st);
+
+cudaError_t launch_f32_expz(const float2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
+                            double* out, const double* norm2, cudaStream_t st) {
+    const int nb = reduce_blocks(len);
+    ExpzMasks mk{};
+    for (uint32_t j = 0; j < k && j < 8; ++j) mk.m[j] = masks[j];
+    k_f32_expz_partials<<<nb, 256, 0, st>>>(a, len, mk, k, partials);
+    return launch_reduce_div(partials, (uint32_t)nb, k, out, norm2, st);
+}
+
 cudaError_t launch_reduce_partials(const double* partials, uint32_t count, double* out, uint32_t* status,
                                    cudaStream_t st);
 

@@ -131,9 +131,12 @@ __device__ __forceinline__ uint64_t tstride(const PassParams& P, uint32_t t) {
 }
 
 // ------------------------------------------------------------ the pass kernel
-__global__ void __launch_bounds__(PASS_THREADS, 4)
-k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
-       double* __restrict__ partials) {
+// One CTA's tile of one pass. `blk` numbers the tile (its bits go to the
+// qubits outside the tile); `nrm` is the input's squared norm (<= 1e-12: the
+// input is |0..0>, synthesised without reading); `partial_out`, when not
+// null, receives the tile's squared norm after the pass.
+__device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const PassParams& P, const double nrm,
+                                          const uint64_t blk, double* __restrict__ partial_out) {
     extern __shared__ double2 tile[];
     __shared__ double red[PASS_THREADS / 32];
     const int lane = threadIdx.x & 31;
@@ -143,7 +146,7 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
     // qubits outside the tile.
     uint64_t g0 = 0;
     {
-        const uint64_t b = blockIdx.x;
+        const uint64_t b = blk;
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((b >> k) & 1ull) << P.outer_qubits[k];
     }
@@ -158,7 +161,6 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
         for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS) scoef[i] = P.coef[i];
     }
 
-    const double nrm = *norm2_in;
     const bool valid = nrm > 1e-12;
     // The input's 1/||psi|| and the pass's factored global phase are applied
     // once, at the end, as part of the per-thread pending factor.
@@ -362,6 +364,7 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
             ss += c_abs2(x);
         }
     }
+    if (!partial_out) return;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
     if (lane == 0) red[wid] = ss;
@@ -370,8 +373,33 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
         double t = 0.0;
 #pragma unroll
         for (int w2 = 0; w2 < PASS_THREADS / 32; ++w2) t += red[w2];
-        partials[blockIdx.x] = t;
+        *partial_out = t;
     }
+}
+
+__global__ void __launch_bounds__(PASS_THREADS, 4)
+k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
+       double* __restrict__ partials) {
+    pass_tile(amps, P, *norm2_in, blockIdx.x, partials + blockIdx.x);
+}
+
+// Arena pass: one launch runs one pass of each of many circuits, whose states
+// lie in one packed arena. CTA b runs tile b - tile_start[j] of job j, where
+// j is the last job with tile_start[j] <= b. Squared norms are not tracked: a
+// batched circuit is unitary, its start |0..0> is synthesised by its first
+// pass, and its consumers normalise.
+__global__ void __launch_bounds__(PASS_THREADS, 4)
+k_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ tile_start) {
+    const uint32_t b = blockIdx.x;
+    uint32_t lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (tile_start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const ArenaJob J = jobs[lo];
+    pass_tile(reinterpret_cast<double2*>(J.amps), *reinterpret_cast<const PassParams*>(J.params),
+              J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr);
 }
 
 // ------------------------------------------------------- per-gate kernels
@@ -676,6 +704,17 @@ cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_
     return cudaGetLastError();
 }
 
+cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                              int max_nops, int max_ncoef, cudaStream_t st) {
+    if (!njobs || !tiles) return cudaSuccess;
+    const int smem = (1 << TILE_BITS) * (int)sizeof(double2) + max_nops * 16 + max_ncoef * 16;
+    cudaError_t e = cudaFuncSetAttribute(k_pass_arena, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (1 << TILE_BITS) * (int)sizeof(double2) + MAX_PASS_OPS * 16 + MAX_PASS_COEF * 16);
+    if (e != cudaSuccess) return e;
+    k_pass_arena<<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st) {
     const int threads = 256;
     const int blocks = grid_for(len, threads, 148 * 16);
@@ -726,6 +765,17 @@ cudaError_t launch_expz(const double2* a, uint64_t len, const uint64_t* masks, u
     for (uint32_t j = 0; j < k && j < 8; ++j) mk.m[j] = masks[j];
     k_expz_partials<<<nb, 256, 0, st>>>(a, len, mk, k, partials);
     k_reduce<<<k, 1024, 0, st>>>(partials, nb, out, norm2, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_div(const double* partials, uint32_t count, uint32_t sets, double* out, const double* divide_by,
+                              cudaStream_t st) {
+    k_reduce<<<sets, 1024, 0, st>>>(partials, count, out, divide_by, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_sets(const double* partials, uint32_t count, uint32_t sets, double* out, cudaStream_t st) {
+    k_reduce<<<sets, 1024, 0, st>>>(partials, count, out, nullptr, nullptr);
     return cudaGetLastError();
 }
 

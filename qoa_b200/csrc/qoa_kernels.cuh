@@ -111,16 +111,30 @@ struct PassParams {
     double2 coef[MAX_PASS_COEF];
 };
 
+// One circuit's pass inside an arena launch: its state, the pass's parameters
+// (PassParams for complex128, F32ArenaPass for complex64), and whether this is
+// the circuit's first pass (input |0..0>, not read).
+struct ArenaJob {
+    void* amps;
+    const void* params;
+    uint32_t fresh;
+    uint32_t pad_;
+};
+
 // ---------------------------------------------------------------------------
 // FP32-fused precision passes (qoa_f32.cu)
 // ---------------------------------------------------------------------------
 constexpr int MAX_F32_OPS = 256;
 
+struct ExpzMasks {
+    uint64_t m[8];
+};
+
 struct F32Op {
-    uint32_t kind;   // 0 = dense block, 1 = phases with <= 1 tile bit, 2 = phases with >= 2 tile bits
+    uint32_t kind;   // 0 = dense block, 1 = phase group
     uint32_t bmask;  // kind 0: the 5 tile bits the block acts on
-    uint32_t index;  // kind 0: matrix index; kind 1/2: first phase entry
-    uint32_t count;  // kind 1/2: number of phase entries
+    uint32_t index;  // kind 0: matrix index; kind 1: F32PhaseOp index
+    uint32_t count;
 };
 
 // Multiply by (re, im) where the global index has every bit of `outer` and
@@ -132,12 +146,65 @@ struct F32Phase {
     double re, im;
 };
 
+// A phase group (F32Op kind 1). Every phase is e^{i theta}. The part that does
+// not depend on the CTA is a host-made table over the 2048 tile indices; the
+// CTA-dependent part with at most one tile bit is a list of (outer mask,
+// angle) per tile bit t (t = TILE_BITS: no tile bit), summed per CTA; the
+// rest (two or more tile bits and an outer condition) is checked per
+// amplitude.
+struct F32Angle {
+    uint64_t outer;
+    double theta;
+};
+struct F32PhaseOp {
+    int32_t table;                      // index of a 2048-entry float2 table, or -1
+    uint32_t bit_start[TILE_BITS + 2];  // F32Angle ranges per tile bit (and scalar)
+    uint32_t multi_start, multi_count;  // F32Phase entries checked per amplitude
+};
+
 struct F32PassParams {
     uint32_t n;
     uint32_t nops;
     uint8_t slot_qubit[HIGH_SLOTS];
     uint8_t outer_qubits[64];
     F32Op ops[MAX_F32_OPS];
+};
+
+// ---------------------------------------------------------------------------
+// Batched small circuits (qoa_batch.cu): whole state in shared memory
+// ---------------------------------------------------------------------------
+constexpr int SMALL_MAX_F64 = 12;  // 2^12 complex128 = 64 KB
+constexpr int SMALL_MAX_F32 = 13;  // 2^13 complex64 = 64 KB
+
+enum SmallKind : uint8_t { SK_G1 = 0, SK_DIAG = 1, SK_SWAP = 2 };
+
+struct SmallOp {
+    uint8_t kind;
+    uint8_t sub;
+    uint8_t t;       // target / selector (255: none)
+    uint8_t t2;
+    uint32_t cmask;  // condition: every bit set
+    double2 m[4];    // SK_G1: m00 m01 m10 m11; SK_DIAG: d0, d1
+};
+
+// Arena circuits' <Z_mask>: chunk partial sums, then one CTA per circuit.
+constexpr uint32_t EXPZ_CHUNK = 4096;
+constexpr uint32_t EXPZ_MAX_MASKS = 255;
+struct ExpzJob {
+    const void* amps;
+    uint32_t n;
+    uint32_t mask_start, mask_count;
+    uint32_t out_start;
+    uint32_t chunk_start;  // first partials-kernel CTA of this circuit
+    uint32_t pad_;
+    uint64_t part_start;   // first partial (chunks x (mask_count + 1) of them)
+};
+
+struct SmallCircuit {
+    uint32_t n;
+    uint32_t op_start, op_count;
+    uint32_t mask_start, mask_count;
+    uint32_t out_start;
 };
 
 // ---------------------------------------------------------------------------

@@ -84,3 +84,22 @@ def test_f32_rejects_non_unitary_ops_and_small_n():
     with qb.QuantumState(12, precision="f32") as st:
         with pytest.raises(qb.QoaError):
             st.execute(C.ops_to_array([C.Op(C.MEASURE, [0])]))
+
+
+@pytest.mark.gpu
+def test_random_state_and_compare():
+    n = 14
+    with qb.QuantumState(n) as a, qb.QuantumState(n, precision="f32") as b, qb.QuantumState(n) as c:
+        a.set_random_state(7)
+        b.set_random_state(7)
+        c.set_random_state(8)
+        va = a.get_state_vector()
+        assert abs(np.linalg.norm(va) - 1) < 1e-12
+        # near-Gaussian amplitudes: E|a|^2 = 1/N per amplitude
+        assert 0.9 < np.mean(np.abs(va) ** 2) * (1 << n) < 1.1
+        r, f = b.compare(a)
+        assert r < 1e-6 and abs(f) < 1e-12
+        r2, f2 = a.compare(c)
+        assert r2 > 1.0 and f2 > 0.9
+        r3, f3 = a.compare(a)
+        assert r3 == 0.0 and abs(f3) < 1e-14
