@@ -392,6 +392,119 @@ def run_qft(args):
     return 0
 
 
+def run_batch(args):
+    """Batching form: 4096 hardware-efficient variational circuits (n ~ U{8..22},
+    L ~ U{2..12} layers of RY+RZ on every qubit then a CZ ladder, 8 random
+    Z-strings each), all in one batch: shared-memory persistent kernel for the
+    small ones, arena tile-pass rounds for the rest, replayed as one CUDA graph.
+    value = circuits/s of graph replays (device time); e2e = circuits/s of a
+    fresh batch per step through the public API (host op lists in, planning,
+    upload, eager launch, results out)."""
+    import numpy as np
+    import torch
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+    from qoa_b200 import autotune
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    circs = C.variational_batch(count=args.batch_count, seed=3)
+    for c in circs:
+        c["ops"] = C.ops_to_array(c["ops"])
+    gen_s = time.perf_counter() - t0
+    count = len(circs)
+    gates = int(sum(len(c["ops"]) for c in circs))
+    out = {"metric": "circuits/s", "unit": "circuits/s", "impl": "qoa_b200", "higher_is_better": True,
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "scaling": "weak", "vs_baseline": None,
+           "data": "synthetic (seeded variational circuits)",
+           "config": {"workload": f"{count} variational circuits, n~U[8,22], L~U[2,12], RY+RZ layers + CZ ladder, "
+                                  "8 Z-strings each", "circuits": count, "gates": gates, "seed": 3,
+                      "l2_policy": "arena larger than L2"}}
+    results = {}
+    for prec in args.precisions.split(","):
+        t1 = time.perf_counter()
+        tuning = autotune.tune(circs, prec, sample=args.tune_sample, budget_s=args.tune_seconds) \
+            if args.tune_sample > 0 else None
+        tune_s = time.perf_counter() - t1
+        b = qb.Batch(prec)
+        if tuning:
+            b.set_tuning(**tuning)
+        t2 = time.perf_counter()
+        for c in circs:
+            b.add(c["n"], c["ops"], c["masks"])
+        b.run()
+        first_s = time.perf_counter() - t2
+        b.run()
+        info = b.info()
+        stream = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)
+        for _ in range(args.warmup):
+            b.launch()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(0)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        res = b.results()
+        b.close()
+        results[prec] = res
+        results[prec + "_line"] = {
+            "value": count / (ms / 1e3), "ms_per_step": ms, "tuning": tuning or "defaults",
+            "autotune_s": tune_s, "first_run_s": first_s, "routes": info, "clocks": clk,
+            "gates_per_s": gates / (ms / 1e3)}
+    prim = args.precisions.split(",")[0]
+    out.update(value=results[prim + "_line"]["value"], ms_per_step=results[prim + "_line"]["ms_per_step"],
+               dtype="f64" if prim == "f64" else "complex64 (3xTF32)", clocks=results[prim + "_line"]["clocks"])
+    for prec in args.precisions.split(","):
+        out[prec] = results[prec + "_line"]
+    if "f64" in results and "f32" in results:
+        out["f32_vs_f64_max_abs_diff"] = float(np.max(np.abs(results["f32"] - results["f64"])))
+    # e2e: a fresh batch per step through the public API
+    k = max(1, args.e2e_steps)
+    t3 = time.perf_counter()
+    for _ in range(k):
+        with qb.Batch(prim) as b:
+            if results[prim + "_line"]["tuning"] != "defaults":
+                b.set_tuning(**results[prim + "_line"]["tuning"])
+            for c in circs:
+                b.add(c["n"], c["ops"], c["masks"])
+            b.run()
+            r = b.results()
+    e2e_s = (time.perf_counter() - t3) / k
+    out["e2e"] = {"value": count / e2e_s, "unit": "circuits/s",
+                  "h2d_bytes_per_step": int(sum(c["ops"].nbytes + 8 * len(c["masks"]) for c in circs)),
+                  "d2h_bytes_per_step": int(r.nbytes), "steps": k,
+                  "note": "wall clock: host planning + upload + eager launches + results"}
+    if not args.no_cpu:
+        from oracle import pyoracle as po
+        po.set_fast(False)
+        rng = np.random.default_rng(5)
+        order = rng.permutation(count)
+        t_cpu, done = 0.0, 0
+        for i in order:
+            c = circs[i]
+            st = po.OracleState(c["n"], 0)
+            tt = time.perf_counter()
+            st.apply(c["ops"])
+            t_cpu += time.perf_counter() - tt
+            st.close()
+            done += 1
+            if t_cpu > args.cpu_seconds:
+                break
+        out["cpu_baseline"] = {"value": done / t_cpu, "unit": "circuits/s", "kind": "port",
+                               "cores": int(po.lib.orc_get_max_threads()),
+                               "sample": f"{done} circuits drawn at random from the same batch, faithful oracle "
+                                         "(per-gate loops + normalize after every gate)"}
+    out["generate_s"] = gen_s
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -406,11 +519,17 @@ def main():
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
     ap.add_argument("--depth", type=int, default=20)
-    ap.add_argument("--workload", default="layered", choices=["layered", "qft"])
+    ap.add_argument("--workload", default="layered", choices=["layered", "qft", "batch"])
     ap.add_argument("--qft-qubits", type=int, default=33)
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--precisions", default="f64,f32")
+    ap.add_argument("--tune-sample", type=int, default=256)
+    ap.add_argument("--tune-seconds", type=float, default=60.0)
     args = ap.parse_args()
     if args.workload == "qft":
         return run_qft(args)
+    if args.workload == "batch":
+        return run_batch(args)
     if (args.qubits, args.depth) != (30, 20):
         set_workload(args.qubits, args.depth)
     if args.impl == "reference":

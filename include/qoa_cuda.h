@@ -206,8 +206,8 @@ const char* qoa_strerror(int code);
  * most 12 for complex128, 13 for complex64) run whole-state in shared memory
  * in one persistent launch; larger ones run as tile passes on views into one
  * packed arena, spread over tune.streams streams. The first qoa_batch_run
- * runs eagerly, then captures the whole batch into a CUDA graph; later runs
- * replay it. Results: <Z_mask> of each circuit's final state for the masks
+ * launches eagerly; the second captures the whole batch into a CUDA graph and
+ * launches it; later runs replay the graph. Results: <Z_mask> of each circuit's final state for the masks
  * given at qoa_batch_add, in order of addition. Unitary ops only. */
 typedef struct qoa_batch_s* qoa_batch_t;
 typedef struct qoa_batch_tuning {

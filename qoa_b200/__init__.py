@@ -399,9 +399,10 @@ class Batch:
     """Many circuits run together (qoa_batch_*): each circuit starts in
     |0..0>, applies its unitary op list and yields <Z_mask> of its final
     normalised state for each mask given. Small circuits run whole-state in
-    shared memory in one persistent launch; larger ones run as tile passes on
-    views into one packed arena. The first run() captures the batch into a
-    CUDA graph that later runs replay."""
+    shared memory in one persistent launch; larger ones run as tile passes
+    over one packed arena, one launch per pass round across all of them. The
+    first run() launches eagerly, the second captures the batch into a CUDA
+    graph, later runs replay it."""
 
     def __init__(self, precision: str = "f64", compat_mask_quirk: bool = False):
         if precision not in ("f64", "f32"):

@@ -39,9 +39,9 @@ cudaError_t launch_collapse(double2* a, uint64_t len, uint32_t q, uint32_t outco
 cudaError_t launch_materialize(double2* a, uint64_t len, double* norm2, double* partials, uint32_t* status, cudaStream_t st);
 cudaError_t launch_set_scalar(double* p, double v, cudaStream_t st);
 cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const double* norm2, double* out, cudaStream_t st);
-cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st);
-cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
-                          uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
+cudaError_t launch_tree(const void* a, bool f32, uint32_t n, const double* norm2, double* tree, cudaStream_t st);
+cudaError_t launch_sample(const void* a, bool f32, uint32_t n, const double* norm2, const double* tree,
+                          const double* u, uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
 cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32PhaseOp* pops,
                             const F32Angle* angles, const F32Phase* phases, const float2* tables,
                             const double* norm2_in, double* partials, cudaStream_t st);
@@ -55,6 +55,13 @@ cudaError_t launch_f32_probs(const float2* a, uint64_t off, uint64_t cnt, const 
 cudaError_t launch_random_state(void* a, bool f32, uint64_t len, uint64_t seed, cudaStream_t st);
 cudaError_t launch_f32_expz(const float2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
                             double* out, const double* norm2, cudaStream_t st);
+cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                              int max_nops, int max_ncoef, cudaStream_t st);
+cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                                  const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
+                                  const F32Phase* phases, const float2* tables, cudaStream_t st);
+cudaError_t launch_arena_expz(bool f32, const ExpzJob* jobs, uint32_t njobs, uint32_t chunks, const uint64_t* masks,
+                              double* partials, double* out, cudaStream_t st);
 cudaError_t launch_small_batch(bool f32, const SmallCircuit* circs, uint32_t count, const SmallOp* ops,
                                const uint64_t* masks, double* out, unsigned int* counter, int max_n, int threads,
                                int ctas_per_sm, cudaStream_t st);
@@ -1325,6 +1332,26 @@ double next_meas_uniform(qoa_state_t s) {
     return uniform01(s->seed, s->noise_stream ^ kMeasStreamXor, s->meas_draws++, 0);
 }
 
+// Packs an FP32 upload (block matrices, phase groups, angle lists, phases,
+// tables) into one 256-byte-aligned image; off[] receives the offsets.
+std::vector<unsigned char> f32_pack(const F32Upload& up, size_t off[5]) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    off[0] = 0;
+    off[1] = al(off[0] + up.mats.size() * sizeof(float));
+    off[2] = al(off[1] + up.pops.size() * sizeof(F32PhaseOp));
+    off[3] = al(off[2] + up.angles.size() * sizeof(F32Angle));
+    off[4] = al(off[3] + up.phases.size() * sizeof(F32Phase));
+    const size_t total = al(off[4] + up.tables.size() * sizeof(float2)) + 256;
+    std::vector<unsigned char> host(total, 0);
+    auto put = [&](size_t o, const void* src, size_t bytes) { if (bytes) memcpy(host.data() + o, src, bytes); };
+    put(off[0], up.mats.data(), up.mats.size() * sizeof(float));
+    put(off[1], up.pops.data(), up.pops.size() * sizeof(F32PhaseOp));
+    put(off[2], up.angles.data(), up.angles.size() * sizeof(F32Angle));
+    put(off[3], up.phases.data(), up.phases.size() * sizeof(F32Phase));
+    put(off[4], up.tables.data(), up.tables.size() * sizeof(float2));
+    return host;
+}
+
 // FP32 precision form: every step must be a fused pass. Prepare builds all
 // passes of an op list and uploads their block matrices and phases at once
 // (synchronously); launch only enqueues kernels, so it can be captured.
@@ -1341,21 +1368,8 @@ int f32_prepare(qoa_state_t s, std::vector<Gate>& G) {
         if (build_f32_pass(G, steps[i], s->n, s->f32_passes[i], up) != 0)
             return set_err(s, QOA_E_ARG, "FP32 pass %zu does not fit one launch", i);
     }
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    size_t* o = s->f32_off;
-    o[0] = 0;
-    o[1] = al(o[0] + up.mats.size() * sizeof(float));
-    o[2] = al(o[1] + up.pops.size() * sizeof(F32PhaseOp));
-    o[3] = al(o[2] + up.angles.size() * sizeof(F32Angle));
-    o[4] = al(o[3] + up.phases.size() * sizeof(F32Phase));
-    const size_t total = al(o[4] + up.tables.size() * sizeof(float2)) + 256;
-    std::vector<unsigned char> host(total, 0);
-    auto put = [&](size_t off, const void* src, size_t bytes) { if (bytes) memcpy(host.data() + off, src, bytes); };
-    put(o[0], up.mats.data(), up.mats.size() * sizeof(float));
-    put(o[1], up.pops.data(), up.pops.size() * sizeof(F32PhaseOp));
-    put(o[2], up.angles.data(), up.angles.size() * sizeof(F32Angle));
-    put(o[3], up.phases.data(), up.phases.size() * sizeof(F32Phase));
-    put(o[4], up.tables.data(), up.tables.size() * sizeof(float2));
+    std::vector<unsigned char> host = f32_pack(up, s->f32_off);
+    const size_t total = host.size();
     CK(cudaStreamSynchronize(s->stream));
     if (total > s->f32_mats_cap) {
         if (s->f32_mats) cudaFree(s->f32_mats);
@@ -1504,12 +1518,21 @@ inline bool shim_bit_ok(size_t b) { return b < 64; }
 }  // namespace
 
 // ================================================================ batching
-// Many circuits in one go. Circuits small enough for a CTA's shared memory run
-// in one persistent launch (k_small_batch); the others run as tile passes on
-// views into one packed arena, spread over a pool of streams. The first run
-// captures all of it (small launch, every large circuit's reset / passes /
-// expectation values, fork and join over the streams) into a CUDA graph;
-// later runs replay the graph.
+// Many circuits in one go, by three routes:
+//  - small: whole state in one CTA's shared memory; all such circuits in one
+//    persistent launch (k_small_batch);
+//  - arena: n >= the tile size and every step a tile pass; states packed in
+//    one arena, and round r is ONE launch of k_pass_arena / k_f32_pass_arena
+//    over the r-th pass of every circuit that has one (a circuit's first pass
+//    synthesises |0..0>, so there is no reset launch);
+//  - view: anything else (per-gate steps) runs through the engine's own
+//    executor on a handle that views its slice of the arena, round-robin
+//    over a pool of streams.
+// All <Z_mask> results of the arena and view circuits come from one pair of
+// launches over the arena. The first run executes eagerly and captures
+// everything into a CUDA graph; later runs replay it.
+enum BatchRoute { R_SMALL = 0, R_ARENA = 1, R_VIEW = 2 };
+
 struct qoa_batch_s {
     int precision = QOA_PREC_F64;
     uint32_t flags = 0;
@@ -1520,23 +1543,39 @@ struct qoa_batch_s {
         std::vector<Gate> gates;
         std::vector<uint64_t> masks;
         uint32_t out_start;
-        bool small;
+        int route;
+        size_t state_off;  // arena / view: offset of the state in the arena
     };
     std::vector<Circ> circs;
     uint32_t nresults = 0;
     bool prepared = false;
+    uint64_t runs = 0;
     // device
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> events;
     void* arena = nullptr;
     SmallCircuit* d_small = nullptr;
     SmallOp* d_ops = nullptr;
-    uint64_t* d_masks = nullptr;
+    uint64_t* d_masks = nullptr;   // every circuit's masks, in order of addition
     double* d_out = nullptr;
     unsigned int* d_counter = nullptr;
     uint32_t nsmall = 0;
     uint32_t small_max_n_used = 0;
-    std::vector<qoa_state_t> views;       // per large circuit
+    // arena route
+    void* d_params = nullptr;      // PassParams[] or F32PassParams[]
+    void* d_f32 = nullptr;         // FP32 upload shared by all arena circuits
+    size_t f32_off[5] = {};
+    ArenaJob* d_jobs = nullptr;
+    uint32_t* d_tstart = nullptr;
+    struct Round { uint32_t job_off, njobs, tiles; int max_nops, max_ncoef; };
+    std::vector<Round> rounds;
+    uint32_t narena = 0;
+    // expectation values of arena and view circuits
+    ExpzJob* d_ejobs = nullptr;
+    uint32_t n_ejobs = 0, e_chunks = 0;
+    double* d_epart = nullptr;
+    // view route
+    std::vector<qoa_state_t> views;
     std::vector<int> view_circ;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1585,6 +1624,12 @@ SmallOp to_small(const Gate& g) {
     return o;
 }
 
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
 void batch_free_device(qoa_batch_t b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -1593,55 +1638,187 @@ void batch_free_device(qoa_batch_t b) {
     for (qoa_state_t v : b->views) qoa_destroy(v);
     b->views.clear();
     b->view_circ.clear();
-    for (void* p : {(void*)b->arena, (void*)b->d_small, (void*)b->d_ops, (void*)b->d_masks, (void*)b->d_out,
-                    (void*)b->d_counter})
-        if (p) cudaFree(p);
-    b->arena = nullptr; b->d_small = nullptr; b->d_ops = nullptr; b->d_masks = nullptr; b->d_out = nullptr;
-    b->d_counter = nullptr;
+    dfree(b->arena); dfree(b->d_small); dfree(b->d_ops); dfree(b->d_masks); dfree(b->d_out); dfree(b->d_counter);
+    dfree(b->d_params); dfree(b->d_f32); dfree(b->d_jobs); dfree(b->d_tstart); dfree(b->d_ejobs); dfree(b->d_epart);
+    b->rounds.clear();
+    b->nsmall = b->narena = b->n_ejobs = b->e_chunks = 0;
     b->prepared = false;
+    b->runs = 0;
+}
+
+template <typename T>
+int upload(qoa_batch_t b, T*& dst, const std::vector<T>& src) {
+    BCK(cudaMalloc((void**)&dst, std::max<size_t>(1, src.size()) * sizeof(T)));
+    if (!src.empty()) BCK(cudaMemcpy((void*)dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return QOA_OK;
 }
 
 int batch_prepare(qoa_batch_t b) {
     const bool f32 = b->precision == QOA_PREC_F32;
     const uint32_t cap = f32 ? SMALL_MAX_F32 : SMALL_MAX_F64;
     const uint32_t smax = std::min<uint32_t>(b->tune.small_max_n, cap);
-    // small circuits
+    const int budget = (int)b->tune.pass_gate_budget;
+    const size_t esz = f32 ? sizeof(float2) : sizeof(double2);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+
     std::vector<SmallCircuit> sc;
     std::vector<SmallOp> sops;
     std::vector<uint64_t> masks;
+    std::vector<uint32_t> mask_start(b->circs.size());
+    for (size_t i = 0; i < b->circs.size(); ++i) {
+        mask_start[i] = (uint32_t)masks.size();
+        masks.insert(masks.end(), b->circs[i].masks.begin(), b->circs[i].masks.end());
+    }
+    // arena route: every pass of every circuit, built on the host
+    std::vector<PassParams> p64;
+    std::vector<F32PassParams> p32;
+    F32Upload up;
+    std::vector<std::vector<uint32_t>> pass_idx(b->circs.size());
     uint32_t maxn = 1;
-    for (auto& c : b->circs) {
-        c.small = c.n <= smax || (f32 && c.n < (uint32_t)TILE_BITS);
-        for (const Gate& g : c.gates) c.small = c.small && small_ok(g);
-        if (!c.small && (c.n < (uint32_t)TILE_BITS && f32))
+    size_t total = 0;  // arena bytes
+    for (size_t i = 0; i < b->circs.size(); ++i) {
+        auto& c = b->circs[i];
+        bool small = c.n <= smax || (f32 && c.n < (uint32_t)TILE_BITS);
+        for (const Gate& g : c.gates) small = small && small_ok(g);
+        if (small) {
+            if (c.n > cap) return bset_err(b, QOA_E_ARG, "circuit too large for the shared-memory kernel");
+            c.route = R_SMALL;
+            SmallCircuit d;
+            d.n = c.n;
+            d.op_start = (uint32_t)sops.size();
+            for (const Gate& g : c.gates) sops.push_back(to_small(g));
+            d.op_count = (uint32_t)c.gates.size();
+            d.mask_start = mask_start[i];
+            d.mask_count = (uint32_t)c.masks.size();
+            d.out_start = c.out_start;
+            sc.push_back(d);
+            maxn = std::max(maxn, c.n);
+            continue;
+        }
+        if (f32 && c.n < (uint32_t)TILE_BITS)
             return bset_err(b, QOA_E_ARG, "circuit below the FP32 tile size with a gate the small kernel lacks");
-        if (!c.small) continue;
-        if (c.n > cap) return bset_err(b, QOA_E_ARG, "circuit too large for the shared-memory kernel");
-        SmallCircuit d;
-        d.n = c.n;
-        d.op_start = (uint32_t)sops.size();
-        for (const Gate& g : c.gates) sops.push_back(to_small(g));
-        d.op_count = (uint32_t)c.gates.size();
-        d.mask_start = (uint32_t)masks.size();
-        masks.insert(masks.end(), c.masks.begin(), c.masks.end());
-        d.mask_count = (uint32_t)c.masks.size();
-        d.out_start = c.out_start;
-        sc.push_back(d);
-        maxn = std::max(maxn, c.n);
+        c.route = R_VIEW;
+        if (c.n >= (uint32_t)TILE_BITS && !c.gates.empty()) {
+            std::vector<Step> steps = schedule(c.gates, c.n, false, f32, budget);
+            bool ok = true;
+            for (const Step& st : steps) ok = ok && st.pass;
+            if (ok && !f32) {
+                const size_t base = p64.size();
+                p64.resize(base + steps.size());
+                for (size_t k = 0; k < steps.size() && ok; ++k) ok = build_pass(c.gates, steps[k], c.n, p64[base + k]) == 0;
+                if (!ok) p64.resize(base);
+                else
+                    for (size_t k = 0; k < steps.size(); ++k) pass_idx[i].push_back((uint32_t)(base + k));
+            } else if (ok) {
+                const size_t base = p32.size();
+                p32.resize(base + steps.size());
+                for (size_t k = 0; k < steps.size(); ++k)
+                    if (build_f32_pass(c.gates, steps[k], c.n, p32[base + k], up) != 0)
+                        return bset_err(b, QOA_E_ARG, "FP32 pass does not fit one launch");
+                for (size_t k = 0; k < steps.size(); ++k) pass_idx[i].push_back((uint32_t)(base + k));
+            } else if (f32) {
+                return bset_err(b, QOA_E_OPCODE, "gate outside an FP32 pass");
+            }
+            if (ok) c.route = R_ARENA;
+        }
+        c.state_off = total;
+        total = al(total + (esz << c.n));
+    }
+    // view scratch (partials, scalars, status) after the states
+    std::vector<size_t> view_off;
+    for (auto& c : b->circs) {
+        if (c.route != R_VIEW) continue;
+        view_off.push_back(total);
+        total = al(total + partials_needed(c.n) * sizeof(double));
+        total = al(total + 16 * sizeof(double));
+        total = al(total + 4 * sizeof(uint32_t));
     }
     b->nsmall = (uint32_t)sc.size();
     b->small_max_n_used = maxn;
     BCK(cudaMalloc(&b->d_out, std::max<size_t>(1, b->nresults) * sizeof(double)));
     BCK(cudaMalloc(&b->d_counter, sizeof(unsigned int)));
+    int rc;
+    if ((rc = upload(b, b->d_masks, masks))) return rc;
     if (!sc.empty()) {
-        BCK(cudaMalloc(&b->d_small, sc.size() * sizeof(SmallCircuit)));
-        BCK(cudaMalloc(&b->d_ops, std::max<size_t>(1, sops.size()) * sizeof(SmallOp)));
-        BCK(cudaMalloc(&b->d_masks, std::max<size_t>(1, masks.size()) * sizeof(uint64_t)));
-        BCK(cudaMemcpy(b->d_small, sc.data(), sc.size() * sizeof(SmallCircuit), cudaMemcpyHostToDevice));
-        if (!sops.empty()) BCK(cudaMemcpy(b->d_ops, sops.data(), sops.size() * sizeof(SmallOp), cudaMemcpyHostToDevice));
-        if (!masks.empty())
-            BCK(cudaMemcpy(b->d_masks, masks.data(), masks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        if ((rc = upload(b, b->d_small, sc))) return rc;
+        if ((rc = upload(b, b->d_ops, sops))) return rc;
     }
+    if (total) BCK(cudaMalloc(&b->arena, total));
+    unsigned char* arena = (unsigned char*)b->arena;
+
+    // arena rounds
+    const size_t psz = f32 ? sizeof(F32PassParams) : sizeof(PassParams);
+    if (f32 ? !p32.empty() : !p64.empty()) {
+        BCK(cudaMalloc(&b->d_params, (f32 ? p32.size() : p64.size()) * psz));
+        BCK(cudaMemcpy(b->d_params, f32 ? (const void*)p32.data() : (const void*)p64.data(),
+                       (f32 ? p32.size() : p64.size()) * psz, cudaMemcpyHostToDevice));
+    }
+    if (f32 && !p32.empty()) {
+        std::vector<unsigned char> img = f32_pack(up, b->f32_off);
+        BCK(cudaMalloc(&b->d_f32, img.size()));
+        BCK(cudaMemcpy(b->d_f32, img.data(), img.size(), cudaMemcpyHostToDevice));
+    }
+    std::vector<ArenaJob> jobs;
+    std::vector<uint32_t> tstart;
+    size_t maxp = 0;
+    for (auto& v : pass_idx) maxp = std::max(maxp, v.size());
+    for (size_t r = 0; r < maxp; ++r) {
+        qoa_batch_s::Round R{(uint32_t)jobs.size(), 0, 0, 0, 0};
+        for (size_t i = 0; i < b->circs.size(); ++i) {
+            if (pass_idx[i].size() <= r) continue;
+            const auto& c = b->circs[i];
+            const uint32_t pi = pass_idx[i][r];
+            ArenaJob J;
+            J.amps = arena + c.state_off;
+            J.params = (const unsigned char*)b->d_params + (size_t)pi * psz;
+            J.fresh = r == 0;
+            J.pad_ = 0;
+            jobs.push_back(J);
+            tstart.push_back(R.tiles);
+            R.tiles += 1u << (c.n - TILE_BITS);
+            R.njobs++;
+            if (!f32) {
+                R.max_nops = std::max(R.max_nops, (int)p64[pi].nops);
+                R.max_ncoef = std::max(R.max_ncoef, (int)p64[pi].ncoef);
+            }
+        }
+        b->rounds.push_back(R);
+    }
+    for (auto& v : pass_idx) b->narena += v.empty() ? 0u : 1u;
+    if (!jobs.empty()) {
+        if ((rc = upload(b, b->d_jobs, jobs))) return rc;
+        if ((rc = upload(b, b->d_tstart, tstart))) return rc;
+    }
+
+    // expectation values of every arena and view circuit
+    std::vector<ExpzJob> ej;
+    uint32_t chunks = 0;
+    uint64_t parts = 0;
+    for (size_t i = 0; i < b->circs.size(); ++i) {
+        const auto& c = b->circs[i];
+        if (c.route == R_SMALL || c.masks.empty()) continue;
+        if (c.masks.size() > EXPZ_MAX_MASKS) return bset_err(b, QOA_E_ARG, "more than 255 masks on one circuit");
+        ExpzJob J;
+        memset(&J, 0, sizeof J);
+        J.amps = arena + c.state_off;
+        J.n = c.n;
+        J.mask_start = mask_start[i];
+        J.mask_count = (uint32_t)c.masks.size();
+        J.out_start = c.out_start;
+        J.chunk_start = chunks;
+        J.part_start = parts;
+        const uint32_t nch = (uint32_t)(((1ull << c.n) + EXPZ_CHUNK - 1) / EXPZ_CHUNK);
+        chunks += nch;
+        parts += (uint64_t)nch * (J.mask_count + 1);
+        ej.push_back(J);
+    }
+    b->n_ejobs = (uint32_t)ej.size();
+    b->e_chunks = chunks;
+    if (!ej.empty()) {
+        if ((rc = upload(b, b->d_ejobs, ej))) return rc;
+        BCK(cudaMalloc(&b->d_epart, parts * sizeof(double)));
+    }
+
     // streams
     const uint32_t ns = std::max<uint32_t>(1, b->tune.streams);
     while (b->streams.size() < ns) {
@@ -1652,37 +1829,23 @@ int batch_prepare(qoa_batch_t b) {
         BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         b->events.push_back(ev);
     }
-    // arena for the large circuits: state, partials, scalars, status
-    const size_t esz = f32 ? sizeof(float2) : sizeof(double2);
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    size_t total = 0;
-    std::vector<size_t> off;
-    for (size_t i = 0; i < b->circs.size(); ++i) {
-        const auto& c = b->circs[i];
-        if (c.small) continue;
-        off.push_back(total);
-        total = al(total + (esz << c.n));
-        total = al(total + partials_needed(c.n) * sizeof(double));
-        total = al(total + 16 * sizeof(double));
-        total = al(total + 4 * sizeof(uint32_t));
-    }
-    if (total) BCK(cudaMalloc(&b->arena, total));
+
+    // view handles
     size_t k = 0;
     for (size_t i = 0; i < b->circs.size(); ++i) {
         auto& c = b->circs[i];
-        if (c.small) continue;
-        unsigned char* base = (unsigned char*)b->arena + off[k];
+        if (c.route != R_VIEW) continue;
+        unsigned char* base = arena + view_off[k];
         qoa_state_t v = new qoa_state_s();
         v->view = true;
         v->n = c.n;
         v->flags = b->flags & QOA_FLAG_COMPAT_MASK_QUIRK;
         v->precision = b->precision;
         v->device = b->device;
-        v->pass_budget = (int)b->tune.pass_gate_budget;
+        v->pass_budget = budget;
         v->stream = b->streams[k % ns];
+        v->amps = (double2*)(arena + c.state_off);
         size_t o = 0;
-        v->amps = (double2*)(base + o);
-        o = al(o + (esz << c.n));
         v->partials = (double*)(base + o);
         v->partials_cap = partials_needed(c.n);
         o = al(o + v->partials_cap * sizeof(double));
@@ -1691,7 +1854,7 @@ int batch_prepare(qoa_batch_t b) {
         v->status = (uint32_t*)(base + o);
         BCK(cudaMemset(v->status, 0, 4 * sizeof(uint32_t)));
         if (f32) {
-            int rc = f32_prepare(v, c.gates);
+            rc = f32_prepare(v, c.gates);
             if (rc) { std::string m = v->err; qoa_destroy(v); return bset_err(b, rc, m.c_str()); }
         }
         b->views.push_back(v);
@@ -1709,30 +1872,35 @@ int batch_enqueue(qoa_batch_t b) {
     const uint32_t ns = (uint32_t)b->streams.size();
     BCK(cudaEventRecord(b->events[0], s0));
     for (uint32_t i = 1; i < ns; ++i) BCK(cudaStreamWaitEvent(b->streams[i], b->events[0], 0));
+    // small circuits beside the arena rounds
+    if (b->nsmall) {
+        BCK(launch_small_batch(f32, b->d_small, b->nsmall, b->d_ops, b->d_masks, b->d_out, b->d_counter,
+                               (int)b->small_max_n_used, (int)b->tune.small_threads, (int)b->tune.small_ctas_per_sm,
+                               b->streams[ns > 1 ? 1 : 0]));
+    }
     for (size_t k = 0; k < b->views.size(); ++k) {
         qoa_state_t v = b->views[k];
         auto& c = b->circs[b->view_circ[k]];
         int rc = do_reset_all(v);
         if (!rc) rc = f32 ? f32_launch(v) : execute(v, c.gates);
         if (rc) return bset_err(b, rc, v->err.c_str());
-        for (size_t m = 0; m < c.masks.size(); m += 8) {
-            const uint32_t kk = (uint32_t)std::min<size_t>(8, c.masks.size() - m);
-            cudaError_t e = f32 ? launch_f32_expz((const float2*)v->amps, state_len(v), c.masks.data() + m, kk,
-                                                  v->partials, b->d_out + c.out_start + m, v->scal, v->stream)
-                                : launch_expz(v->amps, state_len(v), c.masks.data() + m, kk, v->partials,
-                                              b->d_out + c.out_start + m, v->scal, v->stream);
-            BCK(e);
-        }
     }
-    if (b->nsmall) {
-        BCK(launch_small_batch(f32, b->d_small, b->nsmall, b->d_ops, b->d_masks, b->d_out, b->d_counter,
-                               (int)b->small_max_n_used, (int)b->tune.small_threads, (int)b->tune.small_ctas_per_sm,
-                               s0));
+    const unsigned char* fb = (const unsigned char*)b->d_f32;
+    for (const auto& R : b->rounds) {
+        if (f32)
+            BCK(launch_f32_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
+                                      (const float*)(fb + b->f32_off[0]), (const F32PhaseOp*)(fb + b->f32_off[1]),
+                                      (const F32Angle*)(fb + b->f32_off[2]), (const F32Phase*)(fb + b->f32_off[3]),
+                                      (const float2*)(fb + b->f32_off[4]), s0));
+        else
+            BCK(launch_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles, R.max_nops,
+                                  R.max_ncoef, s0));
     }
     for (uint32_t i = 1; i < ns; ++i) {
         BCK(cudaEventRecord(b->events[i], b->streams[i]));
         BCK(cudaStreamWaitEvent(s0, b->events[i], 0));
     }
+    BCK(launch_arena_expz(f32, b->d_ejobs, b->n_ejobs, b->e_chunks, b->d_masks, b->d_epart, b->d_out, s0));
     return QOA_OK;
 }
 
@@ -1869,7 +2037,6 @@ int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome) {
 int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t* out) {
     int rc = check_handle(s);
     if (rc) return rc;
-    if (s->precision == QOA_PREC_F32) return set_err(s, QOA_E_ARG, "not available for an FP32 handle");
     if (!u || !out || (mode != 0 && mode != 1)) return set_err(s, QOA_E_ARG, "bad sample arguments");
     if (shots == 0) return QOA_OK;
     const uint32_t n = s->n;
@@ -1882,8 +2049,9 @@ int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t*
     CK(cudaMallocAsync(&d_u, nu * sizeof(double), s->stream));
     CK(cudaMallocAsync(&d_out, shots * sizeof(unsigned long long), s->stream));
     CK(cudaMemcpyAsync(d_u, u, nu * sizeof(double), cudaMemcpyHostToDevice, s->stream));
-    CK(launch_tree(s->amps, n, s->scal, d_tree, s->stream));
-    CK(launch_sample(s->amps, n, s->scal, d_tree, d_u, shots, mode, d_out, s->stream));
+    const bool f32 = s->precision == QOA_PREC_F32;
+    CK(launch_tree(s->amps, f32, n, s->scal, d_tree, s->stream));
+    CK(launch_sample(s->amps, f32, n, s->scal, d_tree, d_u, shots, mode, d_out, s->stream));
     s->launches += (n >= 2 ? (n - 1) : 0) + 1;
     CK(cudaMemcpyAsync(out, d_out, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaFreeAsync(d_tree, s->stream));
@@ -2175,12 +2343,14 @@ int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, con
     if (ex.first_err != QOA_OK) return bset_err(b, ex.first_err, ex.err.c_str());
     for (const Gate& g : ex.out)
         if (g.kind > K_U2) return bset_err(b, QOA_E_OPCODE, "batched circuits take unitary ops only");
+    if (nmasks > EXPZ_MAX_MASKS) return bset_err(b, QOA_E_ARG, "more than 255 masks on one circuit");
     qoa_batch_s::Circ c;
     c.n = n;
     c.gates = std::move(ex.out);
     c.masks.assign(zmasks, zmasks + nmasks);
     c.out_start = b->nresults;
-    c.small = false;
+    c.route = R_VIEW;
+    c.state_off = 0;
     b->nresults += (uint32_t)nmasks;
     if (id) *id = (uint32_t)b->circs.size();
     b->circs.push_back(std::move(c));
@@ -2214,29 +2384,34 @@ int qoa_batch_run(qoa_batch_t b) {
         int rc = batch_prepare(b);
         if (rc) return rc;
     }
-    if (!b->exec) {
-        // make every kernel attribute the captured launches need first
-        int rc = batch_enqueue(b);  // eager run (also the warm-up)
+    if (b->runs == 0) {
+        // first run: eager launches (a batch that runs once never pays for a graph)
+        int rc = batch_enqueue(b);
         if (rc) return rc;
         BCK(cudaStreamSynchronize(b->streams[0]));
+        b->runs++;
+        return QOA_OK;
+    }
+    if (!b->exec) {
+        // second run: capture the same launches into a graph, then replay it
         BCK(cudaStreamBeginCapture(b->streams[0], cudaStreamCaptureModeThreadLocal));
-        rc = batch_enqueue(b);
+        int rc = batch_enqueue(b);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(b->streams[0], &g);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         BCK(e);
         b->graph = g;
         BCK(cudaGraphInstantiate(&b->exec, g, 0));
-        return QOA_OK;
     }
     BCK(cudaGraphLaunch(b->exec, b->streams[0]));
     BCK(cudaStreamSynchronize(b->streams[0]));
+    b->runs++;
     return QOA_OK;
 }
 
 int qoa_batch_launch(qoa_batch_t b) {
     if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
-    if (!b->exec) return bset_err(b, QOA_E_ARG, "qoa_batch_launch replays the graph that the first qoa_batch_run makes");
+    if (!b->exec) return bset_err(b, QOA_E_ARG, "qoa_batch_launch replays the graph that the second qoa_batch_run makes");
     if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, QOA_E_CUDA, "cudaSetDevice failed");
     BCK(cudaGraphLaunch(b->exec, b->streams[0]));
     return QOA_OK;
@@ -2263,7 +2438,7 @@ int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t*
     if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
     if (circuits) *circuits = (uint32_t)b->circs.size();
     if (small) *small = b->nsmall;
-    if (large) *large = (uint32_t)b->views.size();
+    if (large) *large = b->narena + (uint32_t)b->views.size();
     if (graph_ready) *graph_ready = b->exec ? 1u : 0u;
     return QOA_OK;
 }

@@ -622,17 +622,24 @@ __global__ void k_probs(const double2* __restrict__ a, uint64_t off, uint64_t cn
 // --------------------------------------------------- marginal tree & shots
 // Level k (1 <= k <= n-1) holds h_k[p] = sum_{i mod 2^k == p} |a_i|^2 for
 // p < 2^k at offset 2^k - 2 of `tree`. Level n-1 comes from the amplitudes.
-__global__ void k_tree_leaf(const double2* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
+// |amplitude|^2 in FP64 for either storage precision
+__device__ __forceinline__ double amp2(const double2* a, uint64_t i) { return c_abs2(a[i]); }
+__device__ __forceinline__ double amp2(const float2* a, uint64_t i) {
+    const float2 x = a[i];
+    return (double)x.x * x.x + (double)x.y * x.y;
+}
+
+template <typename T>
+__global__ void k_tree_leaf(const T* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
                             double* __restrict__ lvl) {
     const uint64_t half = 1ull << (n - 1);
     const double nrm = *norm2_in;
     const bool valid = nrm > 1e-12;
     const double inv = valid ? 1.0 / nrm : 0.0;
     for (uint64_t p = gtid(); p < half; p += gstride()) {
-        lvl[p] = valid ? (c_abs2(a[p]) + c_abs2(a[p + half])) * inv : (p == 0 ? 1.0 : 0.0);
+        lvl[p] = valid ? (amp2(a, p) + amp2(a, p + half)) * inv : (p == 0 ? 1.0 : 0.0);
     }
 }
-
 __global__ void k_tree_up(const double* __restrict__ hi, double* __restrict__ lo, uint64_t cnt) {
     for (uint64_t p = gtid(); p < cnt; p += gstride()) lo[p] = hi[p] + hi[p + cnt];
 }
@@ -643,16 +650,17 @@ __global__ void k_tree_up(const double* __restrict__ hi, double* __restrict__ lo
 // probability <= 1e-12 zeroes the state, which normalize() then resets to
 // |0..0>, so every later outcome is 0 (quantum_state.rs:424-455, 888-907).
 // mode 1: inverse CDF with one uniform per shot, walking the same tree.
-__global__ void k_sample(const double2* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
+template <typename T>
+__global__ void k_sample(const T* __restrict__ a, uint32_t n, const double* __restrict__ norm2_in,
                          const double* __restrict__ tree, const double* __restrict__ u, uint64_t shots, int mode,
                          unsigned long long* __restrict__ out) {
     const double nrm = *norm2_in;
     const bool valid = nrm > 1e-12;
     const double inv = valid ? 1.0 / nrm : 0.0;
     auto h = [&](uint32_t k, uint64_t p) -> double {
-        if (k == n) return valid ? c_abs2(a[p]) * inv : (p == 0 ? 1.0 : 0.0);
+        if (k == n) return valid ? amp2(a, p) * inv : (p == 0 ? 1.0 : 0.0);
         if (k == 0) {
-            if (n == 1) return valid ? (c_abs2(a[0]) + c_abs2(a[1])) * inv : 1.0;
+            if (n == 1) return valid ? (amp2(a, 0) + amp2(a, 1)) * inv : 1.0;
             return tree[0] + tree[1];
         }
         return tree[((1ull << k) - 2) + p];
@@ -812,10 +820,12 @@ cudaError_t launch_probs(const double2* a, uint64_t off, uint64_t cnt, const dou
     return cudaGetLastError();
 }
 
-cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, double* tree, cudaStream_t st) {
+cudaError_t launch_tree(const void* a, bool f32, uint32_t n, const double* norm2, double* tree, cudaStream_t st) {
     if (n < 2) return cudaSuccess;
     double* leaf = tree + ((1ull << (n - 1)) - 2);
-    k_tree_leaf<<<grid_for(1ull << (n - 1), 256, 148 * 16), 256, 0, st>>>(a, n, norm2, leaf);
+    const int g = grid_for(1ull << (n - 1), 256, 148 * 16);
+    if (f32) k_tree_leaf<float2><<<g, 256, 0, st>>>((const float2*)a, n, norm2, leaf);
+    else k_tree_leaf<double2><<<g, 256, 0, st>>>((const double2*)a, n, norm2, leaf);
     for (uint32_t k = n - 2; k >= 1; --k) {
         const uint64_t cnt = 1ull << k;
         k_tree_up<<<grid_for(cnt, 256, 148 * 16), 256, 0, st>>>(tree + ((2ull << k) - 2), tree + (cnt - 2), cnt);
@@ -823,9 +833,11 @@ cudaError_t launch_tree(const double2* a, uint32_t n, const double* norm2, doubl
     return cudaGetLastError();
 }
 
-cudaError_t launch_sample(const double2* a, uint32_t n, const double* norm2, const double* tree, const double* u,
-                          uint64_t shots, int mode, unsigned long long* out, cudaStream_t st) {
-    k_sample<<<grid_for(shots, 128, 148 * 16), 128, 0, st>>>(a, n, norm2, tree, u, shots, mode, out);
+cudaError_t launch_sample(const void* a, bool f32, uint32_t n, const double* norm2, const double* tree,
+                          const double* u, uint64_t shots, int mode, unsigned long long* out, cudaStream_t st) {
+    const int g = grid_for(shots, 128, 148 * 16);
+    if (f32) k_sample<float2><<<g, 128, 0, st>>>((const float2*)a, n, norm2, tree, u, shots, mode, out);
+    else k_sample<double2><<<g, 128, 0, st>>>((const double2*)a, n, norm2, tree, u, shots, mode, out);
     return cudaGetLastError();
 }
 

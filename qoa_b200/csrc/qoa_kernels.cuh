@@ -9,6 +9,7 @@
 // means the logical state is |0..0>, which is what QuantumState::normalize
 // (src/runtime/quantum_state.rs:888-907) resets to.
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 #include <vector_types.h>
 
@@ -75,7 +76,8 @@ enum PassCode : uint8_t {
 // the interpreter loop reads; the condition words are read only by ops that
 // take conditions. Conditions: every listed bit must be 1 (controls of CNOT /
 // Toffoli / CY; masks of phase gates, CZ, CPHASE).
-struct PassOp {
+// 16-byte aligned: the pass kernels stage the op stream with 16-byte loads.
+struct alignas(16) PassOp {
     uint8_t code;
     uint8_t k;          // register bit of the op
     uint16_t coef;      // index into PassParams::coef; PC_XCHG: mapping index
@@ -111,9 +113,12 @@ struct PassParams {
     double2 coef[MAX_PASS_COEF];
 };
 
+static_assert(offsetof(PassParams, ops) % 16 == 0 && offsetof(PassParams, coef) % 16 == 0,
+              "the op stream and coefficients are staged with 16-byte loads");
+
 // One circuit's pass inside an arena launch: its state, the pass's parameters
-// (PassParams for complex128, F32ArenaPass for complex64), and whether this is
-// the circuit's first pass (input |0..0>, not read).
+// (PassParams for complex128, F32PassParams for complex64), and whether this
+// is the circuit's first pass (input |0..0>, not read).
 struct ArenaJob {
     void* amps;
     const void* params;

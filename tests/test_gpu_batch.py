@@ -39,11 +39,14 @@ def run_batch(circs, precision, **tuning):
             b.set_tuning(**tuning)
         for c in circs:
             b.add(c["n"], c["ops"], c["masks"])
-        b.run()
+        b.run()  # eager
         first = b.results()
-        info = b.info()
-        b.run()  # graph replay
+        b.run()  # captured into a graph, then launched
         second = b.results()
+        b.run()  # graph replay
+        third = b.results()
+        info = b.info()
+    assert np.array_equal(second, third)
     return first, second, info
 
 
@@ -106,8 +109,16 @@ def test_batch_layered_gates_and_empty():
     for n, seed in ((5, 1), (9, 2), (13, 3)):
         rng_circs.append({"n": n, "ops": C.random_layered(n, 3, seed), "masks": [1, (1 << n) - 1, 0b101]})
     rng_circs.append({"n": 7, "ops": [], "masks": [0b11, 0]})
-    first, _, _ = run_batch(rng_circs, "f64")
-    np.testing.assert_allclose(first, expected(rng_circs), rtol=0, atol=F64_TOL)
+    rng_circs.append({"n": 12, "ops": [], "masks": [0b11]})
+    # a SWAP is a per-gate step in complex128: that circuit takes the view route
+    rng_circs.append({"n": 13, "ops": C.random_layered(13, 2, 4) + [C.Op(C.SWAP, [0, 12])] + C.random_layered(13, 1, 5),
+                      "masks": [1, 1 << 12, 0b1000000000011]})
+    rng_circs.append({"n": 14, "ops": [], "masks": [1]})
+    ref = expected(rng_circs)
+    for prec, tol in (("f64", F64_TOL), ("f32", F32_TOL)):
+        first, second, info = run_batch(rng_circs, prec)
+        np.testing.assert_allclose(first, ref, rtol=0, atol=tol)
+        assert np.array_equal(first, second)
 
 
 @pytest.mark.gpu
