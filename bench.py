@@ -505,6 +505,72 @@ def run_batch(args):
     return 0
 
 
+def serve_requests(count: int, seed: int = 4, nmax: int = 28, dmax: int = 200):
+    """Serving workload: random layered circuits (gate mix of the layered
+    workload), n log-uniform in [10, nmax], depth uniform in [10, dmax],
+    depolarising p = 1e-3 per gate, 64 trajectories x 16 shots, seeded per
+    request; Poisson arrival gaps with mean 1/2000 s."""
+    import numpy as np
+    from qoa_b200 import circuits as C
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    for k in range(count):
+        n = int(np.floor(np.exp(rng.uniform(np.log(10), np.log(nmax + 1)))))
+        n = min(max(n, 10), nmax)
+        depth = int(rng.integers(10, dmax + 1))
+        t += float(rng.exponential(1.0 / 2000.0))
+        out.append(dict(n=n, depth=depth, ops=C.ops_to_array(C.random_layered(n, depth, 7000 + k)), noise_p=1e-3,
+                        trajectories=64, shots=16, seed=90000 + k, arrival=t))
+    return out
+
+
+def run_serve(args):
+    """Serving form: a bounded Poisson request stream through the continuous-
+    batching server, per precision. value = completed requests / (last
+    completion - first submission); p50 / p99 of submit-to-done latency."""
+    import numpy as np
+    import qoa_b200 as qb
+    reqs = serve_requests(args.serve_requests, nmax=args.serve_max_qubits, dmax=args.serve_max_depth)
+    out = {"metric": "circuits/s (served, 64 trajectories x 16 shots each), p50/p99 latency", "unit": "circuits/s",
+           "impl": "qoa_b200", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 0, "scaling": "weak",
+           "vs_baseline": None, "data": "synthetic (seeded random layered circuits, Poisson arrivals)",
+           "config": {"workload": f"{len(reqs)} requests, n log-uniform [10,{args.serve_max_qubits}], depth "
+                                  f"U[10,{args.serve_max_depth}], p=1e-3, 64 traj x 16 shots, mean arrival "
+                                  "2000 req/s, HBM budget 150 GB",
+                      "requests": len(reqs),
+                      "n_hist": np.bincount([r["n"] for r in reqs], minlength=41)[10:args.serve_max_qubits + 1].tolist(),
+                      "gates": int(sum(len(r["ops"]) for r in reqs))}}
+    for prec in args.precisions.split(","):
+        with qb.Server(prec, hbm_budget_gb=150, workers=args.serve_workers) as srv:
+            t0 = srv.now()
+            for r in reqs:
+                while srv.now() - t0 < r["arrival"]:
+                    time.sleep(max(0.0, min(0.001, r["arrival"] - (srv.now() - t0))))
+                srv.submit(r["n"], r["ops"], r["noise_p"], r["trajectories"], r["shots"], r["seed"])
+            res = []
+            while len(res) < len(reqs):
+                res += srv.poll(timeout_ms=1000)
+            st = srv.stats()
+            for x in res:
+                if x["status"] == 0:
+                    srv.take_shots(x["id"], int(x["shots"]))
+        lat = np.array([x["t_done"] - x["t_submit"] for x in res])
+        first = min(x["t_submit"] for x in res)
+        last = max(x["t_done"] for x in res)
+        out[prec] = {"value": len(res) / (last - first), "p50_latency_s": float(np.percentile(lat, 50)),
+                     "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": last - first,
+                     "failed": sum(1 for x in res if x["status"] != 0),
+                     "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": args.serve_workers,
+                     "ran_in": {"f64": sum(1 for x in res if x["precision"] == 0),
+                                "f32": sum(1 for x in res if x["precision"] == 1)}}
+    prim = args.precisions.split(",")[0]
+    out.update(value=out[prim]["value"], p50_latency_s=out[prim]["p50_latency_s"],
+               p99_latency_s=out[prim]["p99_latency_s"], dtype=prim)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,7 +585,11 @@ def main():
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
     ap.add_argument("--depth", type=int, default=20)
-    ap.add_argument("--workload", default="layered", choices=["layered", "qft", "batch"])
+    ap.add_argument("--workload", default="layered", choices=["layered", "qft", "batch", "serve"])
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-workers", type=int, default=16)
+    ap.add_argument("--serve-max-qubits", type=int, default=28)
+    ap.add_argument("--serve-max-depth", type=int, default=200)
     ap.add_argument("--qft-qubits", type=int, default=33)
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--precisions", default="f64,f32")
@@ -530,6 +600,8 @@ def main():
         return run_qft(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if (args.qubits, args.depth) != (30, 20):
         set_workload(args.qubits, args.depth)
     if args.impl == "reference":

@@ -232,6 +232,62 @@ int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t*
 const char* qoa_batch_last_error(qoa_batch_t b);
 int qoa_batch_destroy(qoa_batch_t b);
 
+/* ---- serving form (no reference counterpart) ----------------------------- */
+/* A request loop with continuous batching. Each request is a circuit with
+ * depolarising noise p per gate (QuantumState::apply_noise semantics,
+ * quantum_state.rs:839-885) run as `trajectories` stochastic Pauli
+ * trajectories of `shots_per_trajectory` inverse-CDF shots each. Trajectory t
+ * of a request with seed s draws its noise from counter-based stream t and
+ * its shot uniforms from stream t ^ 0x73686f74, so its result does not depend
+ * on scheduling or on the other requests. Worker threads (one trajectory each,
+ * one stream each) take the next trajectory of the oldest admitted request; a
+ * request is admitted when a worker is free and its state fits the HBM budget
+ * beside the states in use. States stay resident for reuse. With precision
+ * QOA_PREC_F32, requests under 11 qubits run in complex128. */
+typedef struct qoa_server_s* qoa_server_t;
+typedef struct qoa_server_config {
+    int precision;             /* QOA_PREC_F64 / QOA_PREC_F32 */
+    uint32_t flags;            /* handle flags (QOA_FLAG_COMPAT_MASK_QUIRK, ...) */
+    uint64_t hbm_budget_bytes; /* states + sampling scratch held at once */
+    uint32_t workers;          /* host threads = trajectories in flight */
+} qoa_server_config;
+typedef struct qoa_request {
+    uint32_t n;
+    const qoa_op* ops;         /* copied at submission */
+    size_t nops;
+    double noise_p;            /* depolarising probability per qubit per gate; 0 = ideal */
+    uint32_t trajectories;
+    uint32_t shots_per_trajectory;
+    uint64_t seed;
+} qoa_request;
+typedef struct qoa_request_result {
+    uint64_t id;
+    int status;                /* QOA_OK or the first error of its trajectories */
+    uint32_t n;
+    int precision;             /* precision it ran in */
+    double t_submit, t_admit, t_start, t_done; /* seconds on the server's clock */
+    uint64_t shots;            /* trajectories x shots_per_trajectory */
+} qoa_request_result;
+typedef struct qoa_server_stats {
+    uint64_t submitted, done, queued, admitted, trajectories_running, states_resident;
+    uint64_t bytes_reserved, peak_bytes_reserved;
+} qoa_server_stats;
+int qoa_server_create(const qoa_server_config* cfg, qoa_server_t* out);
+int qoa_server_submit(qoa_server_t s, const qoa_request* req, uint64_t* id);
+/* Finished requests (up to cap); waits up to timeout_ms (<0: forever) for one. */
+int qoa_server_poll(qoa_server_t s, qoa_request_result* out, size_t cap, size_t* got, int timeout_ms);
+/* Outcomes of a finished request in (trajectory, shot) order; releases them. */
+int qoa_server_take_shots(qoa_server_t s, uint64_t id, uint64_t* out, size_t cap);
+int qoa_server_get_stats(qoa_server_t s, qoa_server_stats* out);
+double qoa_server_now(qoa_server_t s);
+/* Waits for every submitted request, then stops the workers. */
+int qoa_server_destroy(qoa_server_t s);
+
+/* The engine's counter-based uniform in [0,1): Philox4x32-10 keyed by seed,
+ * counter (event lo, event hi, slot, stream); noise draws of trajectory t use
+ * stream t, slots 2q+1 (hit test) and 2q+2 (Pauli type) of gate event e. */
+double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32_t slot);
+
 /* ---- plan introspection (host only, no GPU needed) ---------------------- */
 /* Runs the pass scheduler on an op list for an n-qubit state and writes, for
  * each expanded gate in submission order, the index of the pass that applies

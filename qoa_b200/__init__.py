@@ -53,6 +53,28 @@ class BatchTuning(ctypes.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("flags", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_uint64),
+                ("workers", ctypes.c_uint32)]
+
+
+class RequestC(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("ops", ctypes.c_void_p), ("nops", ctypes.c_size_t),
+                ("noise_p", ctypes.c_double), ("trajectories", ctypes.c_uint32),
+                ("shots_per_trajectory", ctypes.c_uint32), ("seed", ctypes.c_uint64)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int), ("n", ctypes.c_uint32),
+                ("precision", ctypes.c_int), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_done", ctypes.c_double), ("shots", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "done", "queued", "admitted", "trajectories_running",
+                                               "states_resident", "bytes_reserved", "peak_bytes_reserved")]
+
+
 def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"qoa_b200: {LIB_PATH} is missing; build it with `make -C qoa_b200` "
@@ -96,6 +118,14 @@ def _load() -> ctypes.CDLL:
         "qoa_batch_info": (i32, [vp, P(u32), P(u32), P(u32), P(u32)]),
         "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
         "qoa_batch_destroy": (i32, [vp]),
+        "qoa_server_create": (i32, [P(ServerConfig), P(vp)]),
+        "qoa_server_submit": (i32, [vp, P(RequestC), P(u64)]),
+        "qoa_server_poll": (i32, [vp, P(RequestResult), sz, P(sz), i32]),
+        "qoa_server_take_shots": (i32, [vp, u64, vp, sz]),
+        "qoa_server_get_stats": (i32, [vp, P(ServerStats)]),
+        "qoa_server_now": (dbl, [vp]),
+        "qoa_server_destroy": (i32, [vp]),
+        "qoa_philox_uniform": (dbl, [u64, u32, u64, u32]),
         "qoa_plan": (i32, [u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, P(sz), P(sz)]),
         "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
         "qoa_vec_apply_x": (i32, [vp, sz, sz]),
@@ -470,6 +500,83 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             lib.qoa_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+SHOT_STREAM = 0x73686F74
+
+
+def philox_uniform(seed: int, stream: int, event: int, slot: int) -> float:
+    """The engine's counter-based uniform (Philox4x32-10; stream is 32-bit)."""
+    return lib.qoa_philox_uniform(seed, stream & 0xFFFFFFFF, event, slot)
+
+
+class Server:
+    """Serving form (qoa_server_*): a request loop with continuous batching.
+    Each request is a circuit with depolarising noise p per gate, run as
+    `trajectories` Pauli trajectories of `shots` inverse-CDF shots each;
+    trajectory t of a request seeded s uses counter-based streams t (noise)
+    and t ^ SHOT_STREAM (shot uniforms), so its outcomes do not depend on the
+    other requests or on scheduling. Admission is by HBM footprint."""
+
+    def __init__(self, precision: str = "f64", hbm_budget_gb: float = 150.0, workers: int = 16,
+                 compat_mask_quirk: bool = False):
+        cfg = ServerConfig(QOA_PREC_F32 if precision == "f32" else QOA_PREC_F64,
+                           QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0,
+                           int(hbm_budget_gb * (1 << 30)), int(workers))
+        h = ctypes.c_void_p()
+        rc = lib.qoa_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != QOA_OK:
+            raise QoaError(rc, (lib.qoa_last_error(None) or b"").decode())
+        self._h = h
+
+    def submit(self, n: int, ops, noise_p: float = 0.0, trajectories: int = 1, shots: int = 1,
+               seed: int = 0) -> int:
+        arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
+        req = RequestC(n, _ptr(arr) if len(arr) else None, len(arr), float(noise_p), int(trajectories), int(shots),
+                       int(seed))
+        rid = ctypes.c_uint64()
+        rc = lib.qoa_server_submit(self._h, ctypes.byref(req), ctypes.byref(rid))
+        if rc != QOA_OK:
+            raise QoaError(rc, (lib.qoa_last_error(None) or b"").decode())
+        return rid.value
+
+    def poll(self, timeout_ms: int = -1, cap: int = 256) -> list:
+        buf = (RequestResult * cap)()
+        got = ctypes.c_size_t()
+        _check(lib.qoa_server_poll(self._h, buf, cap, ctypes.byref(got), int(timeout_ms)))
+        return [{k: getattr(buf[i], k) for k, _ in RequestResult._fields_} for i in range(got.value)]
+
+    def take_shots(self, rid: int, count: int) -> np.ndarray:
+        out = np.zeros(count, dtype=np.uint64)
+        rc = lib.qoa_server_take_shots(self._h, rid, _ptr(out) if count else None, count)
+        if rc != QOA_OK:
+            raise QoaError(rc, (lib.qoa_last_error(None) or b"").decode())
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib.qoa_server_get_stats(self._h, ctypes.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in ServerStats._fields_}
+
+    def now(self) -> float:
+        return lib.qoa_server_now(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.qoa_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -2443,6 +2443,10 @@ int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t*
     return QOA_OK;
 }
 
+double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32_t slot) {
+    return uniform01(seed, stream, event, slot);
+}
+
 const char* qoa_batch_last_error(qoa_batch_t b) { return b ? b->err.c_str() : qoa_last_error(nullptr); }
 
 int qoa_batch_destroy(qoa_batch_t b) {

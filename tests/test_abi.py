@@ -32,3 +32,9 @@ def test_library_exports_every_declared_symbol():
 def test_strerror_is_callable_without_gpu():
     assert qoa_b200.lib.qoa_strerror(0) == b"ok"
     assert b"range" in qoa_b200.lib.qoa_strerror(1)
+
+
+def test_philox_uniform_matches_oracle():
+    from oracle import pyoracle as po
+    for seed, stream, event, slot in ((0, 0, 0, 0), (5, 7, 3, 1), (2**63 + 11, 0x73686F74 ^ 9, 2**40 + 3, 17)):
+        assert qoa_b200.philox_uniform(seed, stream, event, slot) == po.uniform(seed, stream, event, slot)
