@@ -288,6 +288,44 @@ int qoa_server_destroy(qoa_server_t s);
  * stream t, slots 2q+1 (hit test) and 2q+2 (Pauli type) of gate event e. */
 double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32_t slot);
 
+/* ---- bytecode front-end: .qexe / .qx programs -------------------------- */
+/* File = 4-byte magic ("QEXE","OEXE","QOX ","XEXE","QEX ","QX\0\0"), version
+ * byte, u32 LE payload length, payload (parse_exe_file, main.rs:1711-1745). */
+typedef struct qoa_exe_info {
+    char kind[8];              /* "qexe", "oexe", "qox", "xexe", "qex", "qx" */
+    uint32_t version;
+    uint32_t inferred_qubits;  /* `qoa run`'s qubit count: largest qubit byte + 1 (main.rs:3844-4226) */
+    uint64_t payload_offset;
+    uint64_t payload_len;
+} qoa_exe_info;
+typedef struct qoa_exe_result {
+    uint64_t instructions;     /* executed */
+    uint64_t gates;            /* quantum ops sent to the engine */
+    uint64_t measurements;
+    uint64_t chars_out;        /* CHAROUT */
+    uint64_t range_errors;     /* ops skipped for out-of-range qubits (printed, ignored upstream) */
+    uint64_t loop_errors;      /* LOOPEND without a pushed LOOPSTART */
+    uint64_t unknown_opcodes;  /* advanced by one byte, as upstream */
+    uint64_t unsupported;      /* QGATE names / rotation axes the executor skips */
+    uint32_t halted;           /* HALT or EXITCODE reached */
+    int32_t exit_code;
+    double registers[24];
+} qoa_exe_result;
+#define QOA_EXE_LOOPS 0x1      /* LOOPSTART n pushes n iterations (upstream pushes none) */
+/* Header + qubit-count scan; host only. */
+int qoa_exe_parse(const uint8_t* file, size_t len, qoa_exe_info* info);
+/* Runs a program on a complex128 handle (run_exe, main.rs:2314-3722); quantum
+ * instructions are batched into qoa_apply calls between measurements. Printed
+ * text (PRINT / PRINTLN / PRINTF / CHAROUT / DUMPREGS) goes to out_text
+ * (NUL-terminated, truncated to out_cap; *out_len = full length). max_steps
+ * bounds executed instructions (0 = none). */
+int qoa_exe_run(qoa_state_t s, const uint8_t* file, size_t len, uint32_t flags, uint64_t max_steps,
+                qoa_exe_result* res, char* out_text, size_t out_cap, size_t* out_len);
+/* The same interpreter without a state (host only): the op list a run would
+ * send, with every measurement outcome taken as 0. */
+int qoa_exe_trace(const uint8_t* file, size_t len, uint32_t flags, uint64_t max_steps, qoa_op* ops, size_t cap,
+                  size_t* nops, qoa_exe_result* res, char* out_text, size_t out_cap, size_t* out_len);
+
 /* ---- plan introspection (host only, no GPU needed) ---------------------- */
 /* Runs the pass scheduler on an op list for an n-qubit state and writes, for
  * each expanded gate in submission order, the index of the pass that applies
