@@ -326,6 +326,21 @@ int qoa_exe_run(qoa_state_t s, const uint8_t* file, size_t len, uint32_t flags, 
 int qoa_exe_trace(const uint8_t* file, size_t len, uint32_t flags, uint64_t max_steps, qoa_op* ops, size_t cap,
                   size_t* nops, qoa_exe_result* res, char* out_text, size_t out_cap, size_t* out_len);
 
+/* ---- checkpoint I/O ------------------------------------------------------- */
+/* Binary: the stored amplitudes and norm2 exactly ("QOAS" v1, checksummed),
+ * any size or precision; a save/load round trip is bit-exact. */
+int qoa_state_save(qoa_state_t s, const char* path);
+int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out);
+/* JSON in the reference's --save-state / --load-state layout: serde_json of
+ * (QuantumState, Vec<f64> registers) (main.rs:3800-3830, 4290-4300); up to
+ * 26 qubits. Loading makes a complex128 handle with the file's noise config
+ * and returns the registers. */
+int qoa_state_save_json(qoa_state_t s, const double* regs, size_t nregs, const char* path);
+int qoa_state_load_json(const char* path, uint32_t flags, qoa_state_t* out, double* regs, size_t regs_cap,
+                        size_t* nregs);
+int qoa_get_noise(qoa_state_t s, int* mode, double* p);
+int qoa_get_precision(qoa_state_t s, int* precision);
+
 /* ---- plan introspection (host only, no GPU needed) ---------------------- */
 /* Runs the pass scheduler on an op list for an n-qubit state and writes, for
  * each expanded gate in submission order, the index of the pass that applies

@@ -126,6 +126,12 @@ def _load() -> ctypes.CDLL:
         "qoa_server_now": (dbl, [vp]),
         "qoa_server_destroy": (i32, [vp]),
         "qoa_philox_uniform": (dbl, [u64, u32, u64, u32]),
+        "qoa_state_save": (i32, [vp, ctypes.c_char_p]),
+        "qoa_state_load": (i32, [ctypes.c_char_p, u32, P(vp)]),
+        "qoa_state_save_json": (i32, [vp, vp, sz, ctypes.c_char_p]),
+        "qoa_state_load_json": (i32, [ctypes.c_char_p, u32, P(vp), vp, sz, P(sz)]),
+        "qoa_get_noise": (i32, [vp, P(ctypes.c_int), P(dbl)]),
+        "qoa_get_precision": (i32, [vp, P(ctypes.c_int)]),
         "qoa_plan": (i32, [u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, P(sz), P(sz)]),
         "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
         "qoa_vec_apply_x": (i32, [vp, sz, sz]),
@@ -219,6 +225,51 @@ class QuantumState:
         self.seed_rng(seed)
         if noise_config is not None:
             self.set_noise_config(noise_config)
+
+    @classmethod
+    def _adopt(cls, h, precision: str, flags: int) -> "QuantumState":
+        self = cls.__new__(cls)
+        self.precision = precision
+        self._dtype = np.complex64 if precision == "f32" else np.complex128
+        self._h = h
+        self.flags = flags
+        self.noise_config = None
+        return self
+
+    # ---- checkpoints (--save-state / --load-state, main.rs:3800-3830, 4290-4300) ----
+    def save(self, path: str):
+        """Exact binary checkpoint (stored amplitudes + norm2)."""
+        _check(lib.qoa_state_save(self._h, os.fsencode(path)), self._h)
+
+    @classmethod
+    def load(cls, path: str, flags: int = 0) -> "QuantumState":
+        h = ctypes.c_void_p()
+        _check(lib.qoa_state_load(os.fsencode(path), flags, ctypes.byref(h)))
+        p = ctypes.c_int()
+        _check(lib.qoa_get_precision(h, ctypes.byref(p)), h)
+        return cls._adopt(h, "f32" if p.value == QOA_PREC_F32 else "f64", flags)
+
+    def save_json(self, path: str, registers: Sequence[float] = ()):
+        """The reference's serde JSON checkpoint of (QuantumState, registers)."""
+        r = np.ascontiguousarray(np.asarray(list(registers), dtype=np.float64))
+        _check(lib.qoa_state_save_json(self._h, _ptr(r) if len(r) else None, len(r), os.fsencode(path)), self._h)
+
+    @classmethod
+    def load_json(cls, path: str, flags: int = 0):
+        """(state, registers) from a reference JSON checkpoint."""
+        h = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        _check(lib.qoa_state_load_json(os.fsencode(path), flags, ctypes.byref(h), None, 0, ctypes.byref(n)))
+        lib.qoa_destroy(h)
+        regs = np.zeros(n.value, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(lib.qoa_state_load_json(os.fsencode(path), flags, ctypes.byref(h), _ptr(regs) if len(regs) else None,
+                                       len(regs), ctypes.byref(n)))
+        st = cls._adopt(h, "f64", flags)
+        m, p = ctypes.c_int(), ctypes.c_double()
+        _check(lib.qoa_get_noise(h, ctypes.byref(m), ctypes.byref(p)), h)
+        st.noise_config = [None, NoiseConfig.Fixed(p.value), NoiseConfig.Random()][m.value]
+        return st, regs
 
     # ---- lifetime -------------------------------------------------------
     def close(self):

@@ -2447,6 +2447,136 @@ double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32
     return uniform01(seed, stream, event, slot);
 }
 
+// ---- checkpoint I/O: exact binary dump of a handle's stored state ------------
+// Layout (little endian): "QOAS", u32 version 1, u32 precision, u32 n,
+// f64 norm2 (the stored vector's squared norm: the logical state is
+// stored / sqrt(norm2)), u64 amplitude bytes, the stored amplitudes, u64
+// checksum (sum of the payload's u64 words after mixing each with its index).
+// Saving does not normalise on the device and loading restores norm2 as it
+// was, so a round trip gives the same logical state bit for bit.
+namespace {
+constexpr size_t kCkptChunk = 64ull << 20;
+uint64_t ckpt_mix(uint64_t w, uint64_t i) {
+    uint64_t x = w ^ (i * 0x9E3779B97F4A7C15ull);
+    x ^= x >> 31;
+    x *= 0xBF58476D1CE4E5B9ull;
+    return x ^ (x >> 29);
+}
+}  // namespace
+
+int qoa_state_save(qoa_state_t s, const char* path) {
+    int rc = check_handle(s);
+    if (rc) return rc;
+    if (!path) return set_err(s, QOA_E_ARG, "null path");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return set_err(s, QOA_E_ARG, "cannot open %s for writing", path);
+    const size_t esz = s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2);
+    const uint64_t bytes = state_len(s) * esz;
+    CK(cudaMemcpyAsync(s->host_scal, s->scal, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const double norm2 = s->host_scal[0];
+    const uint32_t hdr[4] = {0x53414f51u /* "QOAS" */, 1u, (uint32_t)s->precision, s->n};
+    bool ok = std::fwrite(hdr, sizeof hdr, 1, f) == 1 && std::fwrite(&norm2, 8, 1, f) == 1 &&
+              std::fwrite(&bytes, 8, 1, f) == 1;
+    void* stage = nullptr;
+    if (ok && cudaMallocHost(&stage, kCkptChunk) != cudaSuccess) {
+        std::fclose(f);
+        return set_err(s, QOA_E_OOM, "pinned staging buffer");
+    }
+    uint64_t sum = 0, word = 0;
+    for (uint64_t off = 0; ok && off < bytes; off += kCkptChunk) {
+        const size_t k = (size_t)std::min<uint64_t>(kCkptChunk, bytes - off);
+        if (cudaMemcpyAsync(stage, (const unsigned char*)s->amps + off, k, cudaMemcpyDeviceToHost, s->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess) {
+            ok = false;
+            break;
+        }
+        const uint64_t* w = (const uint64_t*)stage;
+        for (size_t j = 0; j < k / 8; ++j) sum += ckpt_mix(w[j], word++);
+        ok = std::fwrite(stage, 1, k, f) == k;
+    }
+    if (stage) cudaFreeHost(stage);
+    ok = ok && std::fwrite(&sum, 8, 1, f) == 1;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return set_err(s, QOA_E_ARG, "writing %s failed", path);
+    return QOA_OK;
+}
+
+int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out) {
+    if (!path || !out) return set_err(nullptr, QOA_E_ARG, "null argument");
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return set_err(nullptr, QOA_E_ARG, "cannot open %s", path);
+    uint32_t hdr[4];
+    double norm2 = 0;
+    uint64_t bytes = 0;
+    if (std::fread(hdr, sizeof hdr, 1, f) != 1 || hdr[0] != 0x53414f51u || hdr[1] != 1u ||
+        std::fread(&norm2, 8, 1, f) != 1 || std::fread(&bytes, 8, 1, f) != 1) {
+        std::fclose(f);
+        return set_err(nullptr, QOA_E_ARG, "%s is not a version-1 state checkpoint", path);
+    }
+    const int prec = (int)hdr[2];
+    const uint32_t n = hdr[3];
+    const size_t esz = prec == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2);
+    if ((prec != QOA_PREC_F64 && prec != QOA_PREC_F32) || n < 1 || n > 40 || bytes != (esz << n)) {
+        std::fclose(f);
+        return set_err(nullptr, QOA_E_ARG, "%s: inconsistent checkpoint header", path);
+    }
+    qoa_state_t s = nullptr;
+    int rc = qoa_create(n, prec, flags, &s);
+    if (rc) {
+        std::fclose(f);
+        return rc;
+    }
+    void* stage = nullptr;
+    if (cudaMallocHost(&stage, kCkptChunk) != cudaSuccess) {
+        std::fclose(f);
+        qoa_destroy(s);
+        return set_err(nullptr, QOA_E_OOM, "pinned staging buffer");
+    }
+    uint64_t sum = 0, word = 0, want = 0;
+    bool ok = true;
+    for (uint64_t off = 0; ok && off < bytes; off += kCkptChunk) {
+        const size_t k = (size_t)std::min<uint64_t>(kCkptChunk, bytes - off);
+        ok = std::fread(stage, 1, k, f) == k;
+        if (!ok) break;
+        const uint64_t* w = (const uint64_t*)stage;
+        for (size_t j = 0; j < k / 8; ++j) sum += ckpt_mix(w[j], word++);
+        ok = cudaMemcpyAsync((unsigned char*)s->amps + off, stage, k, cudaMemcpyHostToDevice, s->stream) ==
+                 cudaSuccess &&
+             cudaStreamSynchronize(s->stream) == cudaSuccess;
+    }
+    cudaFreeHost(stage);
+    ok = ok && std::fread(&want, 8, 1, f) == 1 && want == sum;
+    std::fclose(f);
+    if (!ok) {
+        qoa_destroy(s);
+        return set_err(nullptr, QOA_E_ARG, "%s: truncated or corrupt checkpoint", path);
+    }
+    s->host_scal[0] = norm2;
+    if (cudaMemcpyAsync(s->scal, s->host_scal, sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        qoa_destroy(s);
+        return set_err(nullptr, QOA_E_CUDA, "restoring norm2 failed");
+    }
+    *out = s;
+    return QOA_OK;
+}
+
+int qoa_get_noise(qoa_state_t s, int* mode, double* p) {
+    if (!s || !mode || !p) return set_err(s, QOA_E_ARG, "null argument");
+    *mode = s->noise_mode;
+    *p = s->noise_p;
+    return QOA_OK;
+}
+
+int qoa_get_precision(qoa_state_t s, int* precision) {
+    if (!s || !precision) return set_err(s, QOA_E_ARG, "null argument");
+    *precision = s->precision;
+    return QOA_OK;
+}
+
 const char* qoa_batch_last_error(qoa_batch_t b) { return b ? b->err.c_str() : qoa_last_error(nullptr); }
 
 int qoa_batch_destroy(qoa_batch_t b) {
