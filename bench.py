@@ -361,13 +361,13 @@ def run_qft(args):
     ops_n = C.ops_to_array(C.qft(n))
     with qb.QuantumState(n, precision="f32", profile=True) as st:
         st.set_random_state(2)
-        ms, passes, bw, avg = timed(st, ops_n, args.steps, args.warmup, 2)
+        ms, passes, bw, avg = timed(st, ops_n, args.steps, args.warmup, 3)
     peak, src = measured_peaks()
-    out.update(value=len(ops_n) / (ms / 1e3), dtype="complex64 (3xTF32 tensor cores, FP32 accumulate)",
+    out.update(value=len(ops_n) / (ms / 1e3), dtype="complex64 (FP32 tile passes, FP64-built coefficients)",
                config={"workload": f"QFT n={n}", "gates": len(ops_n), "state_bytes": 8 << n},
                ms_per_step=ms, fp32_passes=passes,
                roofline={"bound": "hbm", "achieved": bw, "peak": peak, "unit": "GB/s",
-                         "frac": bw / peak if bw else None, "kernel": "k_f32_pass", "avg_launch_ms": avg,
+                         "frac": bw / peak if bw else None, "kernel": "k_pass<float2>", "avg_launch_ms": avg,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})"})
     m = n - 1
     ops_m = C.ops_to_array(C.qft(m))
@@ -376,18 +376,29 @@ def run_qft(args):
         ms64, p64, bw64, _ = timed(s64, ops_m, args.steps, args.warmup, 0)
     with qb.QuantumState(m, precision="f32", profile=True) as s32:
         s32.set_random_state(2)
-        ms32, p32, bw32, _ = timed(s32, ops_m, args.steps, args.warmup, 2)
+        ms32, p32, bw32, _ = timed(s32, ops_m, args.steps, args.warmup, 3)
+    with qb.QuantumState(m, precision="f32", profile=True, f32_tensor=True) as s32t:
+        s32t.set_random_state(2)
+        ms32t, p32t, bw32t, _ = timed(s32t, ops_m, args.steps, args.warmup, 2)
     # accuracy: one QFT from the same input on both precisions
-    with qb.QuantumState(m) as a, qb.QuantumState(m, precision="f32") as b:
-        a.set_random_state(2)
-        b.set_random_state(2)
-        a.execute(ops_m)
-        b.execute(ops_m)
-        rel, infid = b.compare(a)
+    acc = {}
+    for tensor in (False, True):
+        with qb.QuantumState(m) as a, qb.QuantumState(m, precision="f32", f32_tensor=tensor) as b:
+            a.set_random_state(2)
+            b.set_random_state(2)
+            a.execute(ops_m)
+            b.execute(ops_m)
+            acc[tensor] = b.compare(a)
     out.update(at_n_minus_1={"n": m, "fp64_gates_s": len(ops_m) / (ms64 / 1e3),
                              "fp32_gates_s": len(ops_m) / (ms32 / 1e3), "fp32_over_fp64": ms64 / ms32,
-                             "fp64_ms": ms64, "fp32_ms": ms32, "fp64_pass_launches": p64, "fp32_passes": p32,
-                             "fp32_rel_l2_vs_fp64": rel, "fp32_infidelity_vs_fp64": infid})
+                             "fp32_tensor_gates_s": len(ops_m) / (ms32t / 1e3),
+                             "fp32_tensor_over_fp64": ms64 / ms32t,
+                             "fp64_ms": ms64, "fp32_ms": ms32, "fp32_tensor_ms": ms32t,
+                             "fp64_pass_launches": p64, "fp32_pass_launches": p32, "fp32_tensor_passes": p32t,
+                             "fp64_pass_gbs": bw64, "fp32_pass_gbs": bw32, "fp32_tensor_pass_gbs": bw32t,
+                             "fp32_rel_l2_vs_fp64": acc[False][0], "fp32_infidelity_vs_fp64": acc[False][1],
+                             "fp32_tensor_rel_l2_vs_fp64": acc[True][0],
+                             "fp32_tensor_infidelity_vs_fp64": acc[True][1]})
     print(json.dumps(out), flush=True)
     return 0
 

@@ -58,9 +58,11 @@ extern "C" {
 
 /* ---- precision -------------------------------------------------------- */
 #define QOA_PREC_F64  0  /* complex128 amplitudes: the plain (drop-in) method */
-/* complex64 amplitudes, gates fused on the host (FP64) into dense blocks of
- * up to 5 qubits applied on the tensor cores (3xTF32, FP32 accumulation);
- * norms and probabilities stay FP64. Needs n >= 11; unitary ops only. */
+/* complex64 amplitudes: the same fused tile passes as complex128 (pass
+ * coefficients built in FP64 on the host, arithmetic in FP32, half the HBM
+ * bytes), or with QOA_FLAG_F32_TENSOR gates fused into dense blocks of up to
+ * 5 qubits on the tensor cores (3xTF32). Norms, probabilities and sampling
+ * stay FP64. Unitary ops only. */
 #define QOA_PREC_F32  1
 
 /* ---- handle flags ------------------------------------------------------ */
@@ -78,6 +80,10 @@ extern "C" {
 /* Depolarising noise only on the qubits the gate touched (the reference
  * applies it to every qubit after every gate, quantum_state.rs:872-885). */
 #define QOA_FLAG_NOISE_GATE_QUBITS  0x8u
+/* complex64 handles: fuse gates into dense <=5-qubit blocks applied on the
+ * tensor cores (3xTF32) instead of the default complex64 tile passes; needs
+ * n >= 11 */
+#define QOA_FLAG_F32_TENSOR         0x10u
 
 /* ---- opcodes: the reference byte code numbers (src/instructions.rs) ---- */
 #define QOA_OP_APPLYGATE   0x02  /* q[0]=qubit, q[1]= 'H','X','Y','Z','T','S' (execute_arithmetic APPLYGATE) */
@@ -216,6 +222,7 @@ typedef struct qoa_batch_tuning {
     uint32_t small_ctas_per_sm; /* its persistent grid = SMs x this */
     uint32_t streams;           /* streams the larger circuits spread over */
     uint32_t pass_gate_budget;  /* max gates per tile pass (fusion width); 0 = default */
+    uint32_t f32_tensor;        /* complex64 batches: 1 = dense tensor-core blocks, 0 = tile passes */
 } qoa_batch_tuning;
 int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out);
 int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, const uint64_t* zmasks, size_t nmasks,
@@ -243,7 +250,8 @@ int qoa_batch_destroy(qoa_batch_t b);
  * one stream each) take the next trajectory of the oldest admitted request; a
  * request is admitted when a worker is free and its state fits the HBM budget
  * beside the states in use. States stay resident for reuse. With precision
- * QOA_PREC_F32, requests under 11 qubits run in complex128. */
+ * QOA_PREC_F32 and QOA_FLAG_F32_TENSOR, requests under 11 qubits run in
+ * complex128. */
 typedef struct qoa_server_s* qoa_server_t;
 typedef struct qoa_server_config {
     int precision;             /* QOA_PREC_F64 / QOA_PREC_F32 */

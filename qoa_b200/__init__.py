@@ -28,6 +28,7 @@ QOA_OK, QOA_E_RANGE, QOA_E_ARG, QOA_E_OPCODE, QOA_E_CUDA, QOA_E_OOM, QOA_E_STATE
 QOA_PREC_F64 = 0
 QOA_PREC_F32 = 1
 QOA_FLAG_COMPAT_MASK_QUIRK = 0x1
+QOA_FLAG_F32_TENSOR = 0x10
 QOA_FLAG_PER_GATE = 0x2
 QOA_FLAG_PROFILE = 0x4
 QOA_FLAG_NOISE_GATE_QUBITS = 0x8
@@ -47,7 +48,7 @@ class QoaStatus(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("small_max_n", ctypes.c_uint32), ("small_threads", ctypes.c_uint32),
                 ("small_ctas_per_sm", ctypes.c_uint32), ("streams", ctypes.c_uint32),
-                ("pass_gate_budget", ctypes.c_uint32)]
+                ("pass_gate_budget", ctypes.c_uint32), ("f32_tensor", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -207,8 +208,10 @@ class QuantumState:
 
     def __init__(self, n_qubits: int, noise_config: Optional[NoiseConfig] = None, *,
                  compat_mask_quirk: bool = False, per_gate: bool = False, profile: bool = False,
-                 noise_gate_qubits_only: bool = False, seed: int = 0, precision: str = "f64"):
-        flags = ((QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0)
+                 noise_gate_qubits_only: bool = False, seed: int = 0, precision: str = "f64",
+                 f32_tensor: bool = False):
+        flags = ((QOA_FLAG_F32_TENSOR if f32_tensor else 0)
+                 | (QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0)
                  | (QOA_FLAG_PER_GATE if per_gate else 0)
                  | (QOA_FLAG_PROFILE if profile else 0)
                  | (QOA_FLAG_NOISE_GATE_QUBITS if noise_gate_qubits_only else 0))

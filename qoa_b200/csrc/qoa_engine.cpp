@@ -55,8 +55,11 @@ cudaError_t launch_f32_probs(const float2* a, uint64_t off, uint64_t cnt, const 
 cudaError_t launch_random_state(void* a, bool f32, uint64_t len, uint64_t seed, cudaStream_t st);
 cudaError_t launch_f32_expz(const float2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
                             double* out, const double* norm2, cudaStream_t st);
-cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
-                              int max_nops, int max_ncoef, cudaStream_t st);
+cudaError_t launch_pass_c64(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                            cudaStream_t st);
+cudaError_t launch_gate_c64(float2* a, uint64_t len, const GGate& g, cudaStream_t st);
+cudaError_t launch_pass_arena(bool c64, const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start,
+                              uint32_t tiles, int max_nops, int max_ncoef, cudaStream_t st);
 cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
                                   const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
                                   const F32Phase* phases, const float2* tables, cudaStream_t st);
@@ -1231,8 +1234,9 @@ GGate to_ggate(const Gate& g) {
 
 int run_gate(qoa_state_t s, const Gate& g) {
     const GGate k = to_ggate(g);
-    Timer tm(s, gate_bytes(g, s->n), 1);
-    CK(launch_gate(s->amps, state_len(s), k, s->stream));
+    Timer tm(s, gate_bytes(g, s->n) * (s->precision == QOA_PREC_F32 ? 0.5 : 1.0), 1);
+    if (s->precision == QOA_PREC_F32) CK(launch_gate_c64((float2*)s->amps, state_len(s), k, s->stream));
+    else CK(launch_gate(s->amps, state_len(s), k, s->stream));
     s->launches++;
     return QOA_OK;
 }
@@ -1247,7 +1251,10 @@ int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
         }
         return QOA_OK;
     }
-    {
+    if (s->precision == QOA_PREC_F32) {
+        Timer tm(s, 2.0 * std::ldexp(8.0, (int)s->n), 3);
+        CK(launch_pass_c64((float2*)s->amps, P, s->scal, s->partials, s->stream));
+    } else {
         Timer tm(s, 2.0 * std::ldexp(16.0, (int)s->n), 0);
         CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
     }
@@ -1404,7 +1411,12 @@ int execute_f32(qoa_state_t s, std::vector<Gate>& G) {
 }
 
 int execute(qoa_state_t s, std::vector<Gate>& G) {
-    if (s->precision == QOA_PREC_F32) return execute_f32(s, G);
+    const bool c64 = s->precision == QOA_PREC_F32;
+    if (c64 && (s->flags & QOA_FLAG_F32_TENSOR)) return execute_f32(s, G);
+    if (c64)
+        for (const Gate& g : G)
+            if (g.kind > K_U2 && g.kind != K_RESETALL)
+                return set_err(s, QOA_E_OPCODE, "the FP32 precision form takes unitary ops only");
     const bool per_gate = (s->flags & QOA_FLAG_PER_GATE) != 0;
     // Split at QINIT (changes n) and run each segment through the scheduler.
     size_t i = 0;
@@ -1659,6 +1671,7 @@ int batch_prepare(qoa_batch_t b) {
     const uint32_t smax = std::min<uint32_t>(b->tune.small_max_n, cap);
     const int budget = (int)b->tune.pass_gate_budget;
     const size_t esz = f32 ? sizeof(float2) : sizeof(double2);
+    const bool tensor = f32 && b->tune.f32_tensor;  // dense tensor-core blocks, else tile passes
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
 
     std::vector<SmallCircuit> sc;
@@ -1678,7 +1691,7 @@ int batch_prepare(qoa_batch_t b) {
     size_t total = 0;  // arena bytes
     for (size_t i = 0; i < b->circs.size(); ++i) {
         auto& c = b->circs[i];
-        bool small = c.n <= smax || (f32 && c.n < (uint32_t)TILE_BITS);
+        bool small = c.n <= smax || (tensor && c.n < (uint32_t)TILE_BITS);
         for (const Gate& g : c.gates) small = small && small_ok(g);
         if (small) {
             if (c.n > cap) return bset_err(b, QOA_E_ARG, "circuit too large for the shared-memory kernel");
@@ -1695,14 +1708,14 @@ int batch_prepare(qoa_batch_t b) {
             maxn = std::max(maxn, c.n);
             continue;
         }
-        if (f32 && c.n < (uint32_t)TILE_BITS)
+        if (tensor && c.n < (uint32_t)TILE_BITS)
             return bset_err(b, QOA_E_ARG, "circuit below the FP32 tile size with a gate the small kernel lacks");
         c.route = R_VIEW;
         if (c.n >= (uint32_t)TILE_BITS && !c.gates.empty()) {
-            std::vector<Step> steps = schedule(c.gates, c.n, false, f32, budget);
+            std::vector<Step> steps = schedule(c.gates, c.n, false, tensor, budget);
             bool ok = true;
             for (const Step& st : steps) ok = ok && st.pass;
-            if (ok && !f32) {
+            if (ok && !tensor) {
                 const size_t base = p64.size();
                 p64.resize(base + steps.size());
                 for (size_t k = 0; k < steps.size() && ok; ++k) ok = build_pass(c.gates, steps[k], c.n, p64[base + k]) == 0;
@@ -1716,7 +1729,7 @@ int batch_prepare(qoa_batch_t b) {
                     if (build_f32_pass(c.gates, steps[k], c.n, p32[base + k], up) != 0)
                         return bset_err(b, QOA_E_ARG, "FP32 pass does not fit one launch");
                 for (size_t k = 0; k < steps.size(); ++k) pass_idx[i].push_back((uint32_t)(base + k));
-            } else if (f32) {
+            } else if (tensor) {
                 return bset_err(b, QOA_E_OPCODE, "gate outside an FP32 pass");
             }
             if (ok) c.route = R_ARENA;
@@ -1747,13 +1760,13 @@ int batch_prepare(qoa_batch_t b) {
     unsigned char* arena = (unsigned char*)b->arena;
 
     // arena rounds
-    const size_t psz = f32 ? sizeof(F32PassParams) : sizeof(PassParams);
-    if (f32 ? !p32.empty() : !p64.empty()) {
-        BCK(cudaMalloc(&b->d_params, (f32 ? p32.size() : p64.size()) * psz));
-        BCK(cudaMemcpy(b->d_params, f32 ? (const void*)p32.data() : (const void*)p64.data(),
-                       (f32 ? p32.size() : p64.size()) * psz, cudaMemcpyHostToDevice));
+    const size_t psz = tensor ? sizeof(F32PassParams) : sizeof(PassParams);
+    if (tensor ? !p32.empty() : !p64.empty()) {
+        BCK(cudaMalloc(&b->d_params, (tensor ? p32.size() : p64.size()) * psz));
+        BCK(cudaMemcpy(b->d_params, tensor ? (const void*)p32.data() : (const void*)p64.data(),
+                       (tensor ? p32.size() : p64.size()) * psz, cudaMemcpyHostToDevice));
     }
-    if (f32 && !p32.empty()) {
+    if (tensor && !p32.empty()) {
         std::vector<unsigned char> img = f32_pack(up, b->f32_off);
         BCK(cudaMalloc(&b->d_f32, img.size()));
         BCK(cudaMemcpy(b->d_f32, img.data(), img.size(), cudaMemcpyHostToDevice));
@@ -1777,7 +1790,7 @@ int batch_prepare(qoa_batch_t b) {
             tstart.push_back(R.tiles);
             R.tiles += 1u << (c.n - TILE_BITS);
             R.njobs++;
-            if (!f32) {
+            if (!tensor) {
                 R.max_nops = std::max(R.max_nops, (int)p64[pi].nops);
                 R.max_ncoef = std::max(R.max_ncoef, (int)p64[pi].ncoef);
             }
@@ -1839,7 +1852,7 @@ int batch_prepare(qoa_batch_t b) {
         qoa_state_t v = new qoa_state_s();
         v->view = true;
         v->n = c.n;
-        v->flags = b->flags & QOA_FLAG_COMPAT_MASK_QUIRK;
+        v->flags = (b->flags & QOA_FLAG_COMPAT_MASK_QUIRK) | (tensor ? QOA_FLAG_F32_TENSOR : 0u);
         v->precision = b->precision;
         v->device = b->device;
         v->pass_budget = budget;
@@ -1853,7 +1866,7 @@ int batch_prepare(qoa_batch_t b) {
         o = al(o + 16 * sizeof(double));
         v->status = (uint32_t*)(base + o);
         BCK(cudaMemset(v->status, 0, 4 * sizeof(uint32_t)));
-        if (f32) {
+        if (tensor) {
             rc = f32_prepare(v, c.gates);
             if (rc) { std::string m = v->err; qoa_destroy(v); return bset_err(b, rc, m.c_str()); }
         }
@@ -1882,19 +1895,20 @@ int batch_enqueue(qoa_batch_t b) {
         qoa_state_t v = b->views[k];
         auto& c = b->circs[b->view_circ[k]];
         int rc = do_reset_all(v);
-        if (!rc) rc = f32 ? f32_launch(v) : execute(v, c.gates);
+        if (!rc) rc = (v->flags & QOA_FLAG_F32_TENSOR) ? f32_launch(v) : execute(v, c.gates);
         if (rc) return bset_err(b, rc, v->err.c_str());
     }
     const unsigned char* fb = (const unsigned char*)b->d_f32;
+    const bool tensor = f32 && b->tune.f32_tensor;
     for (const auto& R : b->rounds) {
-        if (f32)
+        if (tensor)
             BCK(launch_f32_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                       (const float*)(fb + b->f32_off[0]), (const F32PhaseOp*)(fb + b->f32_off[1]),
                                       (const F32Angle*)(fb + b->f32_off[2]), (const F32Phase*)(fb + b->f32_off[3]),
                                       (const float2*)(fb + b->f32_off[4]), s0));
         else
-            BCK(launch_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles, R.max_nops,
-                                  R.max_ncoef, s0));
+            BCK(launch_pass_arena(f32, b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
+                                  R.max_nops, R.max_ncoef, s0));
     }
     for (uint32_t i = 1; i < ns; ++i) {
         BCK(cudaEventRecord(b->events[i], b->streams[i]));
@@ -1935,8 +1949,8 @@ int qoa_create(uint32_t n, int precision, uint32_t flags, qoa_state_t* out) {
     *out = nullptr;
     if (precision != QOA_PREC_F64 && precision != QOA_PREC_F32)
         return set_err(nullptr, QOA_E_ARG, "unsupported precision %d", precision);
-    if (precision == QOA_PREC_F32 && n < (uint32_t)TILE_BITS)
-        return set_err(nullptr, QOA_E_ARG, "the FP32 precision form needs n >= %d", TILE_BITS);
+    if (precision == QOA_PREC_F32 && (flags & QOA_FLAG_F32_TENSOR) && n < (uint32_t)TILE_BITS)
+        return set_err(nullptr, QOA_E_ARG, "the tensor-core block form needs n >= %d", TILE_BITS);
     if (n < 1) n = 1;
     if (n > 40) return set_err(nullptr, QOA_E_ARG, "n=%u qubits exceeds the engine limit", n);
     int ndev = 0;
@@ -2323,6 +2337,7 @@ int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out) {
     b->tune.small_ctas_per_sm = 2;
     b->tune.streams = 8;
     b->tune.pass_gate_budget = 0;
+    b->tune.f32_tensor = 0;
     *out = b;
     return QOA_OK;
 }

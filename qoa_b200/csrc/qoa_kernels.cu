@@ -21,68 +21,87 @@
 namespace qoa {
 
 // ------------------------------------------------------------------ helpers
-__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
-    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+// Amplitudes are complex128 (double2, the plain method) or complex64 (float2,
+// the precision form's tile passes); one template serves both, arithmetic in
+// the amplitude's own precision.
+template <typename T> struct CT;
+template <> struct CT<double2> {
+    using R = double;
+    __device__ __forceinline__ static double2 mk(double x, double y) { return make_double2(x, y); }
+    __device__ __forceinline__ static double2 from(double2 c) { return c; }
+};
+template <> struct CT<float2> {
+    using R = float;
+    __device__ __forceinline__ static float2 mk(float x, float y) { return make_float2(x, y); }
+    __device__ __forceinline__ static float2 from(double2 c) { return make_float2((float)c.x, (float)c.y); }
+};
+
+template <typename T>
+__device__ __forceinline__ T c_mul(T a, T b) {
+    return CT<T>::mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
-__device__ __forceinline__ double2 c_neg(double2 a) { return make_double2(-a.x, -a.y); }
+template <typename T>
+__device__ __forceinline__ T c_neg(T a) { return CT<T>::mk(-a.x, -a.y); }
 __device__ __forceinline__ double c_abs2(double2 a) { return fma(a.x, a.x, a.y * a.y); }
+__device__ __forceinline__ double c_abs2(float2 a) { return (double)a.x * a.x + (double)a.y * a.y; }
 
 // 2x2 on the amplitude pair (a0 = bit 0, a1 = bit 1). G1_H is the exact
 // Hadamard (per-gate kernels); G1_HF drops its 1/sqrt2 (tile passes).
-template <int SUB>
-__device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 m0, const double2 m1,
-                                        const double2 m2, const double2 m3) {
+template <int SUB, typename T>
+__device__ __forceinline__ void g1_pair(T& a0, T& a1, const T m0, const T m1, const T m2, const T m3) {
+    using R = typename CT<T>::R;
+    auto mk = [](R x, R y) { return CT<T>::mk(x, y); };
     if (SUB == G1_H) {
-        const double f = m0.x;
-        const double sx = a0.x + a1.x, sy = a0.y + a1.y;
-        const double dx = a0.x - a1.x, dy = a0.y - a1.y;
-        a0 = make_double2(f * sx, f * sy);
-        a1 = make_double2(f * dx, f * dy);
+        const R f = m0.x;
+        const R sx = a0.x + a1.x, sy = a0.y + a1.y;
+        const R dx = a0.x - a1.x, dy = a0.y - a1.y;
+        a0 = mk(f * sx, f * sy);
+        a1 = mk(f * dx, f * dy);
     } else if (SUB == G1_HF) {
-        const double2 t = a0;
-        a0 = make_double2(t.x + a1.x, t.y + a1.y);
-        a1 = make_double2(t.x - a1.x, t.y - a1.y);
+        const T t = a0;
+        a0 = mk(t.x + a1.x, t.y + a1.y);
+        a1 = mk(t.x - a1.x, t.y - a1.y);
     } else if (SUB == G1_X) {
-        const double2 t = a0;
+        const T t = a0;
         a0 = a1;
         a1 = t;
     } else if (SUB == G1_Y) {
-        const double2 t = a0;
-        a0 = make_double2(a1.y, -a1.x);   // -i * a1
-        a1 = make_double2(-t.y, t.x);     //  i * a0
+        const T t = a0;
+        a0 = mk(a1.y, -a1.x);   // -i * a1
+        a1 = mk(-t.y, t.x);     //  i * a0
     } else if (SUB == G1_RX) {
-        const double c = m0.x, s = m0.y;
-        const double2 t = a0;
-        a0 = make_double2(fma(c, t.x, s * a1.y), fma(c, t.y, -s * a1.x));
-        a1 = make_double2(fma(s, t.y, c * a1.x), fma(-s, t.x, c * a1.y));
+        const R c = m0.x, s = m0.y;
+        const T t = a0;
+        a0 = mk(fma(c, t.x, s * a1.y), fma(c, t.y, -s * a1.x));
+        a1 = mk(fma(s, t.y, c * a1.x), fma(-s, t.x, c * a1.y));
     } else if (SUB == G1_RY) {
-        const double c = m0.x, s = m0.y;
-        const double2 t = a0;
-        a0 = make_double2(fma(c, t.x, -s * a1.x), fma(c, t.y, -s * a1.y));
-        a1 = make_double2(fma(s, t.x, c * a1.x), fma(s, t.y, c * a1.y));
+        const R c = m0.x, s = m0.y;
+        const T t = a0;
+        a0 = mk(fma(c, t.x, -s * a1.x), fma(c, t.y, -s * a1.y));
+        a1 = mk(fma(s, t.x, c * a1.x), fma(s, t.y, c * a1.y));
     } else if (SUB == G1_RXA) {
-        const double t = m0.x;
-        const double2 u = a0;
-        a0 = make_double2(fma(t, a1.y, u.x), fma(-t, a1.x, u.y));
-        a1 = make_double2(fma(t, u.y, a1.x), fma(-t, u.x, a1.y));
+        const R t = m0.x;
+        const T u = a0;
+        a0 = mk(fma(t, a1.y, u.x), fma(-t, a1.x, u.y));
+        a1 = mk(fma(t, u.y, a1.x), fma(-t, u.x, a1.y));
     } else if (SUB == G1_RXB) {
-        const double r = m0.x;
-        const double2 u = a0;
-        a0 = make_double2(fma(r, u.x, a1.y), fma(r, u.y, -a1.x));
-        a1 = make_double2(fma(r, a1.x, u.y), fma(r, a1.y, -u.x));
+        const R r = m0.x;
+        const T u = a0;
+        a0 = mk(fma(r, u.x, a1.y), fma(r, u.y, -a1.x));
+        a1 = mk(fma(r, a1.x, u.y), fma(r, a1.y, -u.x));
     } else if (SUB == G1_RYA) {
-        const double t = m0.x;
-        const double2 u = a0;
-        a0 = make_double2(fma(-t, a1.x, u.x), fma(-t, a1.y, u.y));
-        a1 = make_double2(fma(t, u.x, a1.x), fma(t, u.y, a1.y));
+        const R t = m0.x;
+        const T u = a0;
+        a0 = mk(fma(-t, a1.x, u.x), fma(-t, a1.y, u.y));
+        a1 = mk(fma(t, u.x, a1.x), fma(t, u.y, a1.y));
     } else if (SUB == G1_RYB) {
-        const double r = m0.x;
-        const double2 u = a0;
-        a0 = make_double2(fma(r, u.x, -a1.x), fma(r, u.y, -a1.y));
-        a1 = make_double2(fma(r, a1.x, u.x), fma(r, a1.y, u.y));
+        const R r = m0.x;
+        const T u = a0;
+        a0 = mk(fma(r, u.x, -a1.x), fma(r, u.y, -a1.y));
+        a1 = mk(fma(r, a1.x, u.x), fma(r, a1.y, u.y));
     } else {
-        const double2 t = a0;
-        double2 r0 = c_mul(m0, t), r1 = c_mul(m2, t);
+        const T t = a0;
+        T r0 = c_mul(m0, t), r1 = c_mul(m2, t);
         r0.x = fma(m1.x, a1.x, r0.x); r0.x = fma(-m1.y, a1.y, r0.x);
         r0.y = fma(m1.x, a1.y, r0.y); r0.y = fma(m1.y, a1.x, r0.y);
         r1.x = fma(m3.x, a1.x, r1.x); r1.x = fma(-m3.y, a1.y, r1.x);
@@ -93,9 +112,9 @@ __device__ __forceinline__ void g1_pair(double2& a0, double2& a1, const double2 
 }
 
 // ------------------------------------------------- tile pass building blocks
-template <int SUB, int K>
-__device__ __forceinline__ void g1r(double2 (&a)[REGS], const double2* __restrict__ m) {
-    double2 m0 = make_double2(0, 0), m1 = m0, m2 = m0, m3 = m0;
+template <int SUB, int K, typename T>
+__device__ __forceinline__ void g1r(T (&a)[REGS], const T* __restrict__ m) {
+    T m0 = CT<T>::mk(0, 0), m1 = m0, m2 = m0, m3 = m0;
     if (SUB != G1_HF && SUB != G1_X && SUB != G1_Y) m0 = m[0];
     if (SUB == G1_GEN) { m1 = m[1]; m2 = m[2]; m3 = m[3]; }
 #pragma unroll
@@ -104,16 +123,17 @@ __device__ __forceinline__ void g1r(double2 (&a)[REGS], const double2* __restric
 }
 
 // X / Y where every condition bit is set (tp: lane / warp / outer part)
-template <int SUB, int K>
-__device__ __forceinline__ void g1rc(double2 (&a)[REGS], bool tp, uint32_t creg) {
+template <int SUB, int K, typename T>
+__device__ __forceinline__ void g1rc(T (&a)[REGS], bool tp, uint32_t creg) {
     if (!tp) return;
-    const double2 z = make_double2(0, 0);
+    const T z = CT<T>::mk(0, 0);
 #pragma unroll
     for (int v = 0; v < REGS; ++v)
         if (!(v & (1 << K)) && (v & creg) == creg) g1_pair<SUB>(a[v], a[v | (1 << K)], z, z, z, z);
 }
 
-__device__ __forceinline__ void diag_m(double2 (&a)[REGS], bool tp, uint32_t creg, double2 d) {
+template <typename T>
+__device__ __forceinline__ void diag_m(T (&a)[REGS], bool tp, uint32_t creg, T d) {
     if (!tp) return;
 #pragma unroll
     for (int v = 0; v < REGS; ++v)
@@ -134,10 +154,15 @@ __device__ __forceinline__ uint64_t tstride(const PassParams& P, uint32_t t) {
 // One CTA's tile of one pass. `blk` numbers the tile (its bits go to the
 // qubits outside the tile); `nrm` is the input's squared norm (<= 1e-12: the
 // input is |0..0>, synthesised without reading); `partial_out`, when not
-// null, receives the tile's squared norm after the pass.
-__device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const PassParams& P, const double nrm,
+// null, receives the tile's squared norm after the pass. The pass's
+// coefficients are built in FP64 on the host; a complex64 pass rounds them
+// once when it stages them.
+template <typename T>
+__device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams& P, const double nrm,
                                           const uint64_t blk, double* __restrict__ partial_out) {
-    extern __shared__ double2 tile[];
+    using R = typename CT<T>::R;
+    extern __shared__ __align__(16) unsigned char pass_smem[];
+    T* tile = reinterpret_cast<T*>(pass_smem);
     __shared__ double red[PASS_THREADS / 32];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
@@ -154,21 +179,22 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
     // op stream and coefficients -> shared memory (after the tile)
     const uint32_t nops = P.nops;
     uint4* sops = reinterpret_cast<uint4*>(tile + (1 << TILE_BITS));
-    double2* scoef = reinterpret_cast<double2*>(sops + nops);
+    T* scoef = reinterpret_cast<T*>(sops + nops);
     {
         const uint4* gops = reinterpret_cast<const uint4*>(P.ops);
         for (uint32_t i = threadIdx.x; i < nops; i += PASS_THREADS) sops[i] = gops[i];
-        for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS) scoef[i] = P.coef[i];
+        for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS) scoef[i] = CT<T>::from(P.coef[i]);
     }
 
     const bool valid = nrm > 1e-12;
     // The input's 1/||psi|| and the pass's factored global phase are applied
     // once, at the end, as part of the per-thread pending factor.
-    double2 pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;
+    T pend = valid ? CT<T>::from(make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)))
+                   : CT<T>::from(P.phase);
 
     // Load with the initial mapping: lanes are tile bits 0..4 = qubits 0..4,
-    // so each warp reads 512 contiguous bytes per register.
-    double2 a[REGS];
+    // so each warp reads 32 consecutive amplitudes per register.
+    T a[REGS];
     {
         uint64_t tb = g0 + (uint64_t)lane;
 #pragma unroll
@@ -183,7 +209,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
 #pragma unroll
             for (int k = 0; k < REG_BITS; ++k)
                 if ((v >> k) & 1) g += rst[k];
-            a[v] = valid ? __ldcs(amps + g) : make_double2(g == 0 ? 1.0 : 0.0, 0.0);
+            a[v] = valid ? __ldcs(amps + g) : CT<T>::mk(g == 0 ? (R)1 : (R)0, (R)0);
         }
     }
     __syncthreads();  // op stream staged
@@ -195,7 +221,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
         const uint32_t hot = w;
         if (oi + 1 < nops) w = ow[4 * (oi + 1)];
         const uint32_t code = hot & 0xffu;
-        const double2* m = scoef + (hot >> 16);
+        const T* m = scoef + (hot >> 16);
         // condition of ops that take one: register mask and thread predicate
         auto conds = [&](bool& tp) -> uint32_t {
             const uint32_t cw = ow[4 * oi + 1];
@@ -239,7 +265,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
                 // folds its thread-conditioned factors into one scalar, then
                 // multiplies the matching registers once
                 const uint32_t cnt = (hot >> 8) & 0xffu;
-                double2 f = make_double2(1.0, 0.0);
+                T f = CT<T>::mk(1, 0);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
                     bool tp = true;
@@ -253,7 +279,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
                     const bool last = (e == cnt) || ((sops[oi + e + 1].y & 0xffu) != (cw & 0xffu));
                     if (last) {
                         diag_m(a, true, cw & 0xffu, f);
-                        f = make_double2(1.0, 0.0);
+                        f = CT<T>::mk(1, 0);
                     }
                 }
                 oi += cnt;
@@ -267,7 +293,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
             case PC_DIAG_TM: {
                 // entries oi+1 .. oi+cnt: independent factors, multiplied in
                 const uint32_t cnt = (hot >> 8) & 0xffu;
-                double2 f = make_double2(1.0, 0.0);
+                T f = CT<T>::mk(1, 0);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
                     bool tp = true;
@@ -287,7 +313,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
             case PC_FLUSH:
 #pragma unroll
                 for (int v = 0; v < REGS; ++v) a[v] = c_mul(a[v], pend);
-                pend = make_double2(1.0, 0.0);
+                pend = CT<T>::mk(1, 0);
                 break;
             case PC_XCHG: {
                 // write under the current mapping, read under the new one
@@ -359,7 +385,7 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
 #pragma unroll
             for (int k = 0; k < REG_BITS; ++k)
                 if ((v >> k) & 1) g += rst[k];
-            const double2 x = c_mul(a[v], pend);
+            const T x = c_mul(a[v], pend);
             __stcs(amps + g, x);
             ss += c_abs2(x);
         }
@@ -377,10 +403,16 @@ __device__ __forceinline__ void pass_tile(double2* __restrict__ amps, const Pass
     }
 }
 
-__global__ void __launch_bounds__(PASS_THREADS, 4)
-k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
+// Resident CTAs per SM: the complex128 pass needs 128 registers a thread,
+// the complex64 one fits five CTAs.
+template <typename T> struct PassOcc { static constexpr int value = 4; };
+template <> struct PassOcc<float2> { static constexpr int value = 5; };
+
+template <typename T>
+__global__ void __launch_bounds__(PASS_THREADS, PassOcc<T>::value)
+k_pass(T* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
        double* __restrict__ partials) {
-    pass_tile(amps, P, *norm2_in, blockIdx.x, partials + blockIdx.x);
+    pass_tile<T>(amps, P, *norm2_in, blockIdx.x, partials + blockIdx.x);
 }
 
 // Arena pass: one launch runs one pass of each of many circuits, whose states
@@ -388,7 +420,8 @@ k_pass(double2* __restrict__ amps, const __grid_constant__ PassParams P, const d
 // j is the last job with tile_start[j] <= b. Squared norms are not tracked: a
 // batched circuit is unitary, its start |0..0> is synthesised by its first
 // pass, and its consumers normalise.
-__global__ void __launch_bounds__(PASS_THREADS, 4)
+template <typename T>
+__global__ void __launch_bounds__(PASS_THREADS, PassOcc<T>::value)
 k_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ tile_start) {
     const uint32_t b = blockIdx.x;
     uint32_t lo = 0, hi = njobs - 1;
@@ -398,8 +431,8 @@ k_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* 
         else hi = mid - 1;
     }
     const ArenaJob J = jobs[lo];
-    pass_tile(reinterpret_cast<double2*>(J.amps), *reinterpret_cast<const PassParams*>(J.params),
-              J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr);
+    pass_tile<T>(reinterpret_cast<T*>(J.amps), *reinterpret_cast<const PassParams*>(J.params),
+                 J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr);
 }
 
 // ------------------------------------------------------- per-gate kernels
@@ -408,63 +441,67 @@ k_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* 
 __device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
 
-template <int SUB>
-__global__ void k_gate_g1(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+template <int SUB, typename T>
+__global__ void k_gate_g1(T* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
     const uint64_t bit = 1ull << g.t;
-    const double2 m0 = g.m[0], m1 = g.m[1], m2 = g.m[2], m3 = g.m[3];
+    const T m0 = CT<T>::from(g.m[0]), m1 = CT<T>::from(g.m[1]), m2 = CT<T>::from(g.m[2]), m3 = CT<T>::from(g.m[3]);
     for (uint64_t i = gtid(); i < len; i += gstride()) {
         if (i & bit) continue;
         const uint64_t j = i | bit;
         if (j >= len || (i & g.cmask) != g.cmask) continue;
-        double2 x = a[i], y = a[j];
+        T x = a[i], y = a[j];
         g1_pair<SUB>(x, y, m0, m1, m2, m3);
         a[i] = x;
         a[j] = y;
     }
 }
 
-__global__ void k_gate_diag(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+template <typename T>
+__global__ void k_gate_diag(T* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
     const bool neg = (g.sub & 0x80u) != 0;
     const bool has_sel = g.t < 64;
+    const T d0 = CT<T>::from(g.m[0]), d1 = CT<T>::from(g.m[1]);
     for (uint64_t i = gtid(); i < len; i += gstride()) {
         if ((i & g.cmask) != g.cmask) continue;
         if (neg) {
             a[i] = c_neg(a[i]);
         } else {
             const bool s = has_sel && ((i >> g.t) & 1ull);
-            a[i] = c_mul(a[i], s ? g.m[1] : g.m[0]);
+            a[i] = c_mul(a[i], s ? d1 : d0);
         }
     }
 }
 
-__global__ void k_gate_swap(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+template <typename T>
+__global__ void k_gate_swap(T* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
     const uint64_t m1 = 1ull << g.t, m2 = 1ull << g.t2;
     for (uint64_t i = gtid(); i < len; i += gstride()) {
         if ((i & (m1 | m2)) != 0 || (i & g.cmask) != g.cmask) continue;
         const uint64_t x = i | m2, y = i | m1;
         if (x < len && y < len) {
-            const double2 t = a[x];
+            const T t = a[x];
             a[x] = a[y];
             a[y] = t;
         }
     }
 }
 
-__global__ void k_gate_u2(double2* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
+template <typename T>
+__global__ void k_gate_u2(T* __restrict__ a, uint64_t len, const __grid_constant__ GGate g) {
     const uint64_t ml = 1ull << g.t, mh = 1ull << g.t2;
     for (uint64_t i = gtid(); i < len; i += gstride()) {
         if ((i & (ml | mh)) != 0) continue;
         const uint64_t idx[4] = {i, i | ml, i | mh, i | ml | mh};
         if (idx[3] >= len) continue;
-        double2 x[4];
+        T x[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) x[k] = a[idx[k]];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            double2 acc = c_mul(g.m[4 * r], x[0]);
+            T acc = c_mul(CT<T>::from(g.m[4 * r]), x[0]);
 #pragma unroll
             for (int k = 1; k < 4; ++k) {
-                const double2 c = g.m[4 * r + k];
+                const T c = CT<T>::from(g.m[4 * r + k]);
                 acc.x = fma(c.x, x[k].x, acc.x); acc.x = fma(-c.y, x[k].y, acc.x);
                 acc.y = fma(c.x, x[k].y, acc.y); acc.y = fma(c.y, x[k].x, acc.y);
             }
@@ -473,8 +510,9 @@ __global__ void k_gate_u2(double2* __restrict__ a, uint64_t len, const __grid_co
     }
 }
 
-__global__ void k_reset_all(double2* __restrict__ a, uint64_t len) {
-    for (uint64_t i = gtid(); i < len; i += gstride()) a[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+template <typename T>
+__global__ void k_reset_all(T* __restrict__ a, uint64_t len) {
+    for (uint64_t i = gtid(); i < len; i += gstride()) a[i] = CT<T>::mk(i == 0 ? 1 : 0, 0);
 }
 
 // --------------------------------------------------------------- reductions
@@ -701,50 +739,69 @@ static int grid_for(uint64_t work, int threads, int max_blocks) {
     return (int)b;
 }
 
-cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
-                        cudaStream_t st) {
-    const int smem = (1 << TILE_BITS) * (int)sizeof(double2) + (int)P.nops * 16 + (int)P.ncoef * 16;
-    cudaError_t e = cudaFuncSetAttribute(k_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (1 << TILE_BITS) * (int)sizeof(double2) + MAX_PASS_OPS * 16 + MAX_PASS_COEF * 16);
+template <typename T>
+static cudaError_t launch_pass_t(T* amps, const PassParams& P, const double* norm2_in, double* partials,
+                                 cudaStream_t st) {
+    const int tile_bytes = (1 << TILE_BITS) * (int)sizeof(T);
+    const int smem = tile_bytes + (int)P.nops * 16 + (int)P.ncoef * (int)sizeof(T);
+    cudaError_t e = cudaFuncSetAttribute(k_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tile_bytes + MAX_PASS_OPS * 16 + MAX_PASS_COEF * (int)sizeof(T));
     if (e != cudaSuccess) return e;
     const unsigned blocks = 1u << (P.n - TILE_BITS);
-    k_pass<<<blocks, PASS_THREADS, smem, st>>>(amps, P, norm2_in, partials);
+    k_pass<T><<<blocks, PASS_THREADS, smem, st>>>(amps, P, norm2_in, partials);
     return cudaGetLastError();
 }
-
-cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
-                              int max_nops, int max_ncoef, cudaStream_t st) {
+cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                        cudaStream_t st) {
+    return launch_pass_t<double2>(amps, P, norm2_in, partials, st);
+}
+cudaError_t launch_pass_c64(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                            cudaStream_t st) {
+    return launch_pass_t<float2>(amps, P, norm2_in, partials, st);
+}
+cudaError_t launch_pass_arena(bool c64, const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start,
+                              uint32_t tiles, int max_nops, int max_ncoef, cudaStream_t st) {
     if (!njobs || !tiles) return cudaSuccess;
-    const int smem = (1 << TILE_BITS) * (int)sizeof(double2) + max_nops * 16 + max_ncoef * 16;
-    cudaError_t e = cudaFuncSetAttribute(k_pass_arena, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (1 << TILE_BITS) * (int)sizeof(double2) + MAX_PASS_OPS * 16 + MAX_PASS_COEF * 16);
+    const int esz = c64 ? (int)sizeof(float2) : (int)sizeof(double2);
+    const int tile_bytes = (1 << TILE_BITS) * esz;
+    const int smem = tile_bytes + max_nops * 16 + max_ncoef * esz;
+    const int smax = tile_bytes + MAX_PASS_OPS * 16 + MAX_PASS_COEF * esz;
+    cudaError_t e = c64 ? cudaFuncSetAttribute(k_pass_arena<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)
+                        : cudaFuncSetAttribute(k_pass_arena<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
     if (e != cudaSuccess) return e;
-    k_pass_arena<<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
+    if (c64) k_pass_arena<float2><<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
+    else k_pass_arena<double2><<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
     return cudaGetLastError();
 }
-
-cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st) {
+template <typename T>
+static cudaError_t launch_gate_t(T* a, uint64_t len, const GGate& g, cudaStream_t st) {
     const int threads = 256;
     const int blocks = grid_for(len, threads, 148 * 16);
     switch (g.kind) {
         case GG_G1:
             switch (g.sub) {
-                case G1_H: k_gate_g1<G1_H><<<blocks, threads, 0, st>>>(a, len, g); break;
-                case G1_HF: k_gate_g1<G1_HF><<<blocks, threads, 0, st>>>(a, len, g); break;
-                case G1_X: k_gate_g1<G1_X><<<blocks, threads, 0, st>>>(a, len, g); break;
-                case G1_Y: k_gate_g1<G1_Y><<<blocks, threads, 0, st>>>(a, len, g); break;
-                case G1_RX: k_gate_g1<G1_RX><<<blocks, threads, 0, st>>>(a, len, g); break;
-                case G1_RY: k_gate_g1<G1_RY><<<blocks, threads, 0, st>>>(a, len, g); break;
-                default: k_gate_g1<G1_GEN><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_H: k_gate_g1<G1_H, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_HF: k_gate_g1<G1_HF, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_X: k_gate_g1<G1_X, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_Y: k_gate_g1<G1_Y, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_RX: k_gate_g1<G1_RX, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                case G1_RY: k_gate_g1<G1_RY, T><<<blocks, threads, 0, st>>>(a, len, g); break;
+                default: k_gate_g1<G1_GEN, T><<<blocks, threads, 0, st>>>(a, len, g); break;
             }
             break;
-        case GG_DIAG: k_gate_diag<<<blocks, threads, 0, st>>>(a, len, g); break;
-        case GG_SWAP: k_gate_swap<<<blocks, threads, 0, st>>>(a, len, g); break;
-        case GG_U2: k_gate_u2<<<blocks, threads, 0, st>>>(a, len, g); break;
-        case GG_RESET_ALL: k_reset_all<<<blocks, threads, 0, st>>>(a, len); break;
+        case GG_DIAG: k_gate_diag<T><<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_SWAP: k_gate_swap<T><<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_U2: k_gate_u2<T><<<blocks, threads, 0, st>>>(a, len, g); break;
+        case GG_RESET_ALL: k_reset_all<T><<<blocks, threads, 0, st>>>(a, len); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st) {
+    return launch_gate_t<double2>(a, len, g, st);
+}
+cudaError_t launch_gate_c64(float2* a, uint64_t len, const GGate& g, cudaStream_t st) {
+    return launch_gate_t<float2>(a, len, g, st);
 }
 
 // Partial-sum grid: fixed per length so that reductions are deterministic.

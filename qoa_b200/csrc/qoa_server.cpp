@@ -98,9 +98,11 @@ struct qoa_server_s {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
 
-    // Effective precision of a request: the FP32 form needs n >= 11 qubits.
+    // Effective precision of a request: the tensor-core block form needs
+    // n >= 11 qubits; smaller requests then run in complex128.
     int prec_for(uint32_t n) const {
-        return (cfg.precision == QOA_PREC_F32 && n >= 11) ? QOA_PREC_F32 : QOA_PREC_F64;
+        if (cfg.precision != QOA_PREC_F32) return QOA_PREC_F64;
+        return ((cfg.flags & QOA_FLAG_F32_TENSOR) && n < 11) ? QOA_PREC_F64 : QOA_PREC_F32;
     }
 
     size_t busy_bytes() const {
@@ -192,7 +194,8 @@ struct qoa_server_s {
     int run_traj(Request* r, uint32_t t, Slot* slot) {
         int rc;
         if (!slot->h) {
-            rc = qoa_create(r->n, slot->precision, cfg.flags, &slot->h);
+            const uint32_t fl = slot->precision == QOA_PREC_F32 ? cfg.flags : (cfg.flags & ~QOA_FLAG_F32_TENSOR);
+            rc = qoa_create(r->n, slot->precision, fl, &slot->h);
             if (rc) {
                 slot->h = nullptr;
                 return rc;

@@ -74,8 +74,9 @@ def test_batch_f64_matches_oracle(circs, ref):
 
 
 @pytest.mark.gpu
-def test_batch_f32_matches_oracle(circs, ref):
-    first, second, info = run_batch(circs, "f32")
+@pytest.mark.parametrize("tensor", [0, 1])
+def test_batch_f32_matches_oracle(circs, ref, tensor):
+    first, second, info = run_batch(circs, "f32", f32_tensor=tensor)
     assert info["small"] > 0 and info["large"] > 0
     np.testing.assert_allclose(first, ref, rtol=0, atol=F32_TOL)
     assert np.array_equal(first, second)

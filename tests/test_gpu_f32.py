@@ -1,7 +1,7 @@
-"""FP32-fused precision form: complex64 state, gates fused on the host into
-dense blocks of up to 5 qubits applied on the tensor cores (3xTF32, FP32
-accumulation). Checked against the FP64 oracle (relative L2 and infidelity)
-and, for the QFT, against sqrt(N) * IDFT."""
+"""FP32-fused precision form: complex64 state in both of its forms, the fused
+tile passes (default) and dense blocks of up to 5 qubits on the tensor cores
+(3xTF32, FP32 accumulation, QOA_FLAG_F32_TENSOR). Checked against the FP64
+oracle (relative L2 and infidelity) and, for the QFT, against sqrt(N) * IDFT."""
 import math
 
 import numpy as np
@@ -26,8 +26,8 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a.astype(np.complex128) - b) / np.linalg.norm(b))
 
 
-def f32_run(n, ops, init=None):
-    with qb.QuantumState(n, precision="f32") as st:
+def f32_run(n, ops, init=None, tensor=False):
+    with qb.QuantumState(n, precision="f32", f32_tensor=tensor) as st:
         if init is not None:
             st.set_state_vector(init.astype(np.complex64))
         st.execute(C.ops_to_array(ops))
@@ -50,28 +50,31 @@ def random_state(n, seed):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tensor", [False, True])
 @pytest.mark.parametrize("n", [11, 12, 14, 17])
-def test_f32_layered_matches_oracle(n):
+def test_f32_layered_matches_oracle(n, tensor):
     ops = C.random_layered(n, 6, 300 + n, initial_h=True)
-    got, ref = f32_run(n, ops), oracle_run(n, ops)
+    got, ref = f32_run(n, ops, tensor=tensor), oracle_run(n, ops)
     assert got.dtype == np.complex64
     assert rel_l2(got, ref) < F32_REL_L2
     assert fidelity_err(got, ref) < F32_INFIDELITY
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tensor", [False, True])
 @pytest.mark.parametrize("n", [12, 15])
-def test_f32_mixed_gate_kinds(n):
+def test_f32_mixed_gate_kinds(n, tensor):
     ops = mixed_circuit(n, 150, 11 * n)
-    got, ref = f32_run(n, ops), oracle_run(n, ops)
+    got, ref = f32_run(n, ops, tensor=tensor), oracle_run(n, ops)
     assert rel_l2(got, ref) < F32_REL_L2
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("tensor", [False, True])
 @pytest.mark.parametrize("n", [11, 14, 18])
-def test_f32_qft_matches_inverse_dft(n):
+def test_f32_qft_matches_inverse_dft(n, tensor):
     init = random_state(n, 4)
-    got = f32_run(n, C.qft(n), init=init)
+    got = f32_run(n, C.qft(n), init=init, tensor=tensor)
     ref = np.fft.ifft(init) * math.sqrt(1 << n)
     assert rel_l2(got, ref) < F32_REL_L2
     assert fidelity_err(got, ref) < F32_INFIDELITY
@@ -80,10 +83,19 @@ def test_f32_qft_matches_inverse_dft(n):
 @pytest.mark.gpu
 def test_f32_rejects_non_unitary_ops_and_small_n():
     with pytest.raises(qb.QoaError):
-        qb.QuantumState(8, precision="f32")
-    with qb.QuantumState(12, precision="f32") as st:
-        with pytest.raises(qb.QoaError):
-            st.execute(C.ops_to_array([C.Op(C.MEASURE, [0])]))
+        qb.QuantumState(8, precision="f32", f32_tensor=True)
+    for tensor in (False, True):
+        with qb.QuantumState(12, precision="f32", f32_tensor=tensor) as st:
+            with pytest.raises(qb.QoaError):
+                st.execute(C.ops_to_array([C.Op(C.MEASURE, [0])]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 4, 9])
+def test_f32_small_states_run_per_gate(n):
+    ops = mixed_circuit(n, 60, 5 * n) if n >= 3 else C.random_layered(n, 5, 2)
+    got, ref = f32_run(n, ops), oracle_run(n, ops)
+    assert rel_l2(got, ref) < F32_REL_L2
 
 
 @pytest.mark.gpu
