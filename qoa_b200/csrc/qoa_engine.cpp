@@ -55,8 +55,10 @@ cudaError_t launch_f32_probs(const float2* a, uint64_t off, uint64_t cnt, const 
 cudaError_t launch_random_state(void* a, bool f32, uint64_t len, uint64_t seed, cudaStream_t st);
 cudaError_t launch_f32_expz(const float2* a, uint64_t len, const uint64_t* masks, uint32_t k, double* partials,
                             double* out, const double* norm2, cudaStream_t st);
-cudaError_t launch_pass_c64(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
+cudaError_t launch_pass_p32(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
                             cudaStream_t st);
+cudaError_t launch_pass_p32_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                                  int max_nops, int max_ncoef, cudaStream_t st);
 cudaError_t launch_gate_c64(float2* a, uint64_t len, const GGate& g, cudaStream_t st);
 cudaError_t launch_pass_arena(bool c64, const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start,
                               uint32_t tiles, int max_nops, int max_ncoef, cudaStream_t st);
@@ -136,6 +138,7 @@ inline double2 from_polar(double r, double t) { return d2(r * std::cos(t), r * s
 // must be X or Y (CNOT, Toffoli, CY), which is all the instruction set makes.
 bool is_pass_gate(const Gate& g) {
     if (g.kind == K_DIAG) return true;
+    if (g.kind == K_SWAP) return g.cmask == 0;  // a relabelling of two tile bits
     return g.kind == K_G1 && (g.cmask == 0 || g.sub == G1_X || g.sub == G1_Y);
 }
 bool is_barrier(const Gate& g) { return g.kind >= K_MEASURE; }
@@ -622,17 +625,25 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     int no = 0;
     for (uint32_t q = LANE_BITS; q < n; ++q)
         if (slot_of[q] < 0) P.outer_qubits[no++] = (uint8_t)q;
-    auto tbit = [&](int q) -> int {
-        if (q < LANE_BITS) return q;
-        return slot_of[q] < 0 ? -1 : LANE_BITS + slot_of[q];
-    };
+    // Tile bit holding each qubit (-1: outside the tile). A SWAP of two tile
+    // qubits moves no data: it exchanges their tile bits here and the store
+    // writes each tile bit to the qubit it ends up holding (out_qubit).
+    int tb_of[64];
+    for (int q = 0; q < 64; ++q) tb_of[q] = q < LANE_BITS ? q : (slot_of[q] < 0 ? -1 : LANE_BITS + slot_of[q]);
+    auto tbit = [&](int q) -> int { return tb_of[q]; };
+    auto relabel = [](int* tb, const Gate& g) { std::swap(tb[g.t], tb[g.t2]); };
 
     // register demand per gate (tile bit of each 2x2 target)
     const int ng = (int)st.gates.size();
     std::vector<int> need(ng, -1);
-    for (int i = 0; i < ng; ++i) {
-        const Gate& g = G[st.gates[i]];
-        if (g.kind == K_G1) need[i] = tbit(g.t);
+    {
+        int tb_sim[64];
+        std::memcpy(tb_sim, tb_of, sizeof tb_of);
+        for (int i = 0; i < ng; ++i) {
+            const Gate& g = G[st.gates[i]];
+            if (g.kind == K_G1) need[i] = tb_sim[g.t];
+            else if (g.kind == K_SWAP) relabel(tb_sim, g);
+        }
     }
     auto next_use = [&](int from, int t) {
         for (int i = from; i < ng; ++i)
@@ -802,6 +813,11 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             for (int k = 0; k < WARP_BITS; ++k)
                 if (m.warp[k] == t) nm.warp[k] = (uint8_t)o;
         }
+        // register positions by next use: the last register bit goes to the
+        // tile bit needed last (the complex64 pass pairs amplitudes along it)
+        std::stable_sort(nm.reg, nm.reg + REG_BITS, [&](uint8_t x, uint8_t y) {
+            return (x == must ? -1 : next_use(i, x)) < (y == must ? -1 : next_use(i, y));
+        });
         order_lanes(nm);
         return exchange_to(nm);
     };
@@ -851,6 +867,11 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
 
     for (int i = 0; i < ng; ++i) {
         const Gate& g = G[st.gates[i]];
+        if (g.kind == K_SWAP) {
+            if (g.cmask || tbit(g.t) < 0 || tbit(g.t2) < 0) return -1;
+            relabel(tb_of, g);
+            continue;
+        }
         if (g.kind == K_G1) {
             const int t = tbit(g.t);
             int k = -1;
@@ -915,19 +936,31 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         }
     }
     if (!flush_tab() || !flush_mx() || !flush_tm()) return -1;
-    // lanes back on tile bits 0..4 for the coalesced store
+    // where each tile bit is stored: the qubit it holds after the pass's SWAPs
+    int lane_tb[LANE_BITS];
+    for (int q = 0; q < 64; ++q) {
+        const int t = tb_of[q];
+        if (t < 0) continue;
+        P.out_qubit[t] = (uint8_t)q;
+        if (q < LANE_BITS) lane_tb[q] = t;
+    }
+    // lanes on the tile bits stored to qubits 0..4, in order, for the coalesced store
     bool canonical = true;
-    for (int i = 0; i < LANE_BITS; ++i) canonical &= m.lane[i] == i;
+    for (int i = 0; i < LANE_BITS; ++i) canonical &= m.lane[i] == lane_tb[i];
     if (!canonical) {
         TileMap nm;
-        for (int i = 0; i < LANE_BITS; ++i) nm.lane[i] = (uint8_t)i;
-        std::vector<int> high;
+        bool is_lane[TILE_BITS] = {};
+        for (int i = 0; i < LANE_BITS; ++i) {
+            nm.lane[i] = (uint8_t)lane_tb[i];
+            is_lane[lane_tb[i]] = true;
+        }
+        std::vector<int> high;  // the other tile bits keep registers where they can
         for (int k = 0; k < REG_BITS; ++k)
-            if (m.reg[k] >= LANE_BITS) high.push_back(m.reg[k]);
+            if (!is_lane[m.reg[k]]) high.push_back(m.reg[k]);
         for (int k = 0; k < WARP_BITS; ++k)
-            if (m.warp[k] >= LANE_BITS) high.push_back(m.warp[k]);
+            if (!is_lane[m.warp[k]]) high.push_back(m.warp[k]);
         for (int k = 0; k < LANE_BITS; ++k)
-            if (m.lane[k] >= LANE_BITS) high.push_back(m.lane[k]);
+            if (!is_lane[m.lane[k]]) high.push_back(m.lane[k]);
         for (int k = 0; k < REG_BITS; ++k) nm.reg[k] = (uint8_t)high[k];
         for (int k = 0; k < WARP_BITS; ++k) nm.warp[k] = (uint8_t)high[REG_BITS + k];
         if (!exchange_to(nm)) return -1;
@@ -1253,7 +1286,7 @@ int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
     }
     if (s->precision == QOA_PREC_F32) {
         Timer tm(s, 2.0 * std::ldexp(8.0, (int)s->n), 3);
-        CK(launch_pass_c64((float2*)s->amps, P, s->scal, s->partials, s->stream));
+        CK(launch_pass_p32((float2*)s->amps, P, s->scal, s->partials, s->stream));
     } else {
         Timer tm(s, 2.0 * std::ldexp(16.0, (int)s->n), 0);
         CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
@@ -1906,8 +1939,11 @@ int batch_enqueue(qoa_batch_t b) {
                                       (const float*)(fb + b->f32_off[0]), (const F32PhaseOp*)(fb + b->f32_off[1]),
                                       (const F32Angle*)(fb + b->f32_off[2]), (const F32Phase*)(fb + b->f32_off[3]),
                                       (const float2*)(fb + b->f32_off[4]), s0));
+        else if (f32)
+            BCK(launch_pass_p32_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
+                                      R.max_nops, R.max_ncoef, s0));
         else
-            BCK(launch_pass_arena(f32, b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
+            BCK(launch_pass_arena(false, b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                   R.max_nops, R.max_ncoef, s0));
     }
     for (uint32_t i = 1; i < ns; ++i) {

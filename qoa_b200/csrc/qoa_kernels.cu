@@ -367,18 +367,20 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
         }
     }
 
-    // final flush of the pending factor, store (the last mapping has lanes on
-    // tile bits 0..4 again), and norm partials
+    // final flush of the pending factor, store, and norm partials. Tile bit t
+    // goes to global qubit out_qubit[t] (its load qubit unless SWAPs in the
+    // pass relabelled it); the last mapping has on lane i the tile bit stored
+    // to qubit i, so the store is as coalesced as the load.
     double ss = 0.0;
     {
         const TileMap& mf = cur < 0 ? P.map0 : P.xmap[cur];
         uint64_t tb = g0 + (uint64_t)lane;
 #pragma unroll
         for (int k = 0; k < WARP_BITS; ++k)
-            if ((wid >> k) & 1) tb += tstride(P, mf.warp[k]);
+            if ((wid >> k) & 1) tb += 1ull << P.out_qubit[mf.warp[k]];
         uint64_t rst[REG_BITS];
 #pragma unroll
-        for (int k = 0; k < REG_BITS; ++k) rst[k] = tstride(P, mf.reg[k]);
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = 1ull << P.out_qubit[mf.reg[k]];
 #pragma unroll
         for (int v = 0; v < REGS; ++v) {
             uint64_t g = tb;
@@ -405,8 +407,14 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
 
 // Resident CTAs per SM: the complex128 pass needs 128 registers a thread,
 // the complex64 one fits five CTAs.
-template <typename T> struct PassOcc { static constexpr int value = 4; };
-template <> struct PassOcc<float2> { static constexpr int value = 5; };
+#ifndef QOA_PASS_OCC64
+#define QOA_PASS_OCC64 4
+#endif
+#ifndef QOA_PASS_OCC32
+#define QOA_PASS_OCC32 8
+#endif
+template <typename T> struct PassOcc { static constexpr int value = QOA_PASS_OCC64; };
+template <> struct PassOcc<float2> { static constexpr int value = QOA_PASS_OCC32; };
 
 template <typename T>
 __global__ void __launch_bounds__(PASS_THREADS, PassOcc<T>::value)

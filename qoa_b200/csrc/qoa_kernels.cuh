@@ -105,7 +105,8 @@ struct PassParams {
     uint32_t ncoef;
     uint32_t pad_;
     double2 phase;                    // global phase of the factored gates of this pass
-    uint8_t slot_qubit[HIGH_SLOTS];   // global qubit of each high slot
+    uint8_t slot_qubit[HIGH_SLOTS];   // global qubit of each high slot (at load)
+    uint8_t out_qubit[TILE_BITS];     // global qubit each tile bit is stored to (SWAPs relabel tile bits)
     uint8_t outer_qubits[64];         // qubits outside the tile, ascending (n - TILE_BITS of them)
     TileMap map0;                     // mapping at load (lanes = tile bits 0..4)
     TileMap xmap[MAX_XCHG];           // mappings after each exchange

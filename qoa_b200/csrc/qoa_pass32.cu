@@ -1,0 +1,495 @@
+// qoa_pass32.cu — the complex64 tile pass with packed FP32 arithmetic.
+//
+// Same tile, op stream and pass parameters as k_pass (qoa_kernels.cu), but
+// each thread keeps its 16 amplitudes split by component and paired along
+// register bit 3: re[j] = (Re a[j], Re a[j+8]) and im[j] = (Im a[j], Im
+// a[j+8]) for j = 0..7, each pair one 64-bit register operand of the sm_100
+// packed FP32 instructions (add/sub/mul/fma .f32x2). A gate on register bit
+// 0..2 then updates two amplitude pairs per instruction with no shuffling of
+// real and imaginary parts; a gate on register bit 3 (the pairing bit, given
+// by the host to the tile bit used last) takes the scalar FP32 path. All
+// rounding is single-precision round-to-nearest, as in the complex64 form of
+// k_pass.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qoa_kernels.cuh"
+
+namespace qoa {
+
+namespace {
+
+typedef unsigned long long u64p;  // a packed pair of floats
+
+__device__ __forceinline__ u64p pk(float lo, float hi) {
+    return (u64p)__float_as_uint(lo) | ((u64p)__float_as_uint(hi) << 32);
+}
+__device__ __forceinline__ float lo(u64p a) { return __uint_as_float((unsigned)a); }
+__device__ __forceinline__ float hi(u64p a) { return __uint_as_float((unsigned)(a >> 32)); }
+__device__ __forceinline__ u64p bc(float x) { return pk(x, x); }
+
+__device__ __forceinline__ u64p add2(u64p a, u64p b) {
+    u64p d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64p sub2(u64p a, u64p b) {
+    u64p d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64p mul2(u64p a, u64p b) {
+    u64p d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64p fma2(u64p a, u64p b, u64p c) {
+    u64p d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// (re, im) *= (cr, ci), componentwise complex product of packed pairs
+__device__ __forceinline__ void cmul2(u64p& re, u64p& im, u64p cr, u64p ci) {
+    const u64p r = fma2(cr, re, mul2(sub2(0ull, ci), im));
+    im = fma2(cr, im, mul2(ci, re));
+    re = r;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// 2x2 on register bit K (0..2): pairs (j, j | 1<<K), both halves at once
+template <int SUB, int K>
+__device__ __forceinline__ void g1p(u64p (&re)[8], u64p (&im)[8], const float2* __restrict__ m) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (j & (1 << K)) continue;
+        const int k = j | (1 << K);
+        u64p& r0 = re[j]; u64p& i0 = im[j]; u64p& r1 = re[k]; u64p& i1 = im[k];
+        if (SUB == G1_HF) {
+            const u64p a = r0, b = i0;
+            r0 = add2(a, r1); i0 = add2(b, i1);
+            r1 = sub2(a, r1); i1 = sub2(b, i1);
+        } else if (SUB == G1_X) {
+            u64p t = r0; r0 = r1; r1 = t;
+            t = i0; i0 = i1; i1 = t;
+        } else if (SUB == G1_Y) {  // a0' = -i a1, a1' = i a0
+            const u64p a = r0, b = i0;
+            r0 = i1; i0 = sub2(0ull, r1);
+            r1 = sub2(0ull, b); i1 = a;
+        } else if (SUB == G1_RXA) {  // a0' = a0 - i t a1, a1' = a1 - i t a0
+            const u64p t = bc(m[0].x), a = r0, b = i0;
+            r0 = fma2(t, i1, a); i0 = fma2(sub2(0ull, t), r1, b);
+            r1 = fma2(t, b, r1); i1 = fma2(sub2(0ull, t), a, i1);
+        } else if (SUB == G1_RXB) {  // a0' = r a0 - i a1, a1' = r a1 - i a0
+            const u64p r = bc(m[0].x), a = r0, b = i0;
+            r0 = fma2(r, a, i1); i0 = sub2(mul2(r, b), r1);
+            r1 = fma2(r, r1, b); i1 = sub2(mul2(r, i1), a);
+        } else if (SUB == G1_RYA) {  // a0' = a0 - t a1, a1' = a1 + t a0
+            const u64p t = bc(m[0].x), nt = bc(-m[0].x), a = r0, b = i0;
+            r0 = fma2(nt, r1, a); i0 = fma2(nt, i1, b);
+            r1 = fma2(t, a, r1); i1 = fma2(t, b, i1);
+        } else if (SUB == G1_RYB) {  // a0' = r a0 - a1, a1' = r a1 + a0
+            const u64p r = bc(m[0].x), a = r0, b = i0;
+            r0 = sub2(mul2(r, a), r1); i0 = sub2(mul2(r, b), i1);
+            r1 = fma2(r, r1, a); i1 = fma2(r, i1, b);
+        } else {  // general: a0' = m0 a0 + m1 a1, a1' = m2 a0 + m3 a1
+            const float2 c0 = m[0], c1 = m[1], c2 = m[2], c3 = m[3];
+            const u64p a = r0, b = i0, c = r1, d = i1;
+            r0 = fma2(bc(c0.x), a, fma2(bc(-c0.y), b, fma2(bc(c1.x), c, mul2(bc(-c1.y), d))));
+            i0 = fma2(bc(c0.x), b, fma2(bc(c0.y), a, fma2(bc(c1.x), d, mul2(bc(c1.y), c))));
+            r1 = fma2(bc(c2.x), a, fma2(bc(-c2.y), b, fma2(bc(c3.x), c, mul2(bc(-c3.y), d))));
+            i1 = fma2(bc(c2.x), b, fma2(bc(c2.y), a, fma2(bc(c3.x), d, mul2(bc(c3.y), c))));
+        }
+    }
+}
+
+// scalar 2x2 on a pair of complex floats (register bit 3: the two halves)
+template <int SUB>
+__device__ __forceinline__ void g1s(float2& a0, float2& a1, const float2* __restrict__ m) {
+    if (SUB == G1_HF) {
+        const float2 t = a0;
+        a0 = make_float2(t.x + a1.x, t.y + a1.y);
+        a1 = make_float2(t.x - a1.x, t.y - a1.y);
+    } else if (SUB == G1_X) {
+        const float2 t = a0; a0 = a1; a1 = t;
+    } else if (SUB == G1_Y) {
+        const float2 t = a0;
+        a0 = make_float2(a1.y, -a1.x);
+        a1 = make_float2(-t.y, t.x);
+    } else if (SUB == G1_RXA) {
+        const float t = m[0].x; const float2 u = a0;
+        a0 = make_float2(fmaf(t, a1.y, u.x), fmaf(-t, a1.x, u.y));
+        a1 = make_float2(fmaf(t, u.y, a1.x), fmaf(-t, u.x, a1.y));
+    } else if (SUB == G1_RXB) {
+        const float r = m[0].x; const float2 u = a0;
+        a0 = make_float2(fmaf(r, u.x, a1.y), fmaf(r, u.y, -a1.x));
+        a1 = make_float2(fmaf(r, a1.x, u.y), fmaf(r, a1.y, -u.x));
+    } else if (SUB == G1_RYA) {
+        const float t = m[0].x; const float2 u = a0;
+        a0 = make_float2(fmaf(-t, a1.x, u.x), fmaf(-t, a1.y, u.y));
+        a1 = make_float2(fmaf(t, u.x, a1.x), fmaf(t, u.y, a1.y));
+    } else if (SUB == G1_RYB) {
+        const float r = m[0].x; const float2 u = a0;
+        a0 = make_float2(fmaf(r, u.x, -a1.x), fmaf(r, u.y, -a1.y));
+        a1 = make_float2(fmaf(r, a1.x, u.x), fmaf(r, a1.y, u.y));
+    } else {
+        const float2 t = a0;
+        float2 r0 = cmulf(m[0], t), r1 = cmulf(m[2], t);
+        r0.x = fmaf(m[1].x, a1.x, r0.x); r0.x = fmaf(-m[1].y, a1.y, r0.x);
+        r0.y = fmaf(m[1].x, a1.y, r0.y); r0.y = fmaf(m[1].y, a1.x, r0.y);
+        r1.x = fmaf(m[3].x, a1.x, r1.x); r1.x = fmaf(-m[3].y, a1.y, r1.x);
+        r1.y = fmaf(m[3].x, a1.y, r1.y); r1.y = fmaf(m[3].y, a1.x, r1.y);
+        a0 = r0; a1 = r1;
+    }
+}
+
+template <int SUB>
+__device__ __forceinline__ void g1_bit3(u64p (&re)[8], u64p (&im)[8], const float2* __restrict__ m) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        float2 a0 = make_float2(lo(re[j]), lo(im[j])), a1 = make_float2(hi(re[j]), hi(im[j]));
+        g1s<SUB>(a0, a1, m);
+        re[j] = pk(a0.x, a1.x);
+        im[j] = pk(a0.y, a1.y);
+    }
+}
+
+// X / Y on register bit K under register mask creg (any bits) and thread predicate
+template <int SUB, int K>
+__device__ __forceinline__ void g1c(u64p (&re)[8], u64p (&im)[8], bool tp, uint32_t creg) {
+    if (!tp) return;
+#pragma unroll
+    for (int v = 0; v < 16; ++v) {
+        if ((v & (1 << K)) || (v & creg) != creg) continue;
+        const int w = v | (1 << K);
+        const int jv = v & 7, jw = w & 7;
+        const bool hv = v >= 8, hw = w >= 8;
+        float2 a0 = make_float2(hv ? hi(re[jv]) : lo(re[jv]), hv ? hi(im[jv]) : lo(im[jv]));
+        float2 a1 = make_float2(hw ? hi(re[jw]) : lo(re[jw]), hw ? hi(im[jw]) : lo(im[jw]));
+        g1s<SUB>(a0, a1, nullptr);
+        re[jv] = hv ? pk(lo(re[jv]), a0.x) : pk(a0.x, hi(re[jv]));
+        im[jv] = hv ? pk(lo(im[jv]), a0.y) : pk(a0.y, hi(im[jv]));
+        re[jw] = hw ? pk(lo(re[jw]), a1.x) : pk(a1.x, hi(re[jw]));
+        im[jw] = hw ? pk(lo(im[jw]), a1.y) : pk(a1.y, hi(im[jw]));
+    }
+}
+
+// multiply the registers v with (v & creg) == creg by d
+__device__ __forceinline__ void diag_p(u64p (&re)[8], u64p (&im)[8], bool tp, uint32_t creg, float2 d) {
+    if (!tp) return;
+    const uint32_t cl = creg & 7u;
+    const bool only_hi = (creg & 8u) != 0;
+    const u64p cr = only_hi ? pk(1.f, d.x) : bc(d.x);
+    const u64p ci = only_hi ? pk(0.f, d.y) : bc(d.y);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if (((uint32_t)j & cl) == cl) cmul2(re[j], im[j], cr, ci);
+}
+
+__device__ __forceinline__ uint32_t spos(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
+
+__device__ __forceinline__ uint64_t tstride(const PassParams& P, uint32_t t) {
+    return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+}
+
+__device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const PassParams& P, const double nrm,
+                                              const uint64_t blk, double* __restrict__ partial_out) {
+    extern __shared__ __align__(16) unsigned char p32_smem[];
+    float2* tile = reinterpret_cast<float2*>(p32_smem);
+    __shared__ double red[PASS_THREADS / 32];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+
+    uint64_t g0 = 0;
+    {
+        const int nout = (int)P.n - TILE_BITS;
+        for (int k = 0; k < nout; ++k) g0 |= ((blk >> k) & 1ull) << P.outer_qubits[k];
+    }
+    const uint32_t nops = P.nops;
+    uint4* sops = reinterpret_cast<uint4*>(tile + (1 << TILE_BITS));
+    float2* scoef = reinterpret_cast<float2*>(sops + nops);
+    {
+        const uint4* gops = reinterpret_cast<const uint4*>(P.ops);
+        for (uint32_t i = threadIdx.x; i < nops; i += PASS_THREADS) sops[i] = gops[i];
+        for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS)
+            scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);
+    }
+    const bool valid = nrm > 1e-12;
+    float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))
+                        : make_float2((float)P.phase.x, (float)P.phase.y);
+
+    u64p re[8], im[8];
+    {
+        uint64_t tb = g0 + (uint64_t)lane;
+#pragma unroll
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((wid >> k) & 1) tb += tstride(P, P.map0.warp[k]);
+        uint64_t rst[REG_BITS];
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = tstride(P, P.map0.reg[k]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            uint64_t g = tb;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) g += rst[k];
+            const uint64_t g8 = g + rst[3];
+            float2 a = valid ? __ldcs(amps + g) : make_float2(g == 0 ? 1.f : 0.f, 0.f);
+            float2 b = valid ? __ldcs(amps + g8) : make_float2(0.f, 0.f);
+            re[j] = pk(a.x, b.x);
+            im[j] = pk(a.y, b.y);
+        }
+    }
+    __syncthreads();
+
+    const uint32_t* ow = reinterpret_cast<const uint32_t*>(sops);
+    int cur = -1;
+    uint32_t w = nops ? ow[0] : 0;
+    for (uint32_t oi = 0; oi < nops; ++oi) {
+        const uint32_t hot = w;
+        if (oi + 1 < nops) w = ow[4 * (oi + 1)];
+        const uint32_t code = hot & 0xffu;
+        const float2* m = scoef + (hot >> 16);
+        auto conds = [&](bool& tp) -> uint32_t {
+            const uint32_t cw = ow[4 * oi + 1];
+            tp = true;
+            if (cw >> 24) {
+                const unsigned long long co = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+                const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
+            }
+            return cw & 0xffu;
+        };
+        switch (code) {
+#define QOA_P3(BASE, SUB)                                           \
+    case BASE + 0: g1p<SUB, 0>(re, im, m); break;                   \
+    case BASE + 1: g1p<SUB, 1>(re, im, m); break;                   \
+    case BASE + 2: g1p<SUB, 2>(re, im, m); break;                   \
+    case BASE + 3: g1_bit3<SUB>(re, im, m); break;
+            QOA_P3(PC_HF, G1_HF)
+            QOA_P3(PC_RX, G1_RXA)
+            QOA_P3(PC_RY, G1_RYA)
+            QOA_P3(PC_RXB, G1_RXB)
+            QOA_P3(PC_RYB, G1_RYB)
+            QOA_P3(PC_GEN, G1_GEN)
+#undef QOA_P3
+#define QOA_C4(BASE, SUB)                                                                      \
+    case BASE + 0: { bool tp; const uint32_t cr = conds(tp); g1c<SUB, 0>(re, im, tp, cr); } break; \
+    case BASE + 1: { bool tp; const uint32_t cr = conds(tp); g1c<SUB, 1>(re, im, tp, cr); } break; \
+    case BASE + 2: { bool tp; const uint32_t cr = conds(tp); g1c<SUB, 2>(re, im, tp, cr); } break; \
+    case BASE + 3: { bool tp; const uint32_t cr = conds(tp); g1c<SUB, 3>(re, im, tp, cr); } break;
+            QOA_C4(PC_XC, G1_X)
+            QOA_C4(PC_YC, G1_Y)
+#undef QOA_C4
+            case PC_DIAG_T: {
+                bool tp;
+                conds(tp);
+                if (tp) pend = cmulf(pend, m[0]);
+                break;
+            }
+            case PC_DIAG_M: {
+                bool tp;
+                const uint32_t cr = conds(tp);
+                diag_p(re, im, tp, cr, m[0]);
+                break;
+            }
+            case PC_DIAG_MX: {
+                const uint32_t cnt = (hot >> 8) & 0xffu;
+                float2 f = make_float2(1.f, 0.f);
+                for (uint32_t e = 1; e <= cnt; ++e) {
+                    const uint4 rec = sops[oi + e];
+                    bool tp = true;
+                    const uint32_t cw = rec.y;
+                    if (cw >> 24) {
+                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
+                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
+                    }
+                    if (tp) f = cmulf(f, scoef[rec.x >> 16]);
+                    const bool last = (e == cnt) || ((sops[oi + e + 1].y & 0xffu) != (cw & 0xffu));
+                    if (last) {
+                        diag_p(re, im, true, cw & 0xffu, f);
+                        f = make_float2(1.f, 0.f);
+                    }
+                }
+                oi += cnt;
+                if (oi + 1 < nops) w = ow[4 * (oi + 1)];
+                break;
+            }
+            case PC_DIAG_TAB:
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float2 c0 = m[j], c1 = m[j + 8];
+                    cmul2(re[j], im[j], pk(c0.x, c1.x), pk(c0.y, c1.y));
+                }
+                break;
+            case PC_DIAG_TM: {
+                const uint32_t cnt = (hot >> 8) & 0xffu;
+                float2 f = make_float2(1.f, 0.f);
+                for (uint32_t e = 1; e <= cnt; ++e) {
+                    const uint4 rec = sops[oi + e];
+                    bool tp = true;
+                    const uint32_t cw = rec.y;
+                    if (cw >> 24) {
+                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
+                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
+                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
+                    }
+                    if (tp) f = cmulf(f, scoef[rec.x >> 16]);
+                }
+                pend = cmulf(pend, f);
+                oi += cnt;
+                if (oi + 1 < nops) w = ow[4 * (oi + 1)];
+                break;
+            }
+            case PC_FLUSH: {
+                const u64p cr = bc(pend.x), ci = bc(pend.y);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) cmul2(re[j], im[j], cr, ci);
+                pend = make_float2(1.f, 0.f);
+                break;
+            }
+            case PC_XCHG: {
+                const TileMap& mo = cur < 0 ? P.map0 : P.xmap[cur];
+                const int nxt = (int)(hot >> 16);
+                const TileMap& mn = P.xmap[nxt];
+                __syncthreads();
+                {
+                    uint32_t jb = 0;
+#pragma unroll
+                    for (int i = 0; i < LANE_BITS; ++i) jb |= ((uint32_t)(lane >> i) & 1u) << mo.lane[i];
+#pragma unroll
+                    for (int i = 0; i < WARP_BITS; ++i) jb |= ((uint32_t)(wid >> i) & 1u) << mo.warp[i];
+                    const uint32_t pb = spos(jb);
+                    uint32_t pr[REG_BITS];
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k) pr[k] = spos(1u << mo.reg[k]);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        uint32_t p = pb;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            if ((j >> k) & 1) p ^= pr[k];
+                        tile[p] = make_float2(lo(re[j]), lo(im[j]));
+                        tile[p ^ pr[3]] = make_float2(hi(re[j]), hi(im[j]));
+                    }
+                }
+                __syncthreads();
+                {
+                    uint32_t jb = 0;
+#pragma unroll
+                    for (int i = 0; i < LANE_BITS; ++i) jb |= ((uint32_t)(lane >> i) & 1u) << mn.lane[i];
+#pragma unroll
+                    for (int i = 0; i < WARP_BITS; ++i) jb |= ((uint32_t)(wid >> i) & 1u) << mn.warp[i];
+                    const uint32_t pb = spos(jb);
+                    uint32_t pr[REG_BITS];
+#pragma unroll
+                    for (int k = 0; k < REG_BITS; ++k) pr[k] = spos(1u << mn.reg[k]);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        uint32_t p = pb;
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            if ((j >> k) & 1) p ^= pr[k];
+                        const float2 a = tile[p], b = tile[p ^ pr[3]];
+                        re[j] = pk(a.x, b.x);
+                        im[j] = pk(a.y, b.y);
+                    }
+                }
+                cur = nxt;
+                break;
+            }
+            default: break;
+        }
+    }
+
+    double ss = 0.0;
+    {
+        const u64p cr = bc(pend.x), ci = bc(pend.y);
+        const TileMap& mf = cur < 0 ? P.map0 : P.xmap[cur];
+        uint64_t tb = g0 + (uint64_t)lane;
+#pragma unroll
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((wid >> k) & 1) tb += 1ull << P.out_qubit[mf.warp[k]];
+        uint64_t rst[REG_BITS];
+#pragma unroll
+        for (int k = 0; k < REG_BITS; ++k) rst[k] = 1ull << P.out_qubit[mf.reg[k]];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            uint64_t g = tb;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) g += rst[k];
+            cmul2(re[j], im[j], cr, ci);
+            const float2 a = make_float2(lo(re[j]), lo(im[j])), b = make_float2(hi(re[j]), hi(im[j]));
+            __stcs(amps + g, a);
+            __stcs(amps + g + rst[3], b);
+            ss += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
+        }
+    }
+    if (!partial_out) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if (lane == 0) red[wid] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w2 = 0; w2 < PASS_THREADS / 32; ++w2) t += red[w2];
+        *partial_out = t;
+    }
+}
+
+#ifndef QOA_PASS_OCC32
+#define QOA_PASS_OCC32 8
+#endif
+
+__global__ void __launch_bounds__(PASS_THREADS, QOA_PASS_OCC32)
+k_pass_p32(float2* __restrict__ amps, const __grid_constant__ PassParams P, const double* __restrict__ norm2_in,
+           double* __restrict__ partials) {
+    pass_tile_p32(amps, P, *norm2_in, blockIdx.x, partials + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(PASS_THREADS, QOA_PASS_OCC32)
+k_pass_p32_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ tile_start) {
+    const uint32_t b = blockIdx.x;
+    uint32_t l = 0, h = njobs - 1;
+    while (l < h) {
+        const uint32_t mid = (l + h + 1) >> 1;
+        if (tile_start[mid] <= b) l = mid;
+        else h = mid - 1;
+    }
+    const ArenaJob J = jobs[l];
+    pass_tile_p32(reinterpret_cast<float2*>(J.amps), *reinterpret_cast<const PassParams*>(J.params),
+                  J.fresh ? 0.0 : 1.0, b - tile_start[l], nullptr);
+}
+
+}  // namespace
+
+cudaError_t launch_pass_p32(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                            cudaStream_t st) {
+    const int tile_bytes = (1 << TILE_BITS) * (int)sizeof(float2);
+    const int smem = tile_bytes + (int)P.nops * 16 + (int)P.ncoef * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_p32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tile_bytes + MAX_PASS_OPS * 16 + MAX_PASS_COEF * (int)sizeof(float2));
+    if (e != cudaSuccess) return e;
+    k_pass_p32<<<1u << (P.n - TILE_BITS), PASS_THREADS, smem, st>>>(amps, P, norm2_in, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass_p32_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                                  int max_nops, int max_ncoef, cudaStream_t st) {
+    if (!njobs || !tiles) return cudaSuccess;
+    const int tile_bytes = (1 << TILE_BITS) * (int)sizeof(float2);
+    const int smem = tile_bytes + max_nops * 16 + max_ncoef * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_p32_arena, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         tile_bytes + MAX_PASS_OPS * 16 + MAX_PASS_COEF * (int)sizeof(float2));
+    if (e != cudaSuccess) return e;
+    k_pass_p32_arena<<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
+    return cudaGetLastError();
+}
+
+}  // namespace qoa

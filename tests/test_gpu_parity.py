@@ -173,3 +173,36 @@ def test_qinit_recreates_state():
         assert st.n == 13
         v = st.get_state_vector()
     assert abs(v[0] - 1 / math.sqrt(2)) < 1e-15 and abs(v[1 << 12] - 1 / math.sqrt(2)) < 1e-15
+
+
+def swap_heavy(n, count, seed):
+    """SWAPs interleaved with 1-qubit gates, controlled X and phases on the
+    swapped qubits (tile passes take SWAPs as relabellings of tile bits)."""
+    rng = np.random.default_rng(seed)
+    ops = [C.Op(C.H, [q]) for q in range(n)]
+    for _ in range(count):
+        a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+        k = int(rng.integers(6))
+        if k < 2:
+            ops.append(C.Op(C.SWAP, [a, b]))
+        elif k == 2:
+            ops.append(C.Op(C.RX, [a], float(rng.uniform(0, 2 * math.pi))))
+        elif k == 3:
+            ops.append(C.Op(C.CNOT, [a, b]))
+        elif k == 4:
+            ops.append(C.Op(C.CPHASE, [a, b], float(rng.uniform(0, 2 * math.pi))))
+        else:
+            ops.append(C.Op(C.T, [a]))
+    return ops
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [11, 13, 16])
+def test_swaps_inside_passes(n):
+    ops = swap_heavy(n, 40 * n, n)
+    ref = oracle_run(n, ops, 0)
+    assert rel_l2(engine_run(n, ops, False), ref) < TOL
+    with qb.QuantumState(n, precision="f32") as st:
+        st.execute(C.ops_to_array(ops))
+        got = st.get_state_vector().astype(np.complex128)
+    assert rel_l2(got, ref) < 1e-5
