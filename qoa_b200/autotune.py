@@ -9,6 +9,8 @@ replays of a sample of its circuits over a grid of candidates:
   small_ctas_per_sm  its persistent grid (SMs x this)
   pass_gate_budget   max gates fused into one tile pass (the fusion width;
                      0 = as many as fit)
+  f32_tensor         complex64 only: dense tensor-core blocks instead of
+                     tile passes
 
 The choice is cached in a JSON file keyed by precision, device name and a
 signature of the workload's size mix, so a later process reuses it.
@@ -41,6 +43,8 @@ def candidates(precision: str) -> List[Dict[str, int]]:
                 out.append(dict(small_max_n=smax, small_threads=thr, small_ctas_per_sm=ctas, pass_gate_budget=0))
     for budget in (48, 96, 160):
         out.append(dict(small_max_n=cap, small_threads=256, small_ctas_per_sm=2, pass_gate_budget=budget))
+    if precision == "f32":  # the tensor-core block form as well
+        out.append(dict(small_max_n=cap, small_threads=256, small_ctas_per_sm=2, pass_gate_budget=0, f32_tensor=1))
     return out
 
 

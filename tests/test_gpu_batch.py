@@ -127,3 +127,14 @@ def test_batch_rejects_measurement():
     with qb.Batch("f64") as b:
         with pytest.raises(qb.QoaError):
             b.add(4, [C.Op(C.MEASURE, [0])], [1])
+
+
+@pytest.mark.gpu
+def test_autotune_picks_a_valid_tuning(tmp_path, circs, ref):
+    from qoa_b200 import autotune
+    cache = str(tmp_path / "tune.json")
+    best = autotune.tune(circs, "f64", sample=12, cache=cache, budget_s=20)
+    assert set(best) >= {"small_max_n", "small_threads", "small_ctas_per_sm", "pass_gate_budget"}
+    assert autotune.tune(circs, "f64", sample=12, cache=cache) == best     # served from the cache
+    first, _, _ = run_batch(circs, "f64", **best)
+    np.testing.assert_allclose(first, ref, rtol=0, atol=F64_TOL)
