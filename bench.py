@@ -367,7 +367,7 @@ def run_qft(args):
                config={"workload": f"QFT n={n}", "gates": len(ops_n), "state_bytes": 8 << n},
                ms_per_step=ms, fp32_passes=passes,
                roofline={"bound": "hbm", "achieved": bw, "peak": peak, "unit": "GB/s",
-                         "frac": bw / peak if bw else None, "kernel": "k_pass<float2>", "avg_launch_ms": avg,
+                         "frac": bw / peak if bw else None, "kernel": "k_pass_p32", "avg_launch_ms": avg,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})"})
     m = n - 1
     ops_m = C.ops_to_array(C.qft(m))
@@ -582,6 +582,25 @@ def run_serve(args):
     return 0
 
 
+def run_case(args):
+    """Profiling case: two executions of one circuit on one state, nothing
+    else (no timing line). --case qft: QFT on a seeded Gaussian state;
+    --case layered: the layered circuit (H layer + --depth layers)."""
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+    n = args.qubits
+    ops = C.ops_to_array(C.qft(n) if args.case == "qft" else C.layered_h_workload(n, args.depth, 1))
+    with qb.QuantumState(n, precision=args.case_precision, compat_mask_quirk=(args.case != "qft")) as st:
+        st.set_random_state(2)
+        for _ in range(2):
+            st.execute(ops)
+        st.sync()
+        launches = st.launch_count()
+    print(json.dumps({"case": args.case, "n": n, "precision": args.case_precision, "ops": len(ops),
+                      "launches": launches}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -596,7 +615,9 @@ def main():
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
     ap.add_argument("--depth", type=int, default=20)
-    ap.add_argument("--workload", default="layered", choices=["layered", "qft", "batch", "serve"])
+    ap.add_argument("--workload", default="layered", choices=["layered", "qft", "batch", "serve", "case"])
+    ap.add_argument("--case", default="qft", choices=["qft", "layered"])
+    ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-workers", type=int, default=16)
     ap.add_argument("--serve-max-qubits", type=int, default=28)
@@ -613,6 +634,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "case":
+        return run_case(args)
     if (args.qubits, args.depth) != (30, 20):
         set_workload(args.qubits, args.depth)
     if args.impl == "reference":
