@@ -744,11 +744,14 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             mx.clear();
             return true;
         }
-        // runs of equal register masks share one register multiply in the kernel
+        // runs of equal register masks share one register multiply in the kernel;
+        // the last entry of each run carries the flag that triggers it
         std::stable_sort(mx.begin(), mx.end(), [](const std::pair<PassOp, double2>& x,
                                                   const std::pair<PassOp, double2>& y) {
             return x.first.cond_reg < y.first.cond_reg;
         });
+        for (size_t e = 0; e < mx.size(); ++e)
+            if (e + 1 == mx.size() || mx[e + 1].first.cond_reg != mx[e].first.cond_reg) mx[e].first.has_tp |= 2;
         return emit_group(mx, PC_DIAG_MX);
     };
     // lane positions 0..2 carry a quarter-warp: give them tile bits with
@@ -825,7 +828,11 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         for (int q = 0; q < 64; ++q) {
             if (!((mask >> q) & 1)) continue;
             const int t = tbit(q);
-            if (t < 0) { op.cond_outer |= 1ull << q; continue; }
+            if (t < 0) {  // outside the tile: the CTA's tile-number bit of that qubit
+                for (int k = 0; k < no; ++k)
+                    if (P.outer_qubits[k] == q) op.tmask |= 1ull << (LANE_BITS + WARP_BITS + k);
+                continue;
+            }
             for (int k = 0; k < LANE_BITS; ++k)
                 if (m.lane[k] == t) op.cond_lane |= (uint8_t)(1u << k);
             for (int k = 0; k < REG_BITS; ++k)
@@ -833,7 +840,11 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             for (int k = 0; k < WARP_BITS; ++k)
                 if (m.warp[k] == t) op.cond_warp |= (uint8_t)(1u << k);
         }
-        op.has_tp = (op.cond_lane || op.cond_warp || op.cond_outer) ? 1 : 0;
+        for (int k = 0; k < LANE_BITS; ++k)
+            if ((op.cond_lane >> k) & 1) op.tmask |= 1ull << k;
+        for (int k = 0; k < WARP_BITS; ++k)
+            if ((op.cond_warp >> k) & 1) op.tmask |= 1ull << (LANE_BITS + k);
+        op.has_tp = op.tmask ? 1 : 0;
     };
     auto phase_op = [&](uint64_t mask, double2 d) -> bool {
         if (mask == 0) {  // global factor

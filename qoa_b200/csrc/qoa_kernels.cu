@@ -175,6 +175,10 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((b >> k) & 1ull) << P.outer_qubits[k];
     }
+    // the thread's condition word: lane bits, warp bits, then the tile number
+    // (whose bit k is the bit of the k-th qubit outside the tile)
+    const unsigned long long tw = (unsigned long long)lane | ((unsigned long long)wid << LANE_BITS) |
+                                  (blk << (LANE_BITS + WARP_BITS));
 
     // op stream and coefficients -> shared memory (after the tile)
     const uint32_t nops = P.nops;
@@ -225,12 +229,8 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
         // condition of ops that take one: register mask and thread predicate
         auto conds = [&](bool& tp) -> uint32_t {
             const uint32_t cw = ow[4 * oi + 1];
-            tp = true;
-            if (cw >> 24) {
-                const unsigned long long co = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
-                const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-            }
+            const unsigned long long tm = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+            tp = (tw & tm) == tm;
             return cw & 0xffu;
         };
         switch (code) {
@@ -268,15 +268,11 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
                 T f = CT<T>::mk(1, 0);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    bool tp = true;
                     const uint32_t cw = rec.y;
-                    if (cw >> 24) {
-                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
-                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-                    }
+                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const bool tp = (tw & tm) == tm;
                     if (tp) f = c_mul(f, scoef[rec.x >> 16]);
-                    const bool last = (e == cnt) || ((sops[oi + e + 1].y & 0xffu) != (cw & 0xffu));
+                    const bool last = (e == cnt) || ((cw >> 25) & 1u);
                     if (last) {
                         diag_m(a, true, cw & 0xffu, f);
                         f = CT<T>::mk(1, 0);
@@ -296,13 +292,8 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
                 T f = CT<T>::mk(1, 0);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    bool tp = true;
-                    const uint32_t cw = rec.y;
-                    if (cw >> 24) {
-                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
-                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-                    }
+                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const bool tp = (tw & tm) == tm;
                     if (tp) f = c_mul(f, scoef[rec.x >> 16]);
                 }
                 pend = c_mul(pend, f);

@@ -84,8 +84,9 @@ struct alignas(16) PassOp {
     uint8_t cond_reg;   // register-bit mask
     uint8_t cond_lane;  // lane-bit mask
     uint8_t cond_warp;  // warp-bit mask
-    uint8_t has_tp;     // any lane / warp / outer condition
-    uint64_t cond_outer;// mask over global index bits outside the tile
+    uint8_t has_tp;     // bit 0: any lane / warp / outer condition; bit 1: last entry of a phase run
+    uint64_t tmask;     // thread condition over T = lane | warp << 5 | (tile number) << 7:
+                        // every set bit of tmask must be set in the thread's T
 };
 static_assert(sizeof(PassOp) == 16, "k_pass reads a PassOp as 32/64-bit words");
 

@@ -208,6 +208,8 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((blk >> k) & 1ull) << P.outer_qubits[k];
     }
+    const unsigned long long T = (unsigned long long)lane | ((unsigned long long)wid << LANE_BITS) |
+                                 (blk << (LANE_BITS + WARP_BITS));
     const uint32_t nops = P.nops;
     uint4* sops = reinterpret_cast<uint4*>(tile + (1 << TILE_BITS));
     float2* scoef = reinterpret_cast<float2*>(sops + nops);
@@ -255,12 +257,8 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
         const float2* m = scoef + (hot >> 16);
         auto conds = [&](bool& tp) -> uint32_t {
             const uint32_t cw = ow[4 * oi + 1];
-            tp = true;
-            if (cw >> 24) {
-                const unsigned long long co = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
-                const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-            }
+            const unsigned long long tm = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+            tp = (T & tm) == tm;
             return cw & 0xffu;
         };
         switch (code) {
@@ -301,15 +299,11 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
                 float2 f = make_float2(1.f, 0.f);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    bool tp = true;
                     const uint32_t cw = rec.y;
-                    if (cw >> 24) {
-                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
-                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-                    }
+                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const bool tp = (T & tm) == tm;
                     if (tp) f = cmulf(f, scoef[rec.x >> 16]);
-                    const bool last = (e == cnt) || ((sops[oi + e + 1].y & 0xffu) != (cw & 0xffu));
+                    const bool last = (e == cnt) || ((cw >> 25) & 1u);
                     if (last) {
                         diag_p(re, im, true, cw & 0xffu, f);
                         f = make_float2(1.f, 0.f);
@@ -331,13 +325,8 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
                 float2 f = make_float2(1.f, 0.f);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    bool tp = true;
-                    const uint32_t cw = rec.y;
-                    if (cw >> 24) {
-                        const unsigned long long co = ((unsigned long long)rec.w << 32) | rec.z;
-                        const uint32_t cl = (cw >> 8) & 0xffu, cwp = (cw >> 16) & 0xffu;
-                        tp = ((g0 & co) == co) && (((uint32_t)lane & cl) == cl) && (((uint32_t)wid & cwp) == cwp);
-                    }
+                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const bool tp = (T & tm) == tm;
                     if (tp) f = cmulf(f, scoef[rec.x >> 16]);
                 }
                 pend = cmulf(pend, f);
