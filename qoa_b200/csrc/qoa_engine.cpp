@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -613,6 +614,8 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
 // a per-thread pending factor, flushed only before an exchange that moves
 // amplitudes between threads whose factors may differ.
 int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParams& P) {
+    // thread conditions are 32-bit words: lane, warp and tile-number bits
+    if (n > 32 - (LANE_BITS + WARP_BITS) + TILE_BITS) return -1;
     memset(&P, 0, sizeof P);
     P.n = n;
     P.phase = d2(1.0, 0.0);
@@ -685,6 +688,54 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     std::vector<std::pair<PassOp, double2>> tm;
     std::vector<std::pair<PassOp, double2>> mx;  // register x thread phases
     uint32_t mx_bits = 0;
+    // angle phases (one tile bit at most, plus qubits outside the tile): per
+    // register bit, or per thread condition; summed once per CTA in the kernel
+    typedef std::vector<std::pair<uint64_t, double>> AngList;
+    AngList ang_reg[REG_BITS];
+    std::map<uint64_t, AngList> ang_thr;
+    uint32_t ang_reg_bits = 0;
+    int ang_used = 0, ang_pending = 0;
+    auto emit_ang = [&](AngList& ent, uint8_t code, uint32_t creg, uint64_t tm) -> bool {
+        if (ent.empty()) return true;
+        if (P.nang >= MAX_ANG_OPS || ang_used + (int)ent.size() > MAX_PASS_ANGLES) return false;
+        PassOp* o = new_op();
+        if (!o) return false;
+        o->code = code;
+        o->cond_reg = (uint8_t)creg;
+        o->tmask = tm;
+        o->has_tp = tm ? 1 : 0;
+        o->coef = P.nang;
+        P.ang_start[P.nang] = (uint16_t)ang_used;
+        for (const auto& e : ent) {
+            P.angles[ang_used].omask = e.first;
+            P.angles[ang_used].theta = e.second;
+            ++ang_used;
+        }
+        P.nang++;
+        P.ang_start[P.nang] = (uint16_t)ang_used;
+        ang_pending -= (int)ent.size();
+        ent.clear();
+        return true;
+    };
+    auto flush_ang_reg = [&](uint32_t bits) -> bool {
+        for (int k = 0; k < REG_BITS; ++k)
+            if ((bits >> k) & 1) {
+                if (!emit_ang(ang_reg[k], PC_DIAG_MA, 1u << k, 0)) return false;
+                ang_reg_bits &= ~(1u << k);
+            }
+        return true;
+    };
+    auto flush_ang_thr = [&]() -> bool {
+        for (auto& kv : ang_thr)
+            if (!emit_ang(kv.second, PC_DIAG_TA, 0, kv.first)) return false;
+        ang_thr.clear();
+        return true;
+    };
+    auto ang_keys_pending = [&]() -> int {
+        int c = (int)ang_thr.size();
+        for (int k = 0; k < REG_BITS; ++k) c += ang_reg[k].empty() ? 0 : 1;
+        return c;
+    };
     auto tab_reset = [&]() {
         for (int v = 0; v < REGS; ++v) tab[v] = d2(1, 0);
         tab_bits = 0;
@@ -771,7 +822,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         for (int x : rest) t.lane[k++] = (uint8_t)x;
     };
     auto exchange_to = [&](const TileMap& nm) -> bool {
-        if (!flush_tab() || !flush_mx() || !flush_tm()) return false;
+        if (!flush_tab() || !flush_mx() || !flush_tm() || !flush_ang_reg(0xfu) || !flush_ang_thr()) return false;
         if (dirty) {
             PassOp* f = new_op();
             if (!f) return false;
@@ -854,6 +905,26 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         PassOp o;
         memset(&o, 0, sizeof o);
         cond(mask, o);
+        {
+            const int tb = LANE_BITS + WARP_BITS;
+            const uint64_t thr = o.tmask & ((1ull << tb) - 1), outer = o.tmask >> tb;
+            const bool one_bit = (__builtin_popcount(o.cond_reg) == 1 && !thr) ||
+                                 (!o.cond_reg && __builtin_popcountll(thr) <= 1);
+            const bool room = ang_used + ang_pending < MAX_PASS_ANGLES && (int)P.nang + ang_keys_pending() + 1 < MAX_ANG_OPS;
+            if (outer && one_bit && room && std::fabs(d.x * d.x + d.y * d.y - 1.0) < 1e-14) {
+                const double th = std::atan2(d.y, d.x);
+                if (o.cond_reg) {
+                    const int k = __builtin_ctz(o.cond_reg);
+                    ang_reg[k].push_back({outer, th});
+                    ang_reg_bits |= 1u << k;
+                } else {
+                    ang_thr[thr].push_back({outer, th});
+                    if (thr) dirty = 1;
+                }
+                ++ang_pending;
+                return true;
+            }
+        }
         if (o.cond_reg == 0) {  // thread-only: joins the pending factor
             o.code = PC_DIAG_T;
             if (o.cond_lane || o.cond_warp) dirty = 1;
@@ -903,6 +974,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             }
             if ((tab_bits & touch) && !flush_tab()) return -1;
             if ((mx_bits & touch) && !flush_mx()) return -1;
+            if ((ang_reg_bits & touch) && !flush_ang_reg(ang_reg_bits & touch)) return -1;
             PassOp* o = new_op();
             if (!o) return -1;
             cond(g.cmask, *o);
@@ -946,7 +1018,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             }
         }
     }
-    if (!flush_tab() || !flush_mx() || !flush_tm()) return -1;
+    if (!flush_tab() || !flush_mx() || !flush_tm() || !flush_ang_reg(0xfu) || !flush_ang_thr()) return -1;
     // where each tile bit is stored: the qubit it holds after the pass's SWAPs
     int lane_tb[LANE_BITS];
     for (int q = 0; q < 64; ++q) {
@@ -2340,11 +2412,12 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
                 int cnt[PC_NCODES] = {};
                 for (uint32_t o = 0; o < P.nops; ++o) cnt[P.ops[o].code < PC_NCODES ? P.ops[o].code : 0]++;
                 int g1 = 0;
-                for (int c = PC_HF; c < PC_NCODES; ++c) g1 += cnt[c];
+                for (int c = PC_HF; c < PC_DIAG_TA; ++c) g1 += cnt[c];
                 const int disp = (int)P.nops - cnt[PC_NOP];
-                fprintf(stderr, "pass %zu: gates %zu dispatches %d g1 %d tm %d mx %d (entries %d) tab %d diag_m %d xchg %d flush %d\n",
+                fprintf(stderr, "pass %zu: gates %zu dispatches %d g1 %d tm %d mx %d (entries %d) tab %d diag_m %d xchg %d flush %d ang_ops %d (entries %d)\n",
                         si, steps[si].gates.size(), disp, g1, cnt[PC_DIAG_TM], cnt[PC_DIAG_MX], cnt[PC_NOP],
-                        cnt[PC_DIAG_TAB], cnt[PC_DIAG_M], cnt[PC_XCHG], cnt[PC_FLUSH]);
+                        cnt[PC_DIAG_TAB], cnt[PC_DIAG_M], cnt[PC_XCHG], cnt[PC_FLUSH], (int)P.nang,
+                        (int)P.ang_start[P.nang]);
             }
         }
     }

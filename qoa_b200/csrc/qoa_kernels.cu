@@ -177,8 +177,7 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
     }
     // the thread's condition word: lane bits, warp bits, then the tile number
     // (whose bit k is the bit of the k-th qubit outside the tile)
-    const unsigned long long tw = (unsigned long long)lane | ((unsigned long long)wid << LANE_BITS) |
-                                  (blk << (LANE_BITS + WARP_BITS));
+    const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << LANE_BITS) | ((uint32_t)blk << (LANE_BITS + WARP_BITS));
 
     // op stream and coefficients -> shared memory (after the tile)
     const uint32_t nops = P.nops;
@@ -188,6 +187,18 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
         const uint4* gops = reinterpret_cast<const uint4*>(P.ops);
         for (uint32_t i = threadIdx.x; i < nops; i += PASS_THREADS) sops[i] = gops[i];
         for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS) scoef[i] = CT<T>::from(P.coef[i]);
+    }
+    // angle phases of this CTA: sum the thetas whose outer condition holds
+    __shared__ T sang[MAX_ANG_OPS];
+    for (uint32_t ai = threadIdx.x; ai < P.nang; ai += PASS_THREADS) {
+        double th = 0.0;
+        for (uint32_t e = P.ang_start[ai]; e < P.ang_start[ai + 1]; ++e) {
+            const uint64_t om = P.angles[e].omask;
+            if ((blk & om) == om) th += P.angles[e].theta;
+        }
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        sang[ai] = CT<T>::from(make_double2(cs, sn));
     }
 
     const bool valid = nrm > 1e-12;
@@ -229,7 +240,7 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
         // condition of ops that take one: register mask and thread predicate
         auto conds = [&](bool& tp) -> uint32_t {
             const uint32_t cw = ow[4 * oi + 1];
-            const unsigned long long tm = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+            const uint32_t tm = ow[4 * oi + 2];
             tp = (tw & tm) == tm;
             return cw & 0xffu;
         };
@@ -260,6 +271,15 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
                 diag_m(a, tp, cr, m[0]);
                 break;
             }
+            case PC_DIAG_TA: {
+                bool tp;
+                conds(tp);
+                if (tp) pend = c_mul(pend, sang[hot >> 16]);
+                break;
+            }
+            case PC_DIAG_MA:
+                diag_m(a, true, ow[4 * oi + 1] & 0xffu, sang[hot >> 16]);
+                break;
             case PC_DIAG_MX: {
                 // entries sorted by register mask: each run of equal masks
                 // folds its thread-conditioned factors into one scalar, then
@@ -269,7 +289,7 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
                     const uint32_t cw = rec.y;
-                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const uint32_t tm = rec.z;
                     const bool tp = (tw & tm) == tm;
                     if (tp) f = c_mul(f, scoef[rec.x >> 16]);
                     const bool last = (e == cnt) || ((cw >> 25) & 1u);
@@ -292,7 +312,7 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
                 T f = CT<T>::mk(1, 0);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const uint32_t tm = rec.z;
                     const bool tp = (tw & tm) == tm;
                     if (tp) f = c_mul(f, scoef[rec.x >> 16]);
                 }

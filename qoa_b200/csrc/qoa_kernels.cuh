@@ -33,6 +33,16 @@ constexpr int REGS = 1 << REG_BITS;                        // 16 amps per thread
 constexpr int MAX_PASS_OPS = 640;
 constexpr int MAX_PASS_COEF = 768;                         // double2 coefficients
 constexpr int MAX_XCHG = 48;
+// Angle phases: a phase e^{i theta} whose condition is at most one tile bit
+// plus qubits outside the tile is evaluated once per CTA. Angle op a sums
+// the theta of its entries angles[ang_start[a] .. ang_start[a+1]) whose
+// tile-number mask is satisfied, then applies e^{i sum}.
+constexpr int MAX_ANG_OPS = 64;
+constexpr int MAX_PASS_ANGLES = 320;
+struct PassAngle {
+    uint64_t omask;  // bits of the tile number (qubits outside the tile) that must be 1
+    double theta;
+};
 
 // 2x2 forms. Coefficients at coef[c..]:
 //   G1_HF  (a0+a1, a0-a1): the Hadamard with its 1/sqrt2 left to the pass renormalisation
@@ -69,7 +79,9 @@ enum PassCode : uint8_t {
     PC_YC = 28,       // +k: Y likewise (CY, Y)
     PC_RXB = 32,      // +k (PC_RX carries the A form)
     PC_RYB = 36,      // +k (PC_RY carries the A form)
-    PC_NCODES = 40,
+    PC_DIAG_TA = 40,  // pending factor *= angle phase `coef` where the thread condition holds
+    PC_DIAG_MA = 41,  // registers with (v & cond_reg) == cond_reg *= angle phase `coef`
+    PC_NCODES = 42,
 };
 
 // One op of a pass (16 bytes). The first 32-bit word (code, k, coef) is all
@@ -85,8 +97,9 @@ struct alignas(16) PassOp {
     uint8_t cond_lane;  // lane-bit mask
     uint8_t cond_warp;  // warp-bit mask
     uint8_t has_tp;     // bit 0: any lane / warp / outer condition; bit 1: last entry of a phase run
-    uint64_t tmask;     // thread condition over T = lane | warp << 5 | (tile number) << 7:
-                        // every set bit of tmask must be set in the thread's T
+    uint64_t tmask;     // thread condition over T = lane | warp << 5 | (tile number) << 7
+                        // (kernels read the low 32 bits; passes need n <= 36): every set
+                        // bit of tmask must be set in the thread's T
 };
 static_assert(sizeof(PassOp) == 16, "k_pass reads a PassOp as 32/64-bit words");
 
@@ -111,9 +124,13 @@ struct PassParams {
     uint8_t outer_qubits[64];         // qubits outside the tile, ascending (n - TILE_BITS of them)
     TileMap map0;                     // mapping at load (lanes = tile bits 0..4)
     TileMap xmap[MAX_XCHG];           // mappings after each exchange
+    uint16_t nang;                    // angle ops
+    uint16_t ang_start[MAX_ANG_OPS + 1];
     PassOp ops[MAX_PASS_OPS];
     double2 coef[MAX_PASS_COEF];
+    PassAngle angles[MAX_PASS_ANGLES];
 };
+static_assert(sizeof(PassParams) <= 32000, "PassParams travels as a kernel parameter (32 KB limit)");
 
 static_assert(offsetof(PassParams, ops) % 16 == 0 && offsetof(PassParams, coef) % 16 == 0,
               "the op stream and coefficients are staged with 16-byte loads");

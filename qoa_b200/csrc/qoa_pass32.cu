@@ -208,8 +208,7 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
         const int nout = (int)P.n - TILE_BITS;
         for (int k = 0; k < nout; ++k) g0 |= ((blk >> k) & 1ull) << P.outer_qubits[k];
     }
-    const unsigned long long T = (unsigned long long)lane | ((unsigned long long)wid << LANE_BITS) |
-                                 (blk << (LANE_BITS + WARP_BITS));
+    const uint32_t T = (uint32_t)lane | ((uint32_t)wid << LANE_BITS) | ((uint32_t)blk << (LANE_BITS + WARP_BITS));
     const uint32_t nops = P.nops;
     uint4* sops = reinterpret_cast<uint4*>(tile + (1 << TILE_BITS));
     float2* scoef = reinterpret_cast<float2*>(sops + nops);
@@ -218,6 +217,17 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
         for (uint32_t i = threadIdx.x; i < nops; i += PASS_THREADS) sops[i] = gops[i];
         for (uint32_t i = threadIdx.x; i < P.ncoef; i += PASS_THREADS)
             scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);
+    }
+    __shared__ float2 sang[MAX_ANG_OPS];
+    for (uint32_t ai = threadIdx.x; ai < P.nang; ai += PASS_THREADS) {
+        double th = 0.0;
+        for (uint32_t e = P.ang_start[ai]; e < P.ang_start[ai + 1]; ++e) {
+            const uint64_t om = P.angles[e].omask;
+            if ((blk & om) == om) th += P.angles[e].theta;
+        }
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        sang[ai] = make_float2((float)cs, (float)sn);
     }
     const bool valid = nrm > 1e-12;
     float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))
@@ -257,7 +267,7 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
         const float2* m = scoef + (hot >> 16);
         auto conds = [&](bool& tp) -> uint32_t {
             const uint32_t cw = ow[4 * oi + 1];
-            const unsigned long long tm = reinterpret_cast<const unsigned long long*>(sops)[2 * oi + 1];
+            const uint32_t tm = ow[4 * oi + 2];
             tp = (T & tm) == tm;
             return cw & 0xffu;
         };
@@ -294,13 +304,22 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
                 diag_p(re, im, tp, cr, m[0]);
                 break;
             }
+            case PC_DIAG_TA: {
+                bool tp;
+                conds(tp);
+                if (tp) pend = cmulf(pend, sang[hot >> 16]);
+                break;
+            }
+            case PC_DIAG_MA:
+                diag_p(re, im, true, ow[4 * oi + 1] & 0xffu, sang[hot >> 16]);
+                break;
             case PC_DIAG_MX: {
                 const uint32_t cnt = (hot >> 8) & 0xffu;
                 float2 f = make_float2(1.f, 0.f);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
                     const uint32_t cw = rec.y;
-                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const uint32_t tm = rec.z;
                     const bool tp = (T & tm) == tm;
                     if (tp) f = cmulf(f, scoef[rec.x >> 16]);
                     const bool last = (e == cnt) || ((cw >> 25) & 1u);
@@ -325,7 +344,7 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
                 float2 f = make_float2(1.f, 0.f);
                 for (uint32_t e = 1; e <= cnt; ++e) {
                     const uint4 rec = sops[oi + e];
-                    const unsigned long long tm = ((unsigned long long)rec.w << 32) | rec.z;
+                    const uint32_t tm = rec.z;
                     const bool tp = (T & tm) == tm;
                     if (tp) f = cmulf(f, scoef[rec.x >> 16]);
                 }
@@ -433,7 +452,7 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
 }
 
 #ifndef QOA_PASS_OCC32
-#define QOA_PASS_OCC32 8
+#define QOA_PASS_OCC32 7
 #endif
 
 __global__ void __launch_bounds__(PASS_THREADS, QOA_PASS_OCC32)
