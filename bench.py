@@ -11,7 +11,8 @@ semantics. Seeded synthetic circuit (no dataset involved).
          the engine's stream, max over ranks)
   e2e    gates/s through the public C ABI call sequence with host buffers:
          reset, qoa_apply of the host op list, qoa_get_state into pinned host
-         memory (16 GiB device->host each step)
+         memory (16 GiB device->host each step), wall clock; two states
+         alternate so each step's copy overlaps the next step's gates
   roofline  the tile-pass kernel: 2 x 16 GiB algorithmic bytes per launch over
          its CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs
 
@@ -275,30 +276,43 @@ def run_ours(args):
     # ---- e2e: host op list in, full state out to pinned host memory ----
     e2e = None
     if not args.no_e2e:
+        # Public-API steps with host buffers: reset, qoa_apply of the host op
+        # list, qoa_get_state into pinned host memory. Two states alternate
+        # so that step i's 16 GiB device->host copy (its own host thread)
+        # overlaps step i+1's gates; every copy finishes inside the timed
+        # region (wall clock).
         host = torch.empty((1 << n) * 2, dtype=torch.float64, pin_memory=True)
         hv = host.numpy().view(np.complex128)
+        st2 = qb.QuantumState(n, compat_mask_quirk=True)
+        states = [st, st2]
 
-        def e2e_step():
-            st.apply_reset_all()
-            st.execute(ops)
-            st.get_state_vector(out=hv)
+        def copy_out(s):
+            s.get_state_vector(out=hv)
 
-        e2e_step()
-        st.sync()
+        for s_ in states:  # warm-up
+            s_.apply_reset_all()
+            s_.execute(ops)
+            copy_out(s_)
         if ws > 1:
             dist.barrier()
         k = max(1, min(args.steps, args.e2e_steps))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
-        e0.record(stream)
-        for _ in range(k):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
+        th = None
+        for i in range(k):
+            s_ = states[i % 2]
+            s_.apply_reset_all()
+            s_.execute(ops)
+            if th is not None:
+                th.join()
+            th = threading.Thread(target=copy_out, args=(s_,))
+            th.start()
+        th.join()
         wall = time.perf_counter() - t0
-        et, eu = aggregate(e0.elapsed_time(e1), float(G * k), dev if ws > 1 else None)
+        et, eu = aggregate(wall * 1e3, float(G * k), dev if ws > 1 else None)
         e2e = {"value": eu / (et / 1e3), "unit": "gates/s", "h2d_bytes_per_step": int(ops.nbytes),
-               "d2h_bytes_per_step": int(hv.nbytes), "steps": k, "wall_s": wall}
+               "d2h_bytes_per_step": int(hv.nbytes), "steps": k, "wall_s": wall,
+               "timing": "wall clock, max over ranks; two states alternate so copies overlap the next step"}
+        st2.close()
         del host
 
     cpu = None
@@ -607,7 +621,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-gates", type=int, default=12)

@@ -28,6 +28,7 @@
 namespace qoa {
 cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials, cudaStream_t st);
 cudaError_t launch_gate(double2* a, uint64_t len, const GGate& g, cudaStream_t st);
+cudaError_t launch_swapnet(void* a, bool c64, const PermParams& P, cudaStream_t st);
 int reduce_blocks(uint64_t len);
 cudaError_t launch_norm(const double2* a, uint64_t len, double* partials, double* out, uint32_t* status, cudaStream_t st);
 cudaError_t launch_p01(const double2* a, uint64_t len, uint32_t q, double* partials, double* out2, const double* norm2,
@@ -117,7 +118,8 @@ double uniform01(uint64_t seed, uint64_t stream, uint64_t event, uint32_t slot) 
 const uint64_t kMeasStreamXor = 0x6d656173ull;
 
 // ------------------------------------------------------------------ gates
-enum GateKind { K_G1 = 0, K_DIAG = 1, K_SWAP = 2, K_U2 = 3, K_MEASURE = 4, K_RESET = 5, K_RESETALL = 6, K_QINIT = 7 };
+enum GateKind { K_G1 = 0, K_DIAG = 1, K_SWAP = 2, K_U2 = 3, K_MEASURE = 4, K_RESET = 5, K_RESETALL = 6, K_QINIT = 7,
+                K_PERM = 8 /* a block of disjoint SWAPs, made by the executor */ };
 
 struct Gate {
     int kind = K_G1;
@@ -130,6 +132,7 @@ struct Gate {
     uint64_t dmask = 0;     // qubits acted on diagonally (controls, phase masks, selector)
     int src = -1;           // source op index
     double u = -1.0;        // K_MEASURE: uniform
+    uint8_t pi[64];         // K_PERM: partner of each qubit (itself if unpaired)
 };
 
 inline double2 d2(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
@@ -1526,6 +1529,72 @@ int execute_f32(qoa_state_t s, std::vector<Gate>& G) {
     return f32_launch(s);
 }
 
+// Runs of at least three consecutive disjoint SWAPs (a QFT's final swap
+// network) become one K_PERM step: a single in-place permutation pass instead
+// of several tile passes that only relabel.
+void merge_swap_blocks(std::vector<Gate>& G) {
+    std::vector<Gate> out;
+    out.reserve(G.size());
+    size_t i = 0;
+    while (i < G.size()) {
+        size_t j = i;
+        uint64_t used = 0;
+        while (j < G.size() && G[j].kind == K_SWAP && G[j].cmask == 0 &&
+               !(used & ((1ull << G[j].t) | (1ull << G[j].t2)))) {
+            used |= (1ull << G[j].t) | (1ull << G[j].t2);
+            ++j;
+        }
+        if (j - i >= 3) {
+            Gate p;
+            p.kind = K_PERM;
+            for (int q = 0; q < 64; ++q) p.pi[q] = (uint8_t)q;
+            for (size_t k = i; k < j; ++k) {
+                p.pi[G[k].t] = (uint8_t)G[k].t2;
+                p.pi[G[k].t2] = (uint8_t)G[k].t;
+            }
+            p.nmask = used;
+            p.src = G[i].src;
+            out.push_back(p);
+            i = j;
+        } else {
+            out.push_back(G[i]);
+            ++i;
+        }
+    }
+    G.swap(out);
+}
+
+int run_perm(qoa_state_t s, const Gate& g) {
+    const uint32_t n = s->n;
+    PermParams P;
+    memset(&P, 0, sizeof P);
+    P.n = n;
+    bool in_a[64] = {};
+    const uint32_t low = std::min<uint32_t>(LANE_BITS, n);
+    for (uint32_t q = 0; q < low; ++q) {
+        P.tq[P.na++] = (uint8_t)q;
+        in_a[q] = true;
+    }
+    for (uint32_t q = low; q < n; ++q)  // partners of the lane qubits, ascending
+        for (uint32_t l = 0; l < low; ++l)
+            if (g.pi[l] == q && !in_a[q]) {
+                P.tq[P.na++] = (uint8_t)q;
+                in_a[q] = true;
+            }
+    uint32_t no = 0;
+    for (uint32_t q = 0; q < n; ++q)
+        if (!in_a[q]) P.oq[no++] = (uint8_t)q;
+    for (uint32_t q = 0; q < n; ++q) P.pi[q] = g.pi[q];
+    for (uint32_t k = 0; k < P.na; ++k)
+        for (uint32_t k2 = 0; k2 < P.na; ++k2)
+            if (P.tq[k2] == g.pi[P.tq[k]]) P.src_bit[k] = (uint8_t)k2;
+    const double bytes = 2.0 * std::ldexp(s->precision == QOA_PREC_F32 ? 8.0 : 16.0, (int)n);
+    Timer tm(s, bytes, 4);
+    CK(launch_swapnet(s->amps, s->precision == QOA_PREC_F32, P, s->stream));
+    s->launches++;
+    return QOA_OK;
+}
+
 int execute(qoa_state_t s, std::vector<Gate>& G) {
     const bool c64 = s->precision == QOA_PREC_F32;
     if (c64 && (s->flags & QOA_FLAG_F32_TENSOR)) return execute_f32(s, G);
@@ -1540,6 +1609,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         size_t j = i;
         while (j < G.size() && G[j].kind != K_QINIT) ++j;
         std::vector<Gate> seg(G.begin() + i, G.begin() + j);
+        if (!per_gate) merge_swap_blocks(seg);
         std::vector<Step> steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
         for (const Step& st : steps) {
             int rc;
@@ -1554,6 +1624,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
                     }
                     case K_RESET: rc = do_reset_qubit(s, (uint32_t)g.t); break;
                     case K_RESETALL: rc = do_reset_all(s); break;
+                    case K_PERM: rc = run_perm(s, g); break;
                     default: rc = run_gate(s, g);
                 }
             }

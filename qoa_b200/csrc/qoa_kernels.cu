@@ -534,6 +534,55 @@ __global__ void k_reset_all(T* __restrict__ a, uint64_t len) {
     for (uint64_t i = gtid(); i < len; i += gstride()) a[i] = CT<T>::mk(i == 0 ? 1 : 0, 0);
 }
 
+// ------------------------------------------------------------ SWAP blocks
+// out[pi(i)] = in[i] for an involution pi of the qubits (disjoint SWAPs). The
+// norm is unchanged, so no partial sums are written.
+template <typename T>
+__global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid_constant__ PermParams P) {
+    extern __shared__ __align__(16) unsigned char sw_smem[];
+    T* s0 = reinterpret_cast<T*>(sw_smem);
+    const uint32_t tn = 1u << P.na;
+    T* s1 = s0 + tn;
+    const uint32_t nout = P.n - P.na;
+    const uint64_t b = blockIdx.x;
+    uint64_t o = 0, po = 0, pb = 0;
+    for (uint32_t k = 0; k < nout; ++k)
+        if ((b >> k) & 1) o |= 1ull << P.oq[k];
+    for (uint32_t k = 0; k < nout; ++k)
+        if ((o >> P.oq[k]) & 1) po |= 1ull << P.pi[P.oq[k]];
+    for (uint32_t k = 0; k < nout; ++k)
+        if ((po >> P.oq[k]) & 1) pb |= 1ull << k;
+    if (pb < b) return;  // the partner tile's CTA moves both
+    auto dep = [&](uint32_t j) {
+        uint64_t g = 0;
+        for (uint32_t k = 0; k < P.na; ++k)
+            if ((j >> k) & 1) g |= 1ull << P.tq[k];
+        return g;
+    };
+    for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
+        const uint64_t g = dep(j);
+        s0[j] = a[o | g];
+        if (pb != b) s1[j] = a[po | g];
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
+        uint32_t src = 0;
+        for (uint32_t k = 0; k < P.na; ++k)
+            if ((j >> k) & 1) src |= 1u << P.src_bit[k];
+        const uint64_t g = dep(j);
+        a[po | g] = s0[src];
+        if (pb != b) a[o | g] = s1[src];
+    }
+}
+
+cudaError_t launch_swapnet(void* a, bool c64, const PermParams& P, cudaStream_t st) {
+    const unsigned blocks = 1u << (P.n - P.na);
+    const size_t smem = (size_t)2 << P.na;
+    if (c64) k_swapnet<float2><<<blocks, 256, smem * sizeof(float2), st>>>((float2*)a, P);
+    else k_swapnet<double2><<<blocks, 256, smem * sizeof(double2), st>>>((double2*)a, P);
+    return cudaGetLastError();
+}
+
 // --------------------------------------------------------------- reductions
 template <int NB>
 __device__ __forceinline__ void block_store_partials(double (&v)[NB], double* __restrict__ out, uint32_t stride) {

@@ -244,6 +244,20 @@ enum GGKind : uint8_t {
     GG_SCALE = 6,     // materialise: multiply by the pending scale only
 };
 
+// A block of disjoint SWAPs applied as one in-place permutation of the
+// amplitudes (k_swapnet): pi maps each qubit to its partner (or itself). The
+// tile qubits tq (qubits 0..4 first, then the partners of 0..4) are closed
+// under pi; CTA b handles the tile whose outside bits are b deposited into
+// oq, together with its partner tile, so every CTA writes only what it read.
+struct PermParams {
+    uint32_t n;
+    uint32_t na;       // tile qubits
+    uint8_t tq[16];
+    uint8_t oq[48];
+    uint8_t pi[64];
+    uint8_t src_bit[16];  // tile bit k of an output index reads tile bit src_bit[k] of its source
+};
+
 struct GGate {
     uint8_t kind;
     uint8_t sub;

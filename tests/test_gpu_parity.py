@@ -206,3 +206,22 @@ def test_swaps_inside_passes(n):
         st.execute(C.ops_to_array(ops))
         got = st.get_state_vector().astype(np.complex128)
     assert rel_l2(got, ref) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [4, 7, 12, 17])
+def test_swap_blocks_as_permutations(n):
+    """Runs of >= 3 disjoint SWAPs run as one in-place permutation pass."""
+    rng = np.random.default_rng(n)
+    ops = [C.Op(C.H, [q]) for q in range(n)] + [C.Op(C.T, [q]) for q in range(0, n, 2)]
+    for rep in range(3):
+        perm = [int(x) for x in rng.permutation(n)]
+        for k in range(0, n - 1, 2):
+            ops.append(C.Op(C.SWAP, [perm[k], perm[k + 1]]))
+        ops += [C.Op(C.RY, [int(rng.integers(n))], 0.3 + rep), C.Op(C.CNOT, [0, n - 1])]
+    ref = oracle_run(n, ops, 0)
+    assert rel_l2(engine_run(n, ops, False), ref) < TOL
+    with qb.QuantumState(n, precision="f32") as st:
+        st.execute(C.ops_to_array(ops))
+        got = st.get_state_vector().astype(np.complex128)
+    assert rel_l2(got, ref) < 1e-5
