@@ -559,10 +559,13 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
             if ((j >> k) & 1) g |= 1ull << P.tq[k];
         return g;
     };
+    // shared-memory slot of tile index j: its low five bits XORed with the
+    // next five, so the permuted reads of a warp spread over the banks
+    auto sp = [](uint32_t j) { return j ^ ((j >> 5) & 31u); };
     for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
         const uint64_t g = dep(j);
-        s0[j] = a[o | g];
-        if (pb != b) s1[j] = a[po | g];
+        s0[sp(j)] = a[o | g];
+        if (pb != b) s1[sp(j)] = a[po | g];
     }
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
@@ -570,8 +573,8 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
         for (uint32_t k = 0; k < P.na; ++k)
             if ((j >> k) & 1) src |= 1u << P.src_bit[k];
         const uint64_t g = dep(j);
-        a[po | g] = s0[src];
-        if (pb != b) a[o | g] = s1[src];
+        a[po | g] = s0[sp(src)];
+        if (pb != b) a[o | g] = s1[sp(src)];
     }
 }
 
