@@ -213,12 +213,17 @@ int set_err(qoa_state_t s, int code, const char* fmt, ...) {
     return code;
 }
 
+// A failed call's error is also the thread's "last error"; it is cleared
+// here (when it is not sticky) so that the next launch check does not
+// report it again.
 #define CK(call)                                                                          \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
+        if (e_ != cudaSuccess) {                                                          \
+            cudaGetLastError();                                                           \
             return set_err(s, e_ == cudaErrorMemoryAllocation ? QOA_E_OOM : QOA_E_CUDA,   \
                            "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                 \
     } while (0)
 
 uint64_t state_len(const qoa_state_t s) { return 1ull << s->n; }
@@ -1792,7 +1797,11 @@ int bset_err(qoa_batch_t b, int code, const char* msg) {
 #define BCK(call)                                                                   \
     do {                                                                            \
         cudaError_t e_ = (call);                                                    \
-        if (e_ != cudaSuccess) return bset_err(b, QOA_E_CUDA, cudaGetErrorString(e_)); \
+        if (e_ != cudaSuccess) {                                                    \
+            cudaGetLastError();                                                     \
+            return bset_err(b, e_ == cudaErrorMemoryAllocation ? QOA_E_OOM : QOA_E_CUDA, \
+                            cudaGetErrorString(e_));                                \
+        }                                                                           \
     } while (0)
 
 bool small_ok(const Gate& g) { return g.kind == K_G1 || g.kind == K_DIAG || g.kind == K_SWAP; }
@@ -2150,6 +2159,7 @@ int qoa_create(uint32_t n, int precision, uint32_t flags, qoa_state_t* out) {
     s->precision = precision;
     cudaGetDevice(&s->device);
     auto fail = [&](int rc) {
+        cudaGetLastError();  // do not leave the failure as this thread's last error
         std::string m = s->err;
         qoa_destroy(s);
         set_err(nullptr, rc, "%s", m.c_str());
