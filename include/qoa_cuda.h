@@ -162,7 +162,8 @@ int qoa_reset_all(qoa_state_t s);
 int qoa_apply(qoa_state_t s, const qoa_op* ops, size_t nops);
 /* measure (quantum_state.rs:399-458) with a caller-supplied uniform u in
  * [0,1): outcome = (u < P0) ? 0 : 1. A negative u draws from the handle's
- * counter-based RNG (qoa_seed). */
+ * counter-based RNG (qoa_seed). complex128 handles only (the complex64 form
+ * takes unitary ops; sample it with qoa_sample). */
 int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome);
 /* Shots. mode 0 = measure_all order (quantum_state.rs:909-918): qubits 0..n-1
  * measured one after another, n uniforms per shot (u[shot*n + q]); mode 1 =
@@ -172,7 +173,8 @@ int qoa_measure(qoa_state_t s, uint32_t q, double u, uint32_t* outcome);
 int qoa_sample(qoa_state_t s, const double* u, size_t shots, int mode, uint64_t* out);
 /* get_probabilities (quantum_state.rs:128-133): 2^n doubles. */
 int qoa_probabilities(qoa_state_t s, double* out);
-/* <Z_mask> = sum_i (-1)^popcount(i & mask) |a_i|^2 for k masks. */
+/* <Z_mask> = sum_i (-1)^popcount(i & mask) |a_i|^2 for k masks (FP64 sums,
+ * either precision). */
 int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out);
 /* get_state_vector / set_state_vector (quantum_state.rs:1129-1145); set
  * renormalises. bytes must be 2^n * 16 (complex128), or 2^n * 8 (complex64)

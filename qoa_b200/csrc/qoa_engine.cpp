@@ -62,8 +62,8 @@ cudaError_t launch_pass_p32(float2* amps, const PassParams& P, const double* nor
 cudaError_t launch_pass_p32_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
                                   int max_nops, int max_ncoef, cudaStream_t st);
 cudaError_t launch_gate_c64(float2* a, uint64_t len, const GGate& g, cudaStream_t st);
-cudaError_t launch_pass_arena(bool c64, const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start,
-                              uint32_t tiles, int max_nops, int max_ncoef, cudaStream_t st);
+cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                              int max_nops, int max_ncoef, cudaStream_t st);
 cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
                                   const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
                                   const F32Phase* phases, const float2* tables, cudaStream_t st);
@@ -2106,7 +2106,7 @@ int batch_enqueue(qoa_batch_t b) {
             BCK(launch_pass_p32_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                       R.max_nops, R.max_ncoef, s0));
         else
-            BCK(launch_pass_arena(false, b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
+            BCK(launch_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                   R.max_nops, R.max_ncoef, s0));
     }
     for (uint32_t i = 1; i < ns; ++i) {
@@ -2300,11 +2300,14 @@ int qoa_probabilities(qoa_state_t s, double* out) {
 int qoa_expect_z(qoa_state_t s, const uint64_t* masks, size_t k, double* out) {
     int rc = check_handle(s);
     if (rc) return rc;
-    if (s->precision == QOA_PREC_F32) return set_err(s, QOA_E_ARG, "not available for an FP32 handle");
     if ((!masks || !out) && k) return set_err(s, QOA_E_ARG, "null argument");
     for (size_t i = 0; i < k; i += 8) {
         const uint32_t kk = (uint32_t)std::min<size_t>(8, k - i);
-        CK(launch_expz(s->amps, state_len(s), masks + i, kk, s->partials, s->scal + 8, s->scal, s->stream));
+        if (s->precision == QOA_PREC_F32)  // FP64 sums over the complex64 state
+            CK(launch_f32_expz((const float2*)s->amps, state_len(s), masks + i, kk, s->partials, s->scal + 8,
+                               s->scal, s->stream));
+        else
+            CK(launch_expz(s->amps, state_len(s), masks + i, kk, s->partials, s->scal + 8, s->scal, s->stream));
         s->launches += 2;
         CK(cudaMemcpyAsync(s->host_scal + 8, s->scal + 8, kk * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));

@@ -416,16 +416,12 @@ __device__ __forceinline__ void pass_tile(T* __restrict__ amps, const PassParams
     }
 }
 
-// Resident CTAs per SM: the complex128 pass needs 128 registers a thread,
-// the complex64 one fits five CTAs.
+// Resident CTAs per SM: the complex128 pass needs 128 registers a thread.
+// (The complex64 passes are the packed kernels of qoa_pass32.cu.)
 #ifndef QOA_PASS_OCC64
 #define QOA_PASS_OCC64 4
 #endif
-#ifndef QOA_PASS_OCC32
-#define QOA_PASS_OCC32 8
-#endif
 template <typename T> struct PassOcc { static constexpr int value = QOA_PASS_OCC64; };
-template <> struct PassOcc<float2> { static constexpr int value = QOA_PASS_OCC32; };
 
 template <typename T>
 __global__ void __launch_bounds__(PASS_THREADS, PassOcc<T>::value)
@@ -826,22 +822,16 @@ cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_
                         cudaStream_t st) {
     return launch_pass_t<double2>(amps, P, norm2_in, partials, st);
 }
-cudaError_t launch_pass_c64(float2* amps, const PassParams& P, const double* norm2_in, double* partials,
-                            cudaStream_t st) {
-    return launch_pass_t<float2>(amps, P, norm2_in, partials, st);
-}
-cudaError_t launch_pass_arena(bool c64, const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start,
-                              uint32_t tiles, int max_nops, int max_ncoef, cudaStream_t st) {
+cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
+                              int max_nops, int max_ncoef, cudaStream_t st) {
     if (!njobs || !tiles) return cudaSuccess;
-    const int esz = c64 ? (int)sizeof(float2) : (int)sizeof(double2);
+    const int esz = (int)sizeof(double2);
     const int tile_bytes = (1 << TILE_BITS) * esz;
     const int smem = tile_bytes + max_nops * 16 + max_ncoef * esz;
     const int smax = tile_bytes + MAX_PASS_OPS * 16 + MAX_PASS_COEF * esz;
-    cudaError_t e = c64 ? cudaFuncSetAttribute(k_pass_arena<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax)
-                        : cudaFuncSetAttribute(k_pass_arena<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_arena<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
     if (e != cudaSuccess) return e;
-    if (c64) k_pass_arena<float2><<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
-    else k_pass_arena<double2><<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
+    k_pass_arena<double2><<<tiles, PASS_THREADS, smem, st>>>(jobs, njobs, tile_start);
     return cudaGetLastError();
 }
 template <typename T>

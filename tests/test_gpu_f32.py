@@ -115,3 +115,22 @@ def test_random_state_and_compare():
         assert r2 > 1.0 and f2 > 0.9
         r3, f3 = a.compare(a)
         assert r3 == 0.0 and abs(f3) < 1e-14
+
+
+@pytest.mark.gpu
+def test_f32_expect_z_and_sampling():
+    n = 13
+    ops = C.random_layered(n, 4, 77, initial_h=True)
+    ref = oracle_run(n, ops)
+    p = np.abs(ref) ** 2
+    idx = np.arange(1 << n)
+    masks = [1, 0b101, (1 << n) - 1, 1 << 12]
+    want = [float(np.sum(np.where(np.array([bin(i & m).count("1") & 1 for i in idx]) == 1, -p, p))) for m in masks]
+    with qb.QuantumState(n, precision="f32") as st:
+        st.execute(C.ops_to_array(ops))
+        got = st.expect_z(masks)
+        shots = st.sample(20000, None, mode=1, rng_seed=3)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-5)
+    hist = np.bincount((shots & 7).astype(np.int64), minlength=8) / len(shots)
+    exp8 = np.array([p[(idx & 7) == k].sum() for k in range(8)])
+    assert np.max(np.abs(hist - exp8)) < 0.02
