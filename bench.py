@@ -461,6 +461,7 @@ def run_batch(args):
         first_s = time.perf_counter() - t2
         b.run()
         info = b.info()
+        traffic = b.traffic()
         stream = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)
         for _ in range(args.warmup):
             b.launch()
@@ -478,11 +479,19 @@ def run_batch(args):
         res = b.results()
         b.close()
         results[prec] = res
+        peak, peak_src = measured_peaks()
+        arena_gbs = traffic["arena_pass_bytes"] / (ms / 1e3) / 1e9
         results[prec + "_line"] = {
             "value": count / (ms / 1e3), "ms_per_step": ms, "tuning": tuning or "defaults",
+            "roofline": {"bound": "hbm", "achieved": arena_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": arena_gbs / peak, "traffic_basis": "arena tile-pass bytes (2 x state per pass) "
+                         "over the whole batch step (small circuits and expectation values included in the time)",
+                         "arena_pass_bytes": traffic["arena_pass_bytes"], "rounds": traffic["rounds"],
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})"},
             "autotune_s": tune_s, "first_run_s": first_s, "routes": info, "clocks": clk,
             "gates_per_s": gates / (ms / 1e3)}
     prim = args.precisions.split(",")[0]
+    out.update(roofline=results[prim + "_line"]["roofline"])
     out.update(value=results[prim + "_line"]["value"], ms_per_step=results[prim + "_line"]["ms_per_step"],
                dtype="f64" if prim == "f64" else "complex64 (3xTF32)", clocks=results[prim + "_line"]["clocks"])
     for prec in args.precisions.split(","):
@@ -581,11 +590,18 @@ def run_serve(args):
                 if x["status"] == 0:
                     srv.take_shots(x["id"], int(x["shots"]))
         lat = np.array([x["t_done"] - x["t_submit"] for x in res])
+        buckets = {}
+        for lo_n, hi_n in ((10, 14), (15, 19), (20, 24), (25, 28)):
+            sel = np.array([lo_n <= x["n"] <= hi_n for x in res])
+            if sel.any():
+                buckets[f"n{lo_n}-{hi_n}"] = {"requests": int(sel.sum()),
+                                              "p50_latency_s": float(np.percentile(lat[sel], 50)),
+                                              "p99_latency_s": float(np.percentile(lat[sel], 99))}
         first = min(x["t_submit"] for x in res)
         last = max(x["t_done"] for x in res)
         out[prec] = {"value": len(res) / (last - first), "p50_latency_s": float(np.percentile(lat, 50)),
                      "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": last - first,
-                     "failed": sum(1 for x in res if x["status"] != 0),
+                     "failed": sum(1 for x in res if x["status"] != 0), "by_qubits": buckets,
                      "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": args.serve_workers,
                      "ran_in": {"f64": sum(1 for x in res if x["precision"] == 0),
                                 "f32": sum(1 for x in res if x["precision"] == 1)}}

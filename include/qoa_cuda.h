@@ -238,6 +238,9 @@ int qoa_batch_launch(qoa_batch_t b);
 int qoa_batch_stream(qoa_batch_t b, void** stream);
 int qoa_batch_results(qoa_batch_t b, double* out, size_t count);
 int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t* large, uint32_t* graph_ready);
+/* Algorithmic bytes of one run's arena tile passes (each pass reads and
+ * writes its circuit's state once) and the number of pass rounds. */
+int qoa_batch_traffic(qoa_batch_t b, double* arena_pass_bytes, uint32_t* rounds);
 const char* qoa_batch_last_error(qoa_batch_t b);
 int qoa_batch_destroy(qoa_batch_t b);
 

@@ -117,6 +117,7 @@ def _load() -> ctypes.CDLL:
         "qoa_batch_launch": (i32, [vp]),
         "qoa_batch_stream": (i32, [vp, P(vp)]),
         "qoa_batch_info": (i32, [vp, P(u32), P(u32), P(u32), P(u32)]),
+        "qoa_batch_traffic": (i32, [vp, P(dbl), P(u32)]),
         "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
         "qoa_batch_destroy": (i32, [vp]),
         "qoa_server_create": (i32, [P(ServerConfig), P(vp)]),
@@ -550,6 +551,11 @@ class Batch:
         v = [ctypes.c_uint32() for _ in range(4)]
         self._check(lib.qoa_batch_info(self._h, *[ctypes.byref(x) for x in v]))
         return dict(zip(("circuits", "small", "large", "graph_ready"), (x.value for x in v)))
+
+    def traffic(self) -> dict:
+        by, rounds = ctypes.c_double(), ctypes.c_uint32()
+        self._check(lib.qoa_batch_traffic(self._h, ctypes.byref(by), ctypes.byref(rounds)))
+        return {"arena_pass_bytes": by.value, "rounds": rounds.value}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -1773,6 +1773,7 @@ struct qoa_batch_s {
     uint32_t* d_tstart = nullptr;
     struct Round { uint32_t job_off, njobs, tiles; int max_nops, max_ncoef; };
     std::vector<Round> rounds;
+    double arena_pass_bytes = 0;   // algorithmic bytes of one run's arena passes
     uint32_t narena = 0;
     // expectation values of arena and view circuits
     ExpzJob* d_ejobs = nullptr;
@@ -1849,6 +1850,7 @@ void batch_free_device(qoa_batch_t b) {
     dfree(b->arena); dfree(b->d_small); dfree(b->d_ops); dfree(b->d_masks); dfree(b->d_out); dfree(b->d_counter);
     dfree(b->d_params); dfree(b->d_f32); dfree(b->d_jobs); dfree(b->d_tstart); dfree(b->d_ejobs); dfree(b->d_epart);
     b->rounds.clear();
+    b->arena_pass_bytes = 0;
     b->nsmall = b->narena = b->n_ejobs = b->e_chunks = 0;
     b->prepared = false;
     b->runs = 0;
@@ -1985,6 +1987,7 @@ int batch_prepare(qoa_batch_t b) {
             jobs.push_back(J);
             tstart.push_back(R.tiles);
             R.tiles += 1u << (c.n - TILE_BITS);
+            b->arena_pass_bytes += 2.0 * (double)esz * std::ldexp(1.0, (int)c.n);
             R.njobs++;
             if (!tensor) {
                 R.max_nops = std::max(R.max_nops, (int)p64[pi].nops);
@@ -2659,6 +2662,13 @@ int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t*
     if (small) *small = b->nsmall;
     if (large) *large = b->narena + (uint32_t)b->views.size();
     if (graph_ready) *graph_ready = b->exec ? 1u : 0u;
+    return QOA_OK;
+}
+
+int qoa_batch_traffic(qoa_batch_t b, double* arena_pass_bytes, uint32_t* rounds) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    if (arena_pass_bytes) *arena_pass_bytes = b->arena_pass_bytes;
+    if (rounds) *rounds = (uint32_t)b->rounds.size();
     return QOA_OK;
 }
 

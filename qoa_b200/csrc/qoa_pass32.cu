@@ -465,14 +465,18 @@ __device__ __forceinline__ void pass_tile_p32x2(float2* __restrict__ amps, const
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int nout = (int)P.n - TILE_BITS;
-    uint64_t blk[2] = {blk0, blk0 | (1ull << (nout - 1))};
-    uint64_t g0[2] = {0, 0};
+    const uint64_t blk[2] = {blk0, blk0 | (1ull << (nout - 1))};
+    // tile origins are rebuilt where they are needed (load, store) rather
+    // than held in registers through the op loop
+    auto origin = [&](int h) {
+        uint64_t g = 0;
+        for (int k = 0; k < nout; ++k) g |= ((blk[h] >> k) & 1ull) << P.outer_qubits[k];
+        return g;
+    };
     uint32_t T[2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        for (int k = 0; k < nout; ++k) g0[h] |= ((blk[h] >> k) & 1ull) << P.outer_qubits[k];
+    for (int h = 0; h < 2; ++h)
         T[h] = (uint32_t)lane | ((uint32_t)wid << LANE_BITS) | ((uint32_t)blk[h] << (LANE_BITS + WARP_BITS));
-    }
     const uint32_t nops = P.nops;
     uint4* sops = reinterpret_cast<uint4*>(tile1 + (1 << TILE_BITS));
     float2* scoef = reinterpret_cast<float2*>(sops + nops);
@@ -506,7 +510,7 @@ __device__ __forceinline__ void pass_tile_p32x2(float2* __restrict__ amps, const
         for (int k = 0; k < REG_BITS; ++k) rst[k] = tstride(P, P.map0.reg[k]);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            uint64_t tb = g0[h] + (uint64_t)lane;
+            uint64_t tb = origin(h) + (uint64_t)lane;
 #pragma unroll
             for (int k = 0; k < WARP_BITS; ++k)
                 if ((wid >> k) & 1) tb += tstride(P, P.map0.warp[k]);
@@ -703,7 +707,7 @@ __device__ __forceinline__ void pass_tile_p32x2(float2* __restrict__ amps, const
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const u64p cr = bc(pend[h].x), ci = bc(pend[h].y);
-            uint64_t tb = g0[h] + (uint64_t)lane;
+            uint64_t tb = origin(h) + (uint64_t)lane;
 #pragma unroll
             for (int k = 0; k < WARP_BITS; ++k)
                 if ((wid >> k) & 1) tb += 1ull << P.out_qubit[mf.warp[k]];
