@@ -363,6 +363,43 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
              int32_t* pass_of, int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits,
              double* gate_matrix, size_t* ngates, size_t* npasses);
 
+/* ---- generated pass kernels ------------------------------------------------ */
+/* No counterpart in the reference (its gates are fixed shaders / CPU loops).
+ * A complex128 tile pass can run as the interpreter kernel (k_pass, which
+ * reads the pass's op stream) or as a kernel generated for that pass: CUDA
+ * C++ with every register bit, condition and exchange address a literal,
+ * compiled at run time by NVRTC for sm_100a. Coefficients stay parameters, so
+ * one compiled kernel serves every pass of the same structure (repeated
+ * circuits, angle sweeps); compiled kernels are cached for the process.
+ * Results are identical either way. Per handle:
+ *   QOA_JIT_OFF    interpret every pass
+ *   QOA_JIT_ASYNC  (default) request the kernels, interpret passes whose
+ *                  kernel is still compiling (on one background thread)
+ *   QOA_JIT_SYNC   compile before the first launch
+ * States below min_qubits (default 20) always interpret. */
+#define QOA_JIT_OFF   0
+#define QOA_JIT_ASYNC 1
+#define QOA_JIT_SYNC  2
+int qoa_set_jit(qoa_state_t s, int mode, uint32_t min_qubits);
+/* Blocks until every compile requested so far has finished. */
+int qoa_jit_wait(void);
+typedef struct qoa_jit_stats {
+    uint64_t kernels;    /* compiled pass kernels in the process cache */
+    uint64_t hits;       /* pass requests served from the cache */
+    uint64_t misses;     /* pass requests that were compiled */
+    uint64_t failures;   /* kernels whose compile or load failed (see qoa_last_error(NULL)) */
+    uint64_t launches;   /* generated-kernel passes run by this handle (0 when s is NULL) */
+    double compile_ms;   /* total compile + load time */
+} qoa_jit_stats;
+int qoa_jit_stats_get(qoa_state_t s, qoa_jit_stats* out);
+/* Host only, no GPU needed: plans an op list for an n-qubit complex128 state
+ * and writes the generated source of each pass's kernel (concatenated, NUL
+ * terminated, truncated to cap; *len = full length) and the pass count.
+ * compile != 0 also compiles it with NVRTC (nothing is loaded) and fails
+ * with QOA_E_ARG and the compiler log when it does not compile. */
+int qoa_jit_translate(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int compile, char* out,
+                      size_t cap, size_t* len, size_t* npasses);
+
 /* ---- allocation-free entry point ----------------------------------------- */
 /* No counterpart in the reference. <Z_mask> = sum_i (-1)^popcount(i & mask)
  * |a_i|^2 over a state vector the CALLER owns in device memory (`d_amps`,

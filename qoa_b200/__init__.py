@@ -29,6 +29,7 @@ QOA_PREC_F64 = 0
 QOA_PREC_F32 = 1
 QOA_FLAG_COMPAT_MASK_QUIRK = 0x1
 QOA_FLAG_F32_TENSOR = 0x10
+QOA_JIT_OFF, QOA_JIT_ASYNC, QOA_JIT_SYNC = 0, 1, 2
 QOA_FLAG_PER_GATE = 0x2
 QOA_FLAG_PROFILE = 0x4
 QOA_FLAG_NOISE_GATE_QUBITS = 0x8
@@ -43,6 +44,11 @@ class QoaError(RuntimeError):
 class QoaStatus(ctypes.Structure):
     _fields_ = [("nan_seen", ctypes.c_uint32), ("inf_seen", ctypes.c_uint32),
                 ("zero_norm_resets", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class JitStats(ctypes.Structure):
+    _fields_ = [("kernels", ctypes.c_uint64), ("hits", ctypes.c_uint64), ("misses", ctypes.c_uint64),
+                ("failures", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("compile_ms", ctypes.c_double)]
 
 
 class BatchTuning(ctypes.Structure):
@@ -135,6 +141,10 @@ def _load() -> ctypes.CDLL:
         "qoa_get_noise": (i32, [vp, P(ctypes.c_int), P(dbl)]),
         "qoa_get_precision": (i32, [vp, P(ctypes.c_int)]),
         "qoa_plan": (i32, [u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, P(sz), P(sz)]),
+        "qoa_set_jit": (i32, [vp, i32, u32]),
+        "qoa_jit_wait": (i32, []),
+        "qoa_jit_stats_get": (i32, [vp, P(JitStats)]),
+        "qoa_jit_translate": (i32, [u32, u32, vp, sz, i32, vp, sz, P(sz), P(sz)]),
         "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
         "qoa_vec_apply_x": (i32, [vp, sz, sz]),
         "qoa_vec_apply_y": (i32, [vp, sz, sz]),
@@ -436,6 +446,16 @@ class QuantumState:
         _check(lib.qoa_stream(self._h, ctypes.byref(p)), self._h)
         return int(p.value or 0)
 
+    def set_jit(self, mode: int = QOA_JIT_ASYNC, min_qubits: int = 20):
+        """Generated pass kernels for this handle: QOA_JIT_OFF / _ASYNC / _SYNC,
+        for states of at least min_qubits qubits."""
+        _check(lib.qoa_set_jit(self._h, int(mode), int(min_qubits)), self._h)
+
+    def jit_stats(self) -> dict:
+        st = JitStats()
+        _check(lib.qoa_jit_stats_get(self._h, ctypes.byref(st)), self._h)
+        return {f: getattr(st, f) for f, _ in JitStats._fields_}
+
     def launch_count(self) -> int:
         v = ctypes.c_uint64()
         _check(lib.qoa_launch_count(self._h, ctypes.byref(v)), self._h)
@@ -469,6 +489,30 @@ def plan(n: int, ops, flags: int = 0):
     k = ng.value
     return {"pass_of": pass_of[:k], "order": order[:k], "kind": kind[:k], "qubits": qubits[:k],
             "matrix": mat[:k], "npasses": npasses.value}
+
+
+def jit_wait():
+    """Blocks until every requested pass-kernel compile has finished."""
+    _check(lib.qoa_jit_wait())
+
+
+def jit_stats() -> dict:
+    st = JitStats()
+    _check(lib.qoa_jit_stats_get(None, ctypes.byref(st)))
+    return {f: getattr(st, f) for f, _ in JitStats._fields_}
+
+
+def jit_translate(n: int, ops, flags: int = 0, compile: bool = False):
+    """Host only: the generated CUDA source of every tile pass of `ops` on an
+    n-qubit complex128 state, and the pass count; compile=True also compiles
+    it with NVRTC (raises QoaError with the log if it does not compile)."""
+    arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
+    ln, npasses = ctypes.c_size_t(), ctypes.c_size_t()
+    _check(lib.qoa_jit_translate(n, flags, _ptr(arr), len(arr), 0, None, 0, ctypes.byref(ln), ctypes.byref(npasses)))
+    buf = ctypes.create_string_buffer(ln.value + 1)
+    _check(lib.qoa_jit_translate(n, flags, _ptr(arr), len(arr), 1 if compile else 0, buf, ln.value + 1,
+                                 ctypes.byref(ln), ctypes.byref(npasses)))
+    return buf.value.decode(), npasses.value
 
 
 def vec_call(name: str, amps: np.ndarray, *args) -> int:

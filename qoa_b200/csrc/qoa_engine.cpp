@@ -11,6 +11,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
+#include <functional>
+#include <atomic>
 #include <complex>
 #include <cmath>
 #include <cstdarg>
@@ -24,6 +27,7 @@
 
 #include "../../include/qoa_cuda.h"
 #include "qoa_kernels.cuh"
+#include "qoa_jit.h"
 
 namespace qoa {
 cudaError_t launch_pass(double2* amps, const PassParams& P, const double* norm2_in, double* partials, cudaStream_t st);
@@ -191,6 +195,9 @@ struct qoa_state_s {
     double noise_p = 0.0;
     uint64_t launches = 0;
     uint32_t host_resets = 0;     // normalize() resets decided on the host
+    int jit_mode = QOA_JIT_ASYNC;   // generated complex128 pass kernels (qoa_jit.cpp)
+    uint32_t jit_min_qubits = 20;   // smaller states interpret their passes
+    uint64_t jit_launches = 0;
     std::string err;
     // profiling
     struct Rec { cudaEvent_t a, b; double bytes; int kind; };
@@ -1387,6 +1394,23 @@ int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
     return QOA_OK;
 }
 
+// A complex128 pass whose parameters were built ahead (with its generated
+// kernel requested): the generated kernel when it is ready, else k_pass.
+int run_pass_built(qoa_state_t s, const PassParams& P, const JitKernel& jk) {
+    {
+        Timer tm(s, 2.0 * std::ldexp(16.0, (int)s->n), 0);
+        if (jk.ready()) {
+            CK(jk.launch(s->amps, P, s->scal, s->partials, s->stream));
+            s->jit_launches++;
+        } else {
+            CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
+        }
+    }
+    CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
+    s->launches += 2;
+    return QOA_OK;
+}
+
 // Reads norm2, P0, P1 of qubit q (logical probabilities) to the host.
 int read_p01(qoa_state_t s, uint32_t q, double& p0, double& p1, double& norm2) {
     CK(launch_p01(s->amps, state_len(s), q, s->partials, s->scal + 1, s->scal, s->stream));
@@ -1616,9 +1640,30 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         std::vector<Gate> seg(G.begin() + i, G.begin() + j);
         if (!per_gate) merge_swap_blocks(seg);
         std::vector<Step> steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
-        for (const Step& st : steps) {
+        // complex128 passes of a large state: built ahead, and their
+        // generated kernels requested from the compile cache
+        std::vector<PassParams> built;
+        std::vector<int> built_of(steps.size(), -1);
+        std::vector<JitKernel> jk;
+        if (!c64 && !per_gate && s->jit_mode != QOA_JIT_OFF && s->n >= s->jit_min_qubits) {
+            size_t np = 0;
+            for (const Step& st : steps) np += st.pass ? 1 : 0;
+            built.resize(np);
+            std::vector<std::string> bodies;
+            size_t b = 0;
+            for (size_t k = 0; k < steps.size(); ++k) {
+                if (!steps[k].pass || build_pass(seg, steps[k], s->n, built[b]) != 0) continue;
+                built_of[k] = (int)b;
+                bodies.push_back(jit_pass_body(built[b]));
+                ++b;
+            }
+            jk = jit_request(bodies, s->jit_mode == QOA_JIT_SYNC);
+        }
+        for (size_t k = 0; k < steps.size(); ++k) {
+            const Step& st = steps[k];
             int rc;
-            if (st.pass) rc = run_pass(s, seg, st);
+            if (st.pass && built_of[k] >= 0) rc = run_pass_built(s, built[built_of[k]], jk[built_of[k]]);
+            else if (st.pass) rc = run_pass(s, seg, st);
             else {
                 const Gate& g = seg[st.gates[0]];
                 switch (g.kind) {
@@ -1887,10 +1932,59 @@ int batch_prepare(qoa_batch_t b) {
     std::vector<std::vector<uint32_t>> pass_idx(b->circs.size());
     uint32_t maxn = 1;
     size_t total = 0;  // arena bytes
-    for (size_t i = 0; i < b->circs.size(); ++i) {
-        auto& c = b->circs[i];
+    const size_t NC = b->circs.size();
+    std::vector<char> is_small(NC, 0);
+    for (size_t i = 0; i < NC; ++i) {
+        const auto& c = b->circs[i];
         bool small = c.n <= smax || (tensor && c.n < (uint32_t)TILE_BITS);
         for (const Gate& g : c.gates) small = small && small_ok(g);
+        is_small[i] = small;
+    }
+    // Tile-pass route, planned on all host cores: schedule every candidate
+    // circuit, then build all passes into their final slots.
+    std::vector<std::vector<Step>> steps_of(NC);
+    std::vector<char> all_pass(NC, 0), built_ok(NC, 0);
+    std::vector<size_t> pbase(NC, 0);
+    if (!tensor) {
+        auto parallel_for = [](size_t count, const std::function<void(size_t)>& fn) {
+            const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+            std::atomic<size_t> next{0};
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < nt; ++t)
+                pool.emplace_back([&] {
+                    for (size_t k; (k = next.fetch_add(1)) < count;) fn(k);
+                });
+            for (auto& th : pool) th.join();
+        };
+        parallel_for(NC, [&](size_t i) {
+            const auto& c = b->circs[i];
+            if (is_small[i] || c.n < (uint32_t)TILE_BITS || c.gates.empty()) return;
+            steps_of[i] = schedule(c.gates, c.n, false, false, budget);
+            bool ok = true;
+            for (const Step& st : steps_of[i]) ok = ok && st.pass;
+            all_pass[i] = ok;
+        });
+        size_t np = 0;
+        std::vector<std::pair<size_t, size_t>> jobs;  // (circuit, step)
+        for (size_t i = 0; i < NC; ++i)
+            if (all_pass[i]) {
+                pbase[i] = np;
+                for (size_t k = 0; k < steps_of[i].size(); ++k) jobs.push_back({i, k});
+                np += steps_of[i].size();
+            }
+        p64.resize(np);
+        std::vector<char> step_ok(jobs.size(), 0);
+        parallel_for(jobs.size(), [&](size_t x) {
+            const size_t i = jobs[x].first, k = jobs[x].second;
+            step_ok[x] = build_pass(b->circs[i].gates, steps_of[i][k], b->circs[i].n, p64[pbase[i] + k]) == 0;
+        });
+        for (size_t i = 0; i < NC; ++i) built_ok[i] = all_pass[i];
+        for (size_t x = 0; x < jobs.size(); ++x)
+            if (!step_ok[x]) built_ok[jobs[x].first] = 0;
+    }
+    for (size_t i = 0; i < NC; ++i) {
+        auto& c = b->circs[i];
+        const bool small = is_small[i];
         if (small) {
             if (c.n > cap) return bset_err(b, QOA_E_ARG, "circuit too large for the shared-memory kernel");
             c.route = R_SMALL;
@@ -1909,28 +2003,26 @@ int batch_prepare(qoa_batch_t b) {
         if (tensor && c.n < (uint32_t)TILE_BITS)
             return bset_err(b, QOA_E_ARG, "circuit below the FP32 tile size with a gate the small kernel lacks");
         c.route = R_VIEW;
-        if (c.n >= (uint32_t)TILE_BITS && !c.gates.empty()) {
+        if (!tensor) {
+            if (built_ok[i]) {
+                for (size_t k = 0; k < steps_of[i].size(); ++k) pass_idx[i].push_back((uint32_t)(pbase[i] + k));
+                c.route = R_ARENA;
+            }
+        } else if (c.n >= (uint32_t)TILE_BITS && !c.gates.empty()) {
             std::vector<Step> steps = schedule(c.gates, c.n, false, tensor, budget);
             bool ok = true;
             for (const Step& st : steps) ok = ok && st.pass;
-            if (ok && !tensor) {
-                const size_t base = p64.size();
-                p64.resize(base + steps.size());
-                for (size_t k = 0; k < steps.size() && ok; ++k) ok = build_pass(c.gates, steps[k], c.n, p64[base + k]) == 0;
-                if (!ok) p64.resize(base);
-                else
-                    for (size_t k = 0; k < steps.size(); ++k) pass_idx[i].push_back((uint32_t)(base + k));
-            } else if (ok) {
+            if (ok) {
                 const size_t base = p32.size();
                 p32.resize(base + steps.size());
                 for (size_t k = 0; k < steps.size(); ++k)
                     if (build_f32_pass(c.gates, steps[k], c.n, p32[base + k], up) != 0)
                         return bset_err(b, QOA_E_ARG, "FP32 pass does not fit one launch");
                 for (size_t k = 0; k < steps.size(); ++k) pass_idx[i].push_back((uint32_t)(base + k));
-            } else if (tensor) {
+            } else {
                 return bset_err(b, QOA_E_OPCODE, "gate outside an FP32 pass");
             }
-            if (ok) c.route = R_ARENA;
+            c.route = R_ARENA;
         }
         c.state_off = total;
         total = al(total + (esz << c.n));
@@ -2803,6 +2895,72 @@ int qoa_get_noise(qoa_state_t s, int* mode, double* p) {
 int qoa_get_precision(qoa_state_t s, int* precision) {
     if (!s || !precision) return set_err(s, QOA_E_ARG, "null argument");
     *precision = s->precision;
+    return QOA_OK;
+}
+
+int qoa_set_jit(qoa_state_t s, int mode, uint32_t min_qubits) {
+    if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
+    if (mode != QOA_JIT_OFF && mode != QOA_JIT_ASYNC && mode != QOA_JIT_SYNC)
+        return set_err(s, QOA_E_ARG, "unknown jit mode %d", mode);
+    s->jit_mode = mode;
+    s->jit_min_qubits = std::max<uint32_t>(min_qubits, TILE_BITS);
+    return QOA_OK;
+}
+
+int qoa_jit_wait(void) {
+    jit_wait_all();
+    return QOA_OK;
+}
+
+int qoa_jit_stats_get(qoa_state_t s, qoa_jit_stats* out) {
+    if (!out) return set_err(s, QOA_E_ARG, "null argument");
+    const JitStats j = jit_stats();
+    out->kernels = j.kernels;
+    out->hits = j.hits;
+    out->misses = j.misses;
+    out->failures = j.failures;
+    out->compile_ms = j.compile_ms;
+    out->launches = s ? s->jit_launches : 0;
+    if (j.failures) set_err(nullptr, QOA_E_CUDA, "%s", jit_last_error().c_str());
+    return QOA_OK;
+}
+
+int qoa_jit_translate(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int compile, char* out,
+                      size_t cap, size_t* len, size_t* npasses) {
+    if ((!ops && nops) || (!out && cap)) return set_err(nullptr, QOA_E_ARG, "null argument");
+    if (n < (uint32_t)TILE_BITS || n > 36) return set_err(nullptr, QOA_E_ARG, "tile passes need 11..36 qubits");
+    Expander ex;
+    ex.n = n;
+    ex.flags = flags;
+    ex.s = nullptr;
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    std::vector<Gate>& G = ex.out;
+    for (const Gate& g : G)
+        if (g.kind == K_QINIT) return set_err(nullptr, QOA_E_ARG, "qoa_jit_translate does not take QINIT");
+    merge_swap_blocks(G);
+    std::vector<Step> steps = schedule(G, n, false);
+    std::vector<std::string> bodies;
+    static thread_local PassParams P;
+    for (const Step& st : steps) {
+        if (!st.pass) continue;
+        if (build_pass(G, st, n, P) != 0) return set_err(nullptr, QOA_E_ARG, "a pass does not fit one launch");
+        bodies.push_back(jit_pass_body(P));
+    }
+    if (npasses) *npasses = bodies.size();
+    const std::string text = jit_program(bodies);
+    if (len) *len = text.size();
+    if (cap) {
+        const size_t k = std::min(cap - 1, text.size());
+        memcpy(out, text.data(), k);
+        out[k] = '\0';
+    }
+    if (compile && !bodies.empty()) {
+        std::string err;
+        if (!jit_compile_only(bodies, err)) return set_err(nullptr, QOA_E_ARG, "%s", err.c_str());
+    }
     return QOA_OK;
 }
 

@@ -1,0 +1,550 @@
+// qoa_jit.cpp — complex128 tile passes generated as CUDA C++ and compiled at
+// run time with NVRTC for sm_100a.
+//
+// The generated kernel does exactly what k_pass does for the same
+// PassParams (qoa_kernels.cu: load under map0, the op stream, exchanges
+// through shared memory, the pending factor, the store under out_qubit and
+// the norm partials), with the interpreter's run-time decisions resolved on
+// the host: each op becomes a call of the same device building block
+// (qoa_pass_dev.cuh) with its register bit, condition masks and coefficient
+// slot as literals, and each exchange a list of 16 shared-memory stores and
+// loads at literal swizzled offsets from one per-thread base. What the
+// interpreter pays per op — fetching and decoding the op, the indirect jump,
+// staging coefficients in shared memory, forming exchange addresses from
+// run-time mappings — disappears, and the compiler schedules across gates.
+#include "qoa_jit.h"
+
+#include <nvrtc.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <algorithm>
+
+namespace qoa {
+
+namespace {
+
+const char kTypesHeader[] =
+#include "qoa_kernels.cuh.inc"
+    ;
+const char kDevHeader[] =
+#include "qoa_pass_dev.cuh.inc"
+    ;
+
+// NVRTC has no C library headers: the fixed-width types the headers use.
+const char kPrelude[] =
+    "typedef unsigned char uint8_t;\n"
+    "typedef unsigned short uint16_t;\n"
+    "typedef unsigned int uint32_t;\n"
+    "typedef int int32_t;\n"
+    "typedef unsigned long long uint64_t;\n"
+    "#include \"qoa_pass_dev.cuh\"\n";
+
+// Resident CTAs per SM of a generated pass (128 threads): the same register
+// budget as k_pass.
+constexpr int JIT_OCC = 4;
+
+uint32_t spos_host(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
+
+struct Emit {
+    std::string s;
+    void line(const char* fmt, ...) __attribute__((format(printf, 2, 3))) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        s += buf;
+        s += '\n';
+    }
+};
+
+const char* g1_name(int code) {
+    switch (code & ~3) {
+        case PC_HF: return "G1_HF";
+        case PC_RX: return "G1_RXA";
+        case PC_RY: return "G1_RYA";
+        case PC_RXB: return "G1_RXB";
+        case PC_RYB: return "G1_RYB";
+        case PC_GEN: return "G1_GEN";
+        default: return nullptr;
+    }
+}
+
+// "(tw & m) == m" or "true"
+std::string tcond(uint32_t tm) {
+    if (!tm) return "true";
+    char b[64];
+    snprintf(b, sizeof b, "((tw & 0x%xu) == 0x%xu)", tm, tm);
+    return b;
+}
+
+// Tile index (shared-memory bits) of this thread's register 0 under map m:
+// lane bit i sits at tile bit m.lane[i], warp bit i at m.warp[i].
+std::string tile_base(const TileMap& m) {
+    std::string e = "0u";
+    char b[96];
+    for (int i = 0; i < LANE_BITS; ++i) {
+        snprintf(b, sizeof b, " | ((((uint32_t)lane >> %d) & 1u) << %d)", i, m.lane[i]);
+        e += b;
+    }
+    for (int i = 0; i < WARP_BITS; ++i) {
+        snprintf(b, sizeof b, " | ((((uint32_t)wid >> %d) & 1u) << %d)", i, m.warp[i]);
+        e += b;
+    }
+    return e;
+}
+
+// Swizzled offset of register v's tile-index part under map m (spos is
+// linear over XOR, and lane/warp and register bits are disjoint).
+uint32_t reg_part(const TileMap& m, int v) {
+    uint32_t j = 0;
+    for (int k = 0; k < REG_BITS; ++k)
+        if ((v >> k) & 1) j |= 1u << m.reg[k];
+    return spos_host(j);
+}
+
+}  // namespace
+
+std::string jit_pass_body(const PassParams& P) {
+    Emit E;
+    E.line("(double2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
+    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials) {");
+    E.line("using namespace qoa;");
+    E.line("typedef double2 T;");
+    E.line("__shared__ __align__(16) T tile[1 << TILE_BITS];");
+    E.line("__shared__ double red[PASS_THREADS / 32];");
+    if (P.nang) E.line("__shared__ T sang[%u];", P.nang);
+    E.line("const int lane = threadIdx.x & 31;");
+    E.line("const int wid = threadIdx.x >> 5;");
+    E.line("const uint64_t blk = blockIdx.x;");
+    E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
+           LANE_BITS + WARP_BITS);
+    // tile origin: the tile number's bits deposited into the outer qubits,
+    // one shift per run of consecutive qubits
+    {
+        std::string g = "0ull";
+        const int nout = (int)P.n - TILE_BITS;
+        char b[128];
+        for (int k = 0; k < nout;) {
+            int len = 1;
+            while (k + len < nout && P.outer_qubits[k + len] == P.outer_qubits[k] + len) ++len;
+            snprintf(b, sizeof b, " | (((blk >> %d) & 0x%llxull) << %d)", k,
+                     (unsigned long long)((len >= 64) ? ~0ull : ((1ull << len) - 1)), P.outer_qubits[k]);
+            g += b;
+            k += len;
+        }
+        E.line("const uint64_t g0 = %s;", g.c_str());
+    }
+    E.line("const double nrm = *norm2_in;");
+    if (P.nang) E.line("pass_angles(P, blk, sang);");
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("T pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;");
+    E.line("T a[REGS];");
+    auto stride = [&](int t) -> unsigned long long {
+        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+    };
+    {
+        const TileMap& m = P.map0;
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        unsigned long long off[REGS];
+        for (int v = 0; v < REGS; ++v) {
+            off[v] = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) off[v] += stride(m.reg[k]);
+        }
+        E.line("if (valid) {");
+        for (int v = 0; v < REGS; ++v) E.line("a[%d] = __ldcs(amps + (tb + 0x%llxull));", v, off[v]);
+        E.line("} else {");
+        for (int v = 0; v < REGS; ++v) E.line("a[%d] = make_double2(tb + 0x%llxull == 0 ? 1.0 : 0.0, 0.0);", v, off[v]);
+        E.line("}");
+        E.line("}");
+    }
+    if (P.nang) E.line("__syncthreads();");
+
+    const TileMap* cur = &P.map0;
+    const uint32_t* ow = reinterpret_cast<const uint32_t*>(P.ops);
+    for (uint32_t oi = 0; oi < P.nops; ++oi) {
+        const PassOp& op = P.ops[oi];
+        const int code = op.code;
+        const uint32_t c = op.coef;
+        const uint32_t cr = op.cond_reg;
+        const uint32_t tm = ow[4 * oi + 2];
+        if (code >= PC_HF && code < PC_XC) {
+            E.line("g1r<%s, %d>(a, P.coef + %u);", g1_name(code), code & 3, c);
+        } else if (code >= PC_RXB && code < PC_DIAG_TA) {
+            E.line("g1r<%s, %d>(a, P.coef + %u);", g1_name(code), code & 3, c);
+        } else if (code >= PC_XC && code < PC_RXB) {
+            E.line("g1rc<%s, %d>(a, %s, 0x%xu);", (code & ~3) == PC_XC ? "G1_X" : "G1_Y", code & 3,
+                   tcond(tm).c_str(), cr);
+        } else {
+            switch (code) {
+                case PC_DIAG_T:
+                    if (tm) E.line("if (%s) pend = c_mul(pend, P.coef[%u]);", tcond(tm).c_str(), c);
+                    else E.line("pend = c_mul(pend, P.coef[%u]);", c);
+                    break;
+                case PC_DIAG_M:
+                    E.line("diag_m(a, %s, 0x%xu, P.coef[%u]);", tcond(tm).c_str(), cr, c);
+                    break;
+                case PC_DIAG_TA:
+                    if (tm) E.line("if (%s) pend = c_mul(pend, sang[%u]);", tcond(tm).c_str(), c);
+                    else E.line("pend = c_mul(pend, sang[%u]);", c);
+                    break;
+                case PC_DIAG_MA:
+                    E.line("diag_m(a, true, 0x%xu, sang[%u]);", cr, c);
+                    break;
+                case PC_DIAG_MX:
+                case PC_DIAG_TM: {
+                    // the entries' thread-conditioned factors folded into f;
+                    // MX applies f to its register mask at the end of each run
+                    const uint32_t cnt = op.k;
+                    bool one = true;  // f is known to be 1
+                    E.line("{ T f = make_double2(1.0, 0.0);");
+                    for (uint32_t e = 1; e <= cnt; ++e) {
+                        const PassOp& r = P.ops[oi + e];
+                        const uint32_t rtm = ow[4 * (oi + e) + 2];
+                        if (!rtm && one) E.line("f = P.coef[%u];", (unsigned)r.coef);
+                        else if (one) E.line("f = %s ? P.coef[%u] : make_double2(1.0, 0.0);", tcond(rtm).c_str(), (unsigned)r.coef);
+                        else if (!rtm) E.line("f = c_mul(f, P.coef[%u]);", (unsigned)r.coef);
+                        else E.line("if (%s) f = c_mul(f, P.coef[%u]);", tcond(rtm).c_str(), (unsigned)r.coef);
+                        one = false;
+                        if (code == PC_DIAG_MX && (e == cnt || ((r.has_tp >> 1) & 1u))) {
+                            E.line("diag_m(a, true, 0x%xu, f);", (unsigned)r.cond_reg);
+                            if (e != cnt) E.line("f = make_double2(1.0, 0.0);");
+                            one = true;
+                        }
+                    }
+                    if (code == PC_DIAG_TM && cnt) E.line("pend = c_mul(pend, f);");
+                    E.line("}");
+                    oi += cnt;
+                    break;
+                }
+                case PC_DIAG_TAB:
+                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], P.coef[%u]);", v, v, c + v);
+                    break;
+                case PC_FLUSH:
+                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], pend);", v, v);
+                    E.line("pend = make_double2(1.0, 0.0);");
+                    break;
+                case PC_XCHG: {
+                    const TileMap& mo = *cur;
+                    const TileMap& mn = P.xmap[c];
+                    E.line("__syncthreads();");
+                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mo).c_str());
+                    for (int v = 0; v < REGS; ++v) E.line("tile[pb ^ %uu] = a[%d];", reg_part(mo, v), v);
+                    E.line("}");
+                    E.line("__syncthreads();");
+                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mn).c_str());
+                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[pb ^ %uu];", v, reg_part(mn, v));
+                    E.line("}");
+                    cur = &mn;
+                    break;
+                }
+                default: break;  // PC_NOP
+            }
+        }
+    }
+
+    // store under the final mapping: tile bit t goes to qubit out_qubit[t]
+    {
+        const TileMap& m = *cur;
+        auto ostride = [&](int t) -> unsigned long long { return 1ull << P.out_qubit[t]; };
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               ostride(m.warp[0]), ostride(m.warp[1]));
+        E.line("double ss = 0.0;");
+        for (int v = 0; v < REGS; ++v) {
+            unsigned long long off = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) off += ostride(m.reg[k]);
+            E.line("{ const T x = c_mul(a[%d], pend); __stcs(amps + (tb + 0x%llxull), x); ss += c_abs2(x); }", v, off);
+        }
+        E.line("block_norm_partial(ss, red, partials + blk);");
+        E.line("}");
+    }
+    E.line("}");
+    return E.s;
+}
+
+// ------------------------------------------------------------ the cache
+struct JitEntry {
+    std::atomic<int> state{0};  // 0 compiling, 1 ready, 2 failed
+    cudaKernel_t kernel = nullptr;
+    std::string name;
+};
+
+bool JitKernel::ready() const { return e_ && e_->state.load(std::memory_order_acquire) == 1; }
+bool JitKernel::failed() const { return !e_ || e_->state.load(std::memory_order_acquire) == 2; }
+
+cudaError_t JitKernel::launch(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                              cudaStream_t st) const {
+    if (!ready()) return cudaErrorNotReady;
+    void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials};
+    const unsigned blocks = 1u << (P.n - TILE_BITS);
+    return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(blocks), dim3(PASS_THREADS), args, 0, st);
+}
+
+namespace {
+
+uint64_t fnv64(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char ch : s) {
+        h ^= ch;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+std::string program_text(const std::vector<std::string>& names, const std::vector<std::string>& bodies) {
+    std::string src = kPrelude;
+    char head[160];
+    for (size_t i = 0; i < names.size(); ++i) {
+        snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS, JIT_OCC,
+                 names[i].c_str());
+        src += head;
+        src += bodies[i];
+    }
+    return src;
+}
+
+// NVRTC: the kernels named names[i] with bodies[i], as one sm_100a cubin.
+bool build_cubin(const std::vector<std::string>& names, const std::vector<std::string>& bodies,
+                 std::vector<char>& cubin, std::string& err) {
+    const std::string src = program_text(names, bodies);
+    const char* hdrs[] = {kTypesHeader, kDevHeader};
+    const char* hnames[] = {"qoa_kernels.cuh", "qoa_pass_dev.cuh"};
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src.c_str(), "qoa_jit_pass.cu", 2, hdrs, hnames) != NVRTC_SUCCESS) {
+        err = "nvrtcCreateProgram failed";
+        return false;
+    }
+    const char* opts[] = {"-arch=sm_100a", "-std=c++17", "--fmad=true"};
+    const nvrtcResult rc = nvrtcCompileProgram(prog, 3, opts);
+    if (rc != NVRTC_SUCCESS) {
+        size_t n = 0;
+        nvrtcGetProgramLogSize(prog, &n);
+        std::string log(n, '\0');
+        if (n) nvrtcGetProgramLog(prog, &log[0]);
+        err = std::string("NVRTC: ") + nvrtcGetErrorString(rc) + ": " + log.substr(0, 2000);
+        nvrtcDestroyProgram(&prog);
+        return false;
+    }
+    size_t cs = 0;
+    nvrtcGetCUBINSize(prog, &cs);
+    cubin.resize(cs);
+    nvrtcGetCUBIN(prog, cubin.data());
+    nvrtcDestroyProgram(&prog);
+    return true;
+}
+
+std::string kernel_name(const std::string& body) {
+    char nm[40];
+    snprintf(nm, sizeof nm, "qoa_jit_pass_%016llx", (unsigned long long)fnv64(body));
+    return nm;
+}
+
+// One kernel per NVRTC program: the kernels of a circuit compile side by
+// side on a pool of host threads.
+struct JitJob {
+    std::shared_ptr<JitEntry> entry;
+    std::string body;
+};
+
+class JitCompiler {
+public:
+    ~JitCompiler() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_)
+            if (t.joinable()) t.join();
+    }
+
+    std::vector<JitKernel> request(const std::vector<std::string>& bodies, bool wait) {
+        std::vector<JitKernel> out;
+        std::vector<std::shared_ptr<JitEntry>> mine;
+        out.reserve(bodies.size());
+        bool queued = false;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (const std::string& b : bodies) {
+                auto it = cache_.find(b);
+                if (it != cache_.end()) {
+                    ++hits_;
+                    out.emplace_back(it->second);
+                    mine.push_back(it->second);
+                    continue;
+                }
+                ++misses_;
+                auto e = std::make_shared<JitEntry>();
+                e->name = kernel_name(b);
+                cache_.emplace(b, e);
+                queue_.push_back(JitJob{e, b});
+                ++pending_;
+                queued = true;
+                out.emplace_back(e);
+                mine.push_back(e);
+            }
+            if (queued && workers_.empty()) {
+                const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+                for (unsigned t = 0; t < nt; ++t) workers_.emplace_back([this] { run(); });
+            }
+        }
+        if (queued) cv_.notify_all();
+        if (wait) {
+            std::unique_lock<std::mutex> lk(mu_);
+            done_cv_.wait(lk, [&] {
+                for (auto& e : mine)
+                    if (e->state.load(std::memory_order_acquire) == 0) return false;
+                return true;
+            });
+        }
+        return out;
+    }
+
+    void wait_all() {
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+    JitStats stats() {
+        std::lock_guard<std::mutex> lk(mu_);
+        return JitStats{ready_, hits_, misses_, failures_, compile_ms_};
+    }
+    std::string last_error() {
+        std::lock_guard<std::mutex> lk(mu_);
+        return last_error_;
+    }
+
+private:
+    void run() {
+        // these threads load libraries while other threads may be capturing
+        // graphs: they must not join those captures' rules
+        cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+        cudaThreadExchangeStreamCaptureMode(&mode);
+        for (;;) {
+            JitJob job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+                if (stop_) return;
+                job = std::move(queue_.front());
+                queue_.pop_front();
+            }
+            const auto t0 = std::chrono::steady_clock::now();
+            std::string err;
+            const bool ok = compile(job, err);
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                compile_ms_ += ms;
+                job.entry->state.store(ok ? 1 : 2, std::memory_order_release);
+                if (ok) ++ready_;
+                else {
+                    ++failures_;
+                    last_error_ = err;
+                }
+                --pending_;
+            }
+            done_cv_.notify_all();
+        }
+    }
+
+    bool compile(JitJob& job, std::string& err) {
+        std::vector<char> cubin;
+        if (!build_cubin({job.entry->name}, {job.body}, cubin, err)) return false;
+        {
+            // at exit the CUDA runtime may already be gone: load nothing
+            std::lock_guard<std::mutex> lk(mu_);
+            if (stop_) {
+                err = "process exiting";
+                return false;
+            }
+        }
+        cudaLibrary_t lib = nullptr;
+        cudaError_t ce = cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            err = std::string("cudaLibraryLoadData: ") + cudaGetErrorString(ce);
+            return false;
+        }
+        // the library stays loaded for the life of the process (the cache
+        // keeps its kernel)
+        cudaKernel_t k = nullptr;
+        if (cudaLibraryGetKernel(&k, lib, job.entry->name.c_str()) != cudaSuccess) {
+            cudaGetLastError();
+            err = "kernel missing from the compiled library: " + job.entry->name;
+            return false;
+        }
+        job.entry->kernel = k;
+        return true;
+    }
+
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::unordered_map<std::string, std::shared_ptr<JitEntry>> cache_;
+    std::deque<JitJob> queue_;
+    std::vector<std::thread> workers_;
+    bool stop_ = false;
+    uint64_t pending_ = 0;
+    uint64_t ready_ = 0, hits_ = 0, misses_ = 0, failures_ = 0;
+    double compile_ms_ = 0.0;
+    std::string last_error_;
+};
+
+JitCompiler& compiler() {
+    static JitCompiler c;
+    return c;
+}
+
+}  // namespace
+
+std::string jit_program(const std::vector<std::string>& bodies) {
+    std::vector<std::string> names;
+    for (const std::string& b : bodies) names.push_back(kernel_name(b));
+    return program_text(names, bodies);
+}
+
+bool jit_compile_only(const std::vector<std::string>& bodies, std::string& err) {
+    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+    std::atomic<size_t> next{0};
+    std::mutex emu;
+    bool ok = true;
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t i; (i = next.fetch_add(1)) < bodies.size();) {
+                std::vector<char> cubin;
+                std::string e;
+                if (!build_cubin({kernel_name(bodies[i])}, {bodies[i]}, cubin, e)) {
+                    std::lock_guard<std::mutex> lk(emu);
+                    if (ok) err = e;
+                    ok = false;
+                }
+            }
+        });
+    for (auto& th : pool) th.join();
+    return ok;
+}
+
+std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, bool wait) {
+    return compiler().request(bodies, wait);
+}
+void jit_wait_all() { compiler().wait_all(); }
+JitStats jit_stats() { return compiler().stats(); }
+std::string jit_last_error() { return compiler().last_error(); }
+
+}  // namespace qoa

@@ -1,0 +1,69 @@
+// qoa_jit.h — run-time compiled complex128 tile passes (host side).
+//
+// A pass's op stream is known on the host before it runs. Instead of
+// interpreting it (k_pass: op fetch, dispatch, run-time exchange addresses),
+// the engine can emit the pass as straight-line CUDA C++ — every register
+// bit, condition mask, exchange address and coefficient slot a literal — and
+// compile it with NVRTC for sm_100a. Coefficient values stay kernel
+// parameters (the PassParams travels as before), so the generated text, and
+// the compiled kernel, depend only on the pass's structure: repeated circuits
+// and circuits that differ only in angles reuse one kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "qoa_kernels.cuh"
+
+namespace qoa {
+
+struct JitEntry;
+
+// A compiled (or compiling) pass kernel.
+class JitKernel {
+public:
+    JitKernel() = default;
+    explicit JitKernel(std::shared_ptr<JitEntry> e) : e_(std::move(e)) {}
+    bool ready() const;
+    bool failed() const;
+    // Launches the pass over the state (grid 2^(n - TILE_BITS)); the same
+    // arguments as k_pass.
+    cudaError_t launch(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+                       cudaStream_t st) const;
+
+private:
+    std::shared_ptr<JitEntry> e_;
+};
+
+// The kernel body (everything after the kernel's name) for a pass.
+std::string jit_pass_body(const PassParams& P);
+
+// Looks each body up in the process-wide cache; the missing ones are
+// compiled as one NVRTC program on the compile thread. wait: return only
+// after that compile has finished.
+std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, bool wait);
+
+// The whole NVRTC program text for these bodies (prelude, kernels).
+std::string jit_program(const std::vector<std::string>& bodies);
+
+// Compiles the bodies with NVRTC without loading them (no GPU needed).
+bool jit_compile_only(const std::vector<std::string>& bodies, std::string& err);
+
+// Blocks until every submitted compile has finished.
+void jit_wait_all();
+
+struct JitStats {
+    uint64_t kernels;      // compiled kernels in the cache
+    uint64_t hits;         // requests served from the cache
+    uint64_t misses;       // requests that started a compile
+    uint64_t failures;     // kernels whose compile or load failed
+    double compile_ms;     // total NVRTC + load time
+};
+JitStats jit_stats();
+
+// Last compile error text (empty if none).
+std::string jit_last_error();
+
+}  // namespace qoa

@@ -9,9 +9,11 @@
 // means the logical state is |0..0>, which is what QuantumState::normalize
 // (src/runtime/quantum_state.rs:888-907) resets to.
 #pragma once
+#ifndef __CUDACC_RTC__  // NVRTC (run-time pass kernels) gets the integer types from its prelude
 #include <stddef.h>
 #include <stdint.h>
 #include <vector_types.h>
+#endif
 
 namespace qoa {
 
@@ -132,8 +134,10 @@ struct PassParams {
 };
 static_assert(sizeof(PassParams) <= 32000, "PassParams travels as a kernel parameter (32 KB limit)");
 
+#ifndef __CUDACC_RTC__
 static_assert(offsetof(PassParams, ops) % 16 == 0 && offsetof(PassParams, coef) % 16 == 0,
               "the op stream and coefficients are staged with 16-byte loads");
+#endif
 
 // One circuit's pass inside an arena launch: its state, the pass's parameters
 // (PassParams for complex128, F32PassParams for complex64), and whether this

@@ -1,0 +1,118 @@
+"""Generated (NVRTC-compiled) complex128 pass kernels against the
+interpreter kernel and the oracle: the same PassParams must give the same
+amplitudes bit for bit, and both must be within 1e-12 (relative L2) of the
+oracle."""
+import numpy as np
+import pytest
+
+import qoa_b200 as qb
+from qoa_b200 import circuits as C
+from oracle import pyoracle as po
+from tests.test_plan import mixed_circuit
+from tests.test_gpu_parity import swap_heavy
+
+TOL = 1e-12
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def oracle_run(n, ops, flags):
+    po.set_fast(True)
+    st = po.OracleState(n, flags)
+    st.apply(C.ops_to_array(ops))
+    s = st.state()
+    st.close()
+    return s
+
+
+def run(n, ops, jit, quirk=False, init_seed=None):
+    with qb.QuantumState(n, compat_mask_quirk=quirk) as st:
+        st.set_jit(jit, min_qubits=11)
+        if init_seed is not None:
+            st.set_random_state(init_seed)
+        st.execute(C.ops_to_array(ops))
+        return st.get_state_vector(), st.jit_stats()
+
+
+CASES = [
+    ("layered_h_16x8_quirk", 16, True, lambda: C.random_layered(16, 8, 21, initial_h=True)),
+    ("layered_18x10", 18, False, lambda: C.random_layered(18, 10, 22)),
+    ("qft_17", 17, False, lambda: C.qft(17)),
+    ("mixed_14", 14, False, lambda: mixed_circuit(14, 300, 23)),
+    ("mixed_17", 17, True, lambda: mixed_circuit(17, 200, 24)),
+    ("swaps_15", 15, False, lambda: swap_heavy(15, 600, 25)),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,n,quirk,make", CASES, ids=[c[0] for c in CASES])
+def test_generated_passes_match_interpreter_and_oracle(name, n, quirk, make):
+    ops = make()
+    got_jit, st_jit = run(n, ops, qb.QOA_JIT_SYNC, quirk)
+    got_int, st_int = run(n, ops, qb.QOA_JIT_OFF, quirk)
+    assert st_jit["launches"] > 0, "the generated kernels did not run"
+    assert st_jit["failures"] == 0
+    assert st_int["launches"] == 0
+    assert np.array_equal(got_jit.view(np.float64), got_int.view(np.float64)), "generated != interpreter"
+    ref = oracle_run(n, ops, 1 if quirk else 0)
+    assert rel_l2(got_jit, ref) < TOL
+
+
+@pytest.mark.gpu
+def test_generated_passes_from_a_random_state():
+    n = 16
+    ops = mixed_circuit(n, 150, 31)
+    a, s = run(n, ops, qb.QOA_JIT_SYNC, init_seed=5)
+    b, _ = run(n, ops, qb.QOA_JIT_OFF, init_seed=5)
+    assert s["launches"] > 0
+    assert np.array_equal(a.view(np.float64), b.view(np.float64))
+
+
+@pytest.mark.gpu
+def test_async_mode_switches_to_generated_kernels():
+    n = 15
+    ops = C.ops_to_array(C.random_layered(n, 6, 41, initial_h=True))
+    with qb.QuantumState(n) as st:
+        st.set_jit(qb.QOA_JIT_ASYNC, min_qubits=11)
+        st.execute(ops)          # interpreted while the kernels compile (or generated, if cached)
+        first = st.get_state_vector()
+        qb.jit_wait()
+        st.apply_reset_all()
+        st.execute(ops)          # generated kernels now
+        second = st.get_state_vector()
+        assert st.jit_stats()["launches"] > 0
+    assert np.array_equal(first.view(np.float64), second.view(np.float64))
+
+
+@pytest.mark.gpu
+def test_same_structure_reuses_the_compiled_kernel():
+    n = 14
+    before = qb.jit_stats()
+    outs = []
+    for angle in (0.3, 1.1):   # same pass structure, other angle values
+        ops = [C.Op(C.H, [q]) for q in range(n)] + [C.Op(C.RZ, [q], angle * (q + 1)) for q in range(n)] + \
+              [C.Op(C.CPHASE, [q, (q + 5) % n], angle) for q in range(n)] + [C.Op(C.RY, [q], angle) for q in range(n)]
+        got, _ = run(n, ops, qb.QOA_JIT_SYNC)
+        assert rel_l2(got, oracle_run(n, ops, 0)) < TOL
+        outs.append(got)
+    after = qb.jit_stats()
+    assert after["hits"] > before["hits"], "the second angle set compiled again"
+    assert not np.allclose(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+def test_measurement_between_passes_uses_generated_kernels():
+    n = 16
+    ops = C.random_layered(n, 4, 51, initial_h=True) + [C.Op(C.MEASURE, [3])] + C.random_layered(n, 4, 52)
+    with qb.QuantumState(n, seed=9) as st:
+        st.set_jit(qb.QOA_JIT_SYNC, min_qubits=11)
+        st.execute(C.ops_to_array(ops))
+        a = st.get_state_vector()
+        assert st.jit_stats()["launches"] > 0
+    with qb.QuantumState(n, seed=9) as st:
+        st.set_jit(qb.QOA_JIT_OFF)
+        st.execute(C.ops_to_array(ops))
+        b = st.get_state_vector()
+    assert np.array_equal(a.view(np.float64), b.view(np.float64))
