@@ -119,10 +119,11 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def pass_traffic_bytes(n: int):
+def pass_traffic_bytes(n: int, generated: bool = True):
     """DRAM bytes per tile-pass launch at n qubits, scaled from the committed
-    ncu capture of the 26-qubit instance (traffic grows with the amplitudes)."""
-    p = os.path.join(ROOT, "profiles", "k_pass_layered26.md")
+    ncu capture of the 26-qubit instance (traffic grows with the amplitudes):
+    the generated pass kernel's capture, or the interpreter's."""
+    p = os.path.join(ROOT, "profiles", "qoa_jit_pass_layered26.md" if generated else "k_pass_layered26.md")
     try:
         for line in open(p):
             if line.startswith("dram_bytes_per_amplitude:"):
@@ -227,14 +228,20 @@ def run_ours(args):
         st.apply_reset_all()
         st.execute(ops)
 
+    st.set_jit(JIT_MODES[args.jit])
     for _ in range(max(args.warmup, 0)):
         step()
+    # the warm-up's second sighting of each pass requested its generated
+    # kernel; wait for the compiles, then one more untimed step on them
+    qb.jit_wait()
+    step()
     st.sync()
     if ws > 1:
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     l0 = st.launch_count()
+    j0 = st.jit_stats()["launches"]
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
@@ -244,6 +251,8 @@ def run_ours(args):
     st.sync()
     torch.cuda.synchronize()
     launches = st.launch_count() - l0
+    jit = st.jit_stats()
+    jit_timed = jit["launches"] - j0
     elapsed = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     tmax, units = aggregate(elapsed, float(G * args.steps), dev if ws > 1 else None)
@@ -252,6 +261,7 @@ def run_ours(args):
 
     # ---- roofline: per-launch times of the tile-pass kernel ----
     prof = qb.QuantumState(n, compat_mask_quirk=True, profile=True)
+    prof.set_jit(JIT_MODES[args.jit])
     prof.apply_reset_all()
     prof.execute(ops)
     prof.sync()
@@ -259,6 +269,7 @@ def run_ours(args):
     prof.apply_reset_all()
     prof.execute(ops)
     ms, by, kind = prof.launch_times()
+    prof_jit = prof.jit_stats()["launches"]
     prof.close()
     pass_ms = ms[kind == 0]
     pass_bytes = by[kind == 0]
@@ -266,9 +277,11 @@ def run_ours(args):
     avg_ms = float(pass_ms.mean()) if pass_ms.size else float("nan")
     achieved = float(pass_bytes.mean() / (avg_ms / 1e3) / 1e9) if pass_ms.size else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": pass_traffic_bytes(n),
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": pass_traffic_bytes(n, generated=prof_jit > 0),
                 "traffic_source": "ncu dram bytes of the 26-qubit instance, scaled per amplitude",
-                "kernel": "k_pass", "launches_per_step": int(pass_ms.size), "avg_launch_ms": avg_ms,
+                "kernel": "qoa_jit_pass_* (generated tile pass)" if prof_jit > 0 else "k_pass (interpreter)",
+                "launches_per_step": int(pass_ms.size), "avg_launch_ms": avg_ms,
                 "algorithmic_bytes_per_launch": float(pass_bytes.mean()) if pass_ms.size else None,
                 "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
                 "pass_share_of_step": float(pass_ms.sum() / ms.sum()) if ms.size else None}
@@ -284,6 +297,7 @@ def run_ours(args):
         host = torch.empty((1 << n) * 2, dtype=torch.float64, pin_memory=True)
         hv = host.numpy().view(np.complex128)
         st2 = qb.QuantumState(n, compat_mask_quirk=True)
+        st2.set_jit(JIT_MODES[args.jit])
         states = [st, st2]
 
         def copy_out(s):
@@ -328,7 +342,11 @@ def run_ours(args):
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD),
                 "effective_gbs": C.algorithmic_bytes(ops_list, n, quirk=True) * args.steps * ws / (tmax / 1e3) / 1e9,
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "impl": "qoa_b200"}
+                "e2e": e2e, "impl": "qoa_b200",
+                "jit": {"mode": args.jit, "generated_pass_launches_timed": int(jit_timed),
+                        "kernels_compiled": int(jit["kernels"]), "compile_ms_total": jit["compile_ms"],
+                        "note": "pass kernels compiled once per pass structure during warm-up (NVRTC, "
+                                "16 host threads), cached for the process"}}
         print(json.dumps(line), flush=True)
     st.close()
     if ws > 1:
@@ -353,6 +371,8 @@ def run_qft(args):
         stream = torch.cuda.ExternalStream(st.stream_ptr(), device=dev)
         for _ in range(warmup):
             st.execute(ops)
+        qb.jit_wait()  # generated pass kernels requested during the warm-up
+        st.execute(ops)
         st.sync()
         st.launch_times()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -612,6 +632,9 @@ def run_serve(args):
     return 0
 
 
+JIT_MODES = {"off": 0, "async": 1, "sync": 2}
+
+
 def run_case(args):
     """Profiling case: two executions of one circuit on one state, nothing
     else (no timing line). --case qft: QFT on a seeded Gaussian state;
@@ -621,6 +644,7 @@ def run_case(args):
     n = args.qubits
     ops = C.ops_to_array(C.qft(n) if args.case == "qft" else C.layered_h_workload(n, args.depth, 1))
     with qb.QuantumState(n, precision=args.case_precision, compat_mask_quirk=(args.case != "qft")) as st:
+        st.set_jit(JIT_MODES[args.jit] if args.jit != "async" else qb.QOA_JIT_SYNC)
         st.set_random_state(2)
         for _ in range(2):
             st.execute(ops)
@@ -657,6 +681,8 @@ def main():
     ap.add_argument("--precisions", default="f64,f32")
     ap.add_argument("--tune-sample", type=int, default=256)
     ap.add_argument("--tune-seconds", type=float, default=60.0)
+    ap.add_argument("--jit", default="async", choices=list(JIT_MODES),
+                    help="complex128 pass kernels: generated (async / sync compile) or interpreted (off)")
     args = ap.parse_args()
     if args.workload == "qft":
         return run_qft(args)

@@ -373,8 +373,10 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
  * circuits, angle sweeps); compiled kernels are cached for the process.
  * Results are identical either way. Per handle:
  *   QOA_JIT_OFF    interpret every pass
- *   QOA_JIT_ASYNC  (default) request the kernels, interpret passes whose
- *                  kernel is still compiling (on one background thread)
+ *   QOA_JIT_ASYNC  (default) a pass structure seen for the second time is
+ *                  compiled on background threads; passes interpret until
+ *                  their kernel is ready (one-off structures, such as a
+ *                  noisy trajectory's Pauli draws, are never compiled)
  *   QOA_JIT_SYNC   compile before the first launch
  * States below min_qubits (default 20) always interpret. */
 #define QOA_JIT_OFF   0

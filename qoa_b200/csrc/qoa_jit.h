@@ -40,9 +40,10 @@ private:
 // The kernel body (everything after the kernel's name) for a pass.
 std::string jit_pass_body(const PassParams& P);
 
-// Looks each body up in the process-wide cache; the missing ones are
-// compiled as one NVRTC program on the compile thread. wait: return only
-// after that compile has finished.
+// Looks each body up in the process-wide cache. wait: the missing ones are
+// compiled now and the call returns when they are loaded. Otherwise a
+// missing body is queued for the compile threads the second time it is
+// requested (the first request returns an empty, never-ready kernel).
 std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, bool wait);
 
 // The whole NVRTC program text for these bodies (prelude, kernels).

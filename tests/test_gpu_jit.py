@@ -76,14 +76,17 @@ def test_async_mode_switches_to_generated_kernels():
     ops = C.ops_to_array(C.random_layered(n, 6, 41, initial_h=True))
     with qb.QuantumState(n) as st:
         st.set_jit(qb.QOA_JIT_ASYNC, min_qubits=11)
-        st.execute(ops)          # interpreted while the kernels compile (or generated, if cached)
+        st.execute(ops)          # first sighting: interpreted, nothing compiled
         first = st.get_state_vector()
+        assert st.jit_stats()["launches"] == 0
+        st.apply_reset_all()
+        st.execute(ops)          # second sighting: compiles in the background
         qb.jit_wait()
         st.apply_reset_all()
         st.execute(ops)          # generated kernels now
-        second = st.get_state_vector()
+        third = st.get_state_vector()
         assert st.jit_stats()["launches"] > 0
-    assert np.array_equal(first.view(np.float64), second.view(np.float64))
+    assert np.array_equal(first.view(np.float64), third.view(np.float64))
 
 
 @pytest.mark.gpu
