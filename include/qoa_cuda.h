@@ -371,6 +371,7 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
  * compiled at run time by NVRTC for sm_100a. Coefficients stay parameters, so
  * one compiled kernel serves every pass of the same structure (repeated
  * circuits, angle sweeps); compiled kernels are cached for the process.
+ * complex128 and complex64 (non-tensor) handles both have the form.
  * Results are identical either way. Per handle:
  *   QOA_JIT_OFF    interpret every pass
  *   QOA_JIT_ASYNC  (default) a pass structure seen for the second time is
@@ -394,13 +395,14 @@ typedef struct qoa_jit_stats {
     double compile_ms;   /* total compile + load time */
 } qoa_jit_stats;
 int qoa_jit_stats_get(qoa_state_t s, qoa_jit_stats* out);
-/* Host only, no GPU needed: plans an op list for an n-qubit complex128 state
- * and writes the generated source of each pass's kernel (concatenated, NUL
- * terminated, truncated to cap; *len = full length) and the pass count.
- * compile != 0 also compiles it with NVRTC (nothing is loaded) and fails
- * with QOA_E_ARG and the compiler log when it does not compile. */
-int qoa_jit_translate(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int compile, char* out,
-                      size_t cap, size_t* len, size_t* npasses);
+/* Host only, no GPU needed: plans an op list for an n-qubit state of the
+ * given precision (QOA_PREC_F64 / QOA_PREC_F32 tile passes) and writes the
+ * generated source of each pass's kernel (concatenated, NUL terminated,
+ * truncated to cap; *len = full length) and the pass count. compile != 0
+ * also compiles it with NVRTC (nothing is loaded) and fails with QOA_E_ARG
+ * and the compiler log when it does not compile. */
+int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* ops, size_t nops, int compile,
+                      char* out, size_t cap, size_t* len, size_t* npasses);
 
 /* ---- allocation-free entry point ----------------------------------------- */
 /* No counterpart in the reference. <Z_mask> = sum_i (-1)^popcount(i & mask)

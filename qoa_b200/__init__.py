@@ -144,7 +144,7 @@ def _load() -> ctypes.CDLL:
         "qoa_set_jit": (i32, [vp, i32, u32]),
         "qoa_jit_wait": (i32, []),
         "qoa_jit_stats_get": (i32, [vp, P(JitStats)]),
-        "qoa_jit_translate": (i32, [u32, u32, vp, sz, i32, vp, sz, P(sz), P(sz)]),
+        "qoa_jit_translate": (i32, [u32, i32, u32, vp, sz, i32, vp, sz, P(sz), P(sz)]),
         "qoa_vec_apply_hadamard": (i32, [vp, sz, dbl, dbl, sz]),
         "qoa_vec_apply_x": (i32, [vp, sz, sz]),
         "qoa_vec_apply_y": (i32, [vp, sz, sz]),
@@ -502,15 +502,18 @@ def jit_stats() -> dict:
     return {f: getattr(st, f) for f, _ in JitStats._fields_}
 
 
-def jit_translate(n: int, ops, flags: int = 0, compile: bool = False):
+def jit_translate(n: int, ops, flags: int = 0, compile: bool = False, precision: str = "f64"):
     """Host only: the generated CUDA source of every tile pass of `ops` on an
-    n-qubit complex128 state, and the pass count; compile=True also compiles
-    it with NVRTC (raises QoaError with the log if it does not compile)."""
+    n-qubit state (precision "f64" or "f32"), and the pass count;
+    compile=True also compiles it with NVRTC (raises QoaError with the log
+    if it does not compile)."""
     arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
+    prec = QOA_PREC_F32 if precision == "f32" else QOA_PREC_F64
     ln, npasses = ctypes.c_size_t(), ctypes.c_size_t()
-    _check(lib.qoa_jit_translate(n, flags, _ptr(arr), len(arr), 0, None, 0, ctypes.byref(ln), ctypes.byref(npasses)))
+    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), 0, None, 0, ctypes.byref(ln),
+                                 ctypes.byref(npasses)))
     buf = ctypes.create_string_buffer(ln.value + 1)
-    _check(lib.qoa_jit_translate(n, flags, _ptr(arr), len(arr), 1 if compile else 0, buf, ln.value + 1,
+    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), 1 if compile else 0, buf, ln.value + 1,
                                  ctypes.byref(ln), ctypes.byref(npasses)))
     return buf.value.decode(), npasses.value
 

@@ -1397,11 +1397,14 @@ int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
 // A complex128 pass whose parameters were built ahead (with its generated
 // kernel requested): the generated kernel when it is ready, else k_pass.
 int run_pass_built(qoa_state_t s, const PassParams& P, const JitKernel& jk) {
+    const bool c64 = s->precision == QOA_PREC_F32;
     {
-        Timer tm(s, 2.0 * std::ldexp(16.0, (int)s->n), 0);
+        Timer tm(s, 2.0 * std::ldexp(c64 ? 8.0 : 16.0, (int)s->n), c64 ? 3 : 0);
         if (jk.ready()) {
             CK(jk.launch(s->amps, P, s->scal, s->partials, s->stream));
             s->jit_launches++;
+        } else if (c64) {
+            CK(launch_pass_p32((float2*)s->amps, P, s->scal, s->partials, s->stream));
         } else {
             CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
         }
@@ -1640,12 +1643,12 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         std::vector<Gate> seg(G.begin() + i, G.begin() + j);
         if (!per_gate) merge_swap_blocks(seg);
         std::vector<Step> steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
-        // complex128 passes of a large state: built ahead, and their
-        // generated kernels requested from the compile cache
+        // tile passes of a large state: built ahead, and their generated
+        // kernels requested from the compile cache
         std::vector<PassParams> built;
         std::vector<int> built_of(steps.size(), -1);
         std::vector<JitKernel> jk;
-        if (!c64 && !per_gate && s->jit_mode != QOA_JIT_OFF && s->n >= s->jit_min_qubits) {
+        if (!per_gate && s->jit_mode != QOA_JIT_OFF && s->n >= s->jit_min_qubits) {
             size_t np = 0;
             for (const Step& st : steps) np += st.pass ? 1 : 0;
             built.resize(np);
@@ -1654,7 +1657,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
             for (size_t k = 0; k < steps.size(); ++k) {
                 if (!steps[k].pass || build_pass(seg, steps[k], s->n, built[b]) != 0) continue;
                 built_of[k] = (int)b;
-                bodies.push_back(jit_pass_body(built[b]));
+                bodies.push_back(c64 ? jit_pass32_body(built[b]) : jit_pass_body(built[b]));
                 ++b;
             }
             jk = jit_request(bodies, s->jit_mode == QOA_JIT_SYNC);
@@ -2925,9 +2928,10 @@ int qoa_jit_stats_get(qoa_state_t s, qoa_jit_stats* out) {
     return QOA_OK;
 }
 
-int qoa_jit_translate(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int compile, char* out,
-                      size_t cap, size_t* len, size_t* npasses) {
+int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* ops, size_t nops, int compile,
+                      char* out, size_t cap, size_t* len, size_t* npasses) {
     if ((!ops && nops) || (!out && cap)) return set_err(nullptr, QOA_E_ARG, "null argument");
+    if (precision != QOA_PREC_F64 && precision != QOA_PREC_F32) return set_err(nullptr, QOA_E_ARG, "bad precision");
     if (n < (uint32_t)TILE_BITS || n > 36) return set_err(nullptr, QOA_E_ARG, "tile passes need 11..36 qubits");
     Expander ex;
     ex.n = n;
@@ -2947,7 +2951,7 @@ int qoa_jit_translate(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops
     for (const Step& st : steps) {
         if (!st.pass) continue;
         if (build_pass(G, st, n, P) != 0) return set_err(nullptr, QOA_E_ARG, "a pass does not fit one launch");
-        bodies.push_back(jit_pass_body(P));
+        bodies.push_back(precision == QOA_PREC_F32 ? jit_pass32_body(P) : jit_pass_body(P));
     }
     if (npasses) *npasses = bodies.size();
     const std::string text = jit_program(bodies);

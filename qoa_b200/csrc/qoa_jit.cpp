@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <deque>
 #include <mutex>
 #include <thread>
@@ -39,6 +40,9 @@ const char kTypesHeader[] =
 const char kDevHeader[] =
 #include "qoa_pass_dev.cuh.inc"
     ;
+const char kDev32Header[] =
+#include "qoa_pass32_dev.cuh.inc"
+    ;
 
 // NVRTC has no C library headers: the fixed-width types the headers use.
 const char kPrelude[] =
@@ -47,11 +51,22 @@ const char kPrelude[] =
     "typedef unsigned int uint32_t;\n"
     "typedef int int32_t;\n"
     "typedef unsigned long long uint64_t;\n"
-    "#include \"qoa_pass_dev.cuh\"\n";
+    "#include \"qoa_pass_dev.cuh\"\n"
+    "#include \"qoa_pass32_dev.cuh\"\n";
 
-// Resident CTAs per SM of a generated pass (128 threads): the same register
-// budget as k_pass.
+// Resident CTAs per SM of a generated pass (128 threads): complex128 the
+// same register budget as k_pass (128), complex64 up to 80 registers.
 constexpr int JIT_OCC = 4;
+constexpr int JIT_OCC32 = 6;
+
+// QOA_JIT_OCC / QOA_JIT_OCC32 override the resident-CTA targets (tuning).
+int occ_target(bool c64) {
+    const char* v = getenv(c64 ? "QOA_JIT_OCC32" : "QOA_JIT_OCC");
+    const int d = c64 ? JIT_OCC32 : JIT_OCC;
+    if (!v) return d;
+    const int k = atoi(v);
+    return (k >= 1 && k <= 16) ? k : d;
+}
 
 uint32_t spos_host(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
 
@@ -277,6 +292,189 @@ std::string jit_pass_body(const PassParams& P) {
     return E.s;
 }
 
+// The complex64 form: the packed FP32 tile pass of qoa_pass32.cu
+// (pass_tile_p32) for the same PassParams. Registers hold re[j] / im[j] =
+// packed (amplitude j, amplitude j + 8); coefficients are rounded to float
+// once per CTA into shared memory, as the interpreter stages them.
+std::string jit_pass32_body(const PassParams& P) {
+    Emit E;
+    E.line("(float2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
+    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials) {");
+    E.line("using namespace qoa;");
+    E.line("using namespace qoa::p32;");
+    E.line("__shared__ __align__(16) float2 tile[1 << TILE_BITS];");
+    E.line("__shared__ double red[PASS_THREADS / 32];");
+    const uint32_t ncoef = P.ncoef ? P.ncoef : 1;
+    E.line("__shared__ float2 scoef[%u];", ncoef);
+    if (P.nang) E.line("__shared__ float2 sang[%u];", P.nang);
+    E.line("const int lane = threadIdx.x & 31;");
+    E.line("const int wid = threadIdx.x >> 5;");
+    E.line("const uint64_t blk = blockIdx.x;");
+    E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
+           LANE_BITS + WARP_BITS);
+    {
+        std::string g = "0ull";
+        const int nout = (int)P.n - TILE_BITS;
+        char b[128];
+        for (int k = 0; k < nout;) {
+            int len = 1;
+            while (k + len < nout && P.outer_qubits[k + len] == P.outer_qubits[k] + len) ++len;
+            snprintf(b, sizeof b, " | (((blk >> %d) & 0x%llxull) << %d)", k,
+                     (unsigned long long)((len >= 64) ? ~0ull : ((1ull << len) - 1)), P.outer_qubits[k]);
+            g += b;
+            k += len;
+        }
+        E.line("const uint64_t g0 = %s;", g.c_str());
+    }
+    E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);",
+           P.ncoef);
+    if (P.nang) E.line("pass_angles(P, blk, sang);");
+    E.line("const double nrm = *norm2_in;");
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))");
+    E.line("                    : make_float2((float)P.phase.x, (float)P.phase.y);");
+    E.line("u64p re[8], im[8];");
+    auto stride = [&](int t) -> unsigned long long {
+        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+    };
+    {
+        const TileMap& m = P.map0;
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        const unsigned long long r3 = stride(m.reg[3]);
+        E.line("if (valid) {");
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += stride(m.reg[k]);
+            E.line("{ const float2 a = __ldcs(amps + (tb + 0x%llxull)), b = __ldcs(amps + (tb + 0x%llxull)); re[%d] = pk(a.x, b.x); im[%d] = pk(a.y, b.y); }",
+                   off, off + r3, j, j);
+        }
+        E.line("} else {");
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += stride(m.reg[k]);
+            E.line("re[%d] = pk(tb + 0x%llxull == 0 ? 1.f : 0.f, 0.f); im[%d] = 0ull;", j, off, j);
+        }
+        E.line("}");
+        E.line("}");
+    }
+    E.line("__syncthreads();");
+
+    const TileMap* cur = &P.map0;
+    const uint32_t* ow = reinterpret_cast<const uint32_t*>(P.ops);
+    for (uint32_t oi = 0; oi < P.nops; ++oi) {
+        const PassOp& op = P.ops[oi];
+        const int code = op.code;
+        const uint32_t c = op.coef;
+        const uint32_t cr = op.cond_reg;
+        const uint32_t tm = ow[4 * oi + 2];
+        const bool g1 = (code >= PC_HF && code < PC_XC) || (code >= PC_RXB && code < PC_DIAG_TA);
+        if (g1) {
+            if ((code & 3) == 3) E.line("g1_bit3<%s>(re, im, scoef + %u);", g1_name(code), c);
+            else E.line("g1p<%s, %d>(re, im, scoef + %u);", g1_name(code), code & 3, c);
+        } else if (code >= PC_XC && code < PC_RXB) {
+            E.line("g1c<%s, %d>(re, im, %s, 0x%xu);", (code & ~3) == PC_XC ? "G1_X" : "G1_Y", code & 3,
+                   tcond(tm).c_str(), cr);
+        } else {
+            switch (code) {
+                case PC_DIAG_T:
+                    if (tm) E.line("if (%s) pend = cmulf(pend, scoef[%u]);", tcond(tm).c_str(), c);
+                    else E.line("pend = cmulf(pend, scoef[%u]);", c);
+                    break;
+                case PC_DIAG_M:
+                    E.line("diag_p(re, im, %s, 0x%xu, scoef[%u]);", tcond(tm).c_str(), cr, c);
+                    break;
+                case PC_DIAG_TA:
+                    if (tm) E.line("if (%s) pend = cmulf(pend, sang[%u]);", tcond(tm).c_str(), c);
+                    else E.line("pend = cmulf(pend, sang[%u]);", c);
+                    break;
+                case PC_DIAG_MA:
+                    E.line("diag_p(re, im, true, 0x%xu, sang[%u]);", cr, c);
+                    break;
+                case PC_DIAG_MX:
+                case PC_DIAG_TM: {
+                    const uint32_t cnt = op.k;
+                    bool one = true;
+                    E.line("{ float2 f = make_float2(1.f, 0.f);");
+                    for (uint32_t e = 1; e <= cnt; ++e) {
+                        const PassOp& r = P.ops[oi + e];
+                        const uint32_t rtm = ow[4 * (oi + e) + 2];
+                        if (!rtm && one) E.line("f = scoef[%u];", (unsigned)r.coef);
+                        else if (one) E.line("f = %s ? scoef[%u] : make_float2(1.f, 0.f);", tcond(rtm).c_str(), (unsigned)r.coef);
+                        else if (!rtm) E.line("f = cmulf(f, scoef[%u]);", (unsigned)r.coef);
+                        else E.line("if (%s) f = cmulf(f, scoef[%u]);", tcond(rtm).c_str(), (unsigned)r.coef);
+                        one = false;
+                        if (code == PC_DIAG_MX && (e == cnt || ((r.has_tp >> 1) & 1u))) {
+                            E.line("diag_p(re, im, true, 0x%xu, f);", (unsigned)r.cond_reg);
+                            if (e != cnt) E.line("f = make_float2(1.f, 0.f);");
+                            one = true;
+                        }
+                    }
+                    if (code == PC_DIAG_TM && cnt) E.line("pend = cmulf(pend, f);");
+                    E.line("}");
+                    oi += cnt;
+                    break;
+                }
+                case PC_DIAG_TAB:
+                    for (int j = 0; j < 8; ++j)
+                        E.line("cmul2(re[%d], im[%d], pk(scoef[%u].x, scoef[%u].x), pk(scoef[%u].y, scoef[%u].y));", j, j,
+                               c + j, c + j + 8, c + j, c + j + 8);
+                    break;
+                case PC_FLUSH:
+                    E.line("{ const u64p cr = bc(pend.x), ci = bc(pend.y);");
+                    for (int j = 0; j < 8; ++j) E.line("cmul2(re[%d], im[%d], cr, ci);", j, j);
+                    E.line("pend = make_float2(1.f, 0.f); }");
+                    break;
+                case PC_XCHG: {
+                    const TileMap& mo = *cur;
+                    const TileMap& mn = P.xmap[c];
+                    E.line("__syncthreads();");
+                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mo).c_str());
+                    for (int j = 0; j < 8; ++j)
+                        E.line("tile[pb ^ %uu] = make_float2(lo(re[%d]), lo(im[%d])); tile[pb ^ %uu] = make_float2(hi(re[%d]), hi(im[%d]));",
+                               reg_part(mo, j), j, j, reg_part(mo, j | 8), j, j);
+                    E.line("}");
+                    E.line("__syncthreads();");
+                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mn).c_str());
+                    for (int j = 0; j < 8; ++j)
+                        E.line("{ const float2 a = tile[pb ^ %uu], b = tile[pb ^ %uu]; re[%d] = pk(a.x, b.x); im[%d] = pk(a.y, b.y); }",
+                               reg_part(mn, j), reg_part(mn, j | 8), j, j);
+                    E.line("}");
+                    cur = &mn;
+                    break;
+                }
+                default: break;
+            }
+        }
+    }
+    {
+        const TileMap& m = *cur;
+        auto ostride = [&](int t) -> unsigned long long { return 1ull << P.out_qubit[t]; };
+        E.line("{");
+        E.line("const u64p cr = bc(pend.x), ci = bc(pend.y);");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               ostride(m.warp[0]), ostride(m.warp[1]));
+        E.line("double ss = 0.0;");
+        const unsigned long long r3 = ostride(m.reg[3]);
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += ostride(m.reg[k]);
+            E.line("{ cmul2(re[%d], im[%d], cr, ci); const float2 a = make_float2(lo(re[%d]), lo(im[%d])), b = make_float2(hi(re[%d]), hi(im[%d]));",
+                   j, j, j, j, j, j);
+            E.line("  __stcs(amps + (tb + 0x%llxull), a); __stcs(amps + (tb + 0x%llxull), b);", off, off + r3);
+            E.line("  ss += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y; }");
+        }
+        E.line("block_norm_partial(ss, red, partials + blk);");
+        E.line("}");
+    }
+    E.line("}");
+    return E.s;
+}
+
 // ------------------------------------------------------------ the cache
 struct JitEntry {
     std::atomic<int> state{0};  // 0 compiling, 1 ready, 2 failed
@@ -287,7 +485,7 @@ struct JitEntry {
 bool JitKernel::ready() const { return e_ && e_->state.load(std::memory_order_acquire) == 1; }
 bool JitKernel::failed() const { return !e_ || e_->state.load(std::memory_order_acquire) == 2; }
 
-cudaError_t JitKernel::launch(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+cudaError_t JitKernel::launch(void* amps, const PassParams& P, const double* norm2_in, double* partials,
                               cudaStream_t st) const {
     if (!ready()) return cudaErrorNotReady;
     void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials};
@@ -310,8 +508,9 @@ std::string program_text(const std::vector<std::string>& names, const std::vecto
     std::string src = kPrelude;
     char head[160];
     for (size_t i = 0; i < names.size(); ++i) {
-        snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS, JIT_OCC,
-                 names[i].c_str());
+        const bool c64 = bodies[i].compare(0, 7, "(float2") == 0;
+        snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS,
+                 occ_target(c64), names[i].c_str());
         src += head;
         src += bodies[i];
     }
@@ -322,10 +521,10 @@ std::string program_text(const std::vector<std::string>& names, const std::vecto
 bool build_cubin(const std::vector<std::string>& names, const std::vector<std::string>& bodies,
                  std::vector<char>& cubin, std::string& err) {
     const std::string src = program_text(names, bodies);
-    const char* hdrs[] = {kTypesHeader, kDevHeader};
-    const char* hnames[] = {"qoa_kernels.cuh", "qoa_pass_dev.cuh"};
+    const char* hdrs[] = {kTypesHeader, kDevHeader, kDev32Header};
+    const char* hnames[] = {"qoa_kernels.cuh", "qoa_pass_dev.cuh", "qoa_pass32_dev.cuh"};
     nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src.c_str(), "qoa_jit_pass.cu", 2, hdrs, hnames) != NVRTC_SUCCESS) {
+    if (nvrtcCreateProgram(&prog, src.c_str(), "qoa_jit_pass.cu", 3, hdrs, hnames) != NVRTC_SUCCESS) {
         err = "nvrtcCreateProgram failed";
         return false;
     }
@@ -349,8 +548,9 @@ bool build_cubin(const std::vector<std::string>& names, const std::vector<std::s
 }
 
 std::string kernel_name(const std::string& body) {
-    char nm[40];
-    snprintf(nm, sizeof nm, "qoa_jit_pass_%016llx", (unsigned long long)fnv64(body));
+    char nm[48];
+    snprintf(nm, sizeof nm, "%s_%016llx", body.compare(0, 7, "(float2") == 0 ? "qoa_jit_pass32" : "qoa_jit_pass",
+             (unsigned long long)fnv64(body));
     return nm;
 }
 

@@ -30,15 +30,19 @@ public:
     bool failed() const;
     // Launches the pass over the state (grid 2^(n - TILE_BITS)); the same
     // arguments as k_pass.
-    cudaError_t launch(double2* amps, const PassParams& P, const double* norm2_in, double* partials,
+    // amps: double2* (complex128 kernels) or float2* (complex64 kernels).
+    cudaError_t launch(void* amps, const PassParams& P, const double* norm2_in, double* partials,
                        cudaStream_t st) const;
 
 private:
     std::shared_ptr<JitEntry> e_;
 };
 
-// The kernel body (everything after the kernel's name) for a pass.
+// The kernel body (everything after the kernel's name) for a pass:
+// complex128 (the k_pass form) or complex64 (the packed FP32 form of
+// k_pass_p32).
 std::string jit_pass_body(const PassParams& P);
+std::string jit_pass32_body(const PassParams& P);
 
 // Looks each body up in the process-wide cache. wait: the missing ones are
 // compiled now and the call returns when they are loaded. Otherwise a

@@ -504,8 +504,16 @@ __global__ void k_reduce(const double* __restrict__ partials, uint32_t count, do
                          const double* __restrict__ divide_by, uint32_t* __restrict__ status) {
     __shared__ double sh[32];
     const double* p = partials + (uint64_t)blockIdx.x * count;
-    double x = 0.0;
-    for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) x += p[i];
+    // eight independent accumulators per thread keep eight loads in flight
+    const uint32_t B = blockDim.x;
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    uint32_t i = threadIdx.x;
+    for (; i + 7 * B < count; i += 8 * B) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += p[i + k * B];
+    }
+    for (; i < count; i += B) acc[0] += p[i];
+    double x = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

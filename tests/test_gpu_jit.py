@@ -27,8 +27,8 @@ def oracle_run(n, ops, flags):
     return s
 
 
-def run(n, ops, jit, quirk=False, init_seed=None):
-    with qb.QuantumState(n, compat_mask_quirk=quirk) as st:
+def run(n, ops, jit, quirk=False, init_seed=None, precision="f64"):
+    with qb.QuantumState(n, compat_mask_quirk=quirk, precision=precision) as st:
         st.set_jit(jit, min_qubits=11)
         if init_seed is not None:
             st.set_random_state(init_seed)
@@ -119,3 +119,18 @@ def test_measurement_between_passes_uses_generated_kernels():
         st.execute(C.ops_to_array(ops))
         b = st.get_state_vector()
     assert np.array_equal(a.view(np.float64), b.view(np.float64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,n,quirk,make", CASES, ids=[c[0] for c in CASES])
+def test_generated_complex64_passes_match_interpreter(name, n, quirk, make):
+    """The packed FP32 form: generated kernels against the packed interpreter
+    (bit for bit) and against the FP64 oracle (relative L2 < 1e-5)."""
+    ops = make()
+    got_jit, st_jit = run(n, ops, qb.QOA_JIT_SYNC, quirk, precision="f32")
+    got_int, st_int = run(n, ops, qb.QOA_JIT_OFF, quirk, precision="f32")
+    assert st_jit["launches"] > 0 and st_jit["failures"] == 0
+    assert st_int["launches"] == 0
+    assert np.array_equal(got_jit.view(np.float32), got_int.view(np.float32)), "generated != interpreter"
+    ref = oracle_run(n, ops, 1 if quirk else 0)
+    assert rel_l2(got_jit.astype(np.complex128), ref) < 1e-5

@@ -29,6 +29,16 @@ def test_one_kernel_per_pass_and_it_compiles(n, make, flags):
     assert qb.plan(n, ops, flags=flags)["npasses"] >= npasses
 
 
+@pytest.mark.parametrize("n,make,flags", [
+    (13, lambda: C.random_layered(13, 5, 3, initial_h=True), 1),
+    (13, lambda: mixed_circuit(13, 120, 4), 0),
+])
+def test_complex64_kernels_compile(n, make, flags):
+    src, npasses = qb.jit_translate(n, make(), flags=flags, compile=True, precision="f32")
+    assert npasses > 0
+    assert len(re.findall(r"qoa_jit_pass32_[0-9a-f]{16}\(float2\*", src)) == npasses
+
+
 def test_text_depends_on_structure_not_angles():
     n = 13
     def circ(a):
