@@ -328,6 +328,29 @@ std::string jit_pass32_body(const PassParams& P) {
     }
     E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);",
            P.ncoef);
+    // register tables (PC_DIAG_TAB): staged once per CTA already packed as
+    // (factor j, factor j + 8) pairs, real parts then imaginary parts
+    std::vector<uint32_t> tab_at(P.nops, 0);
+    {
+        uint32_t ntab = 0;
+        for (uint32_t oi = 0; oi < P.nops; ++oi) {
+            const int code = P.ops[oi].code;
+            if (code == PC_DIAG_TAB) tab_at[oi] = ntab++;
+            if (code == PC_DIAG_MX || code == PC_DIAG_TM) oi += P.ops[oi].k;
+        }
+        if (ntab) {
+            E.line("__shared__ u64p stab[%u];", 16 * ntab);
+            for (uint32_t oi = 0; oi < P.nops; ++oi) {
+                const PassOp& op = P.ops[oi];
+                if (op.code == PC_DIAG_TAB) {
+                    const uint32_t t = tab_at[oi], c = op.coef;
+                    E.line("if (threadIdx.x < 8) { const int j = threadIdx.x; const double2 x = P.coef[%u + j], y = P.coef[%u + j];", c, c + 8);
+                    E.line("  stab[%u + j] = pk((float)x.x, (float)y.x); stab[%u + j] = pk((float)x.y, (float)y.y); }", 16 * t, 16 * t + 8);
+                }
+                if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) oi += op.k;
+            }
+        }
+    }
     if (P.nang) E.line("pass_angles(P, blk, sang);");
     E.line("const double nrm = *norm2_in;");
     E.line("const bool valid = nrm > 1e-12;");
@@ -420,8 +443,7 @@ std::string jit_pass32_body(const PassParams& P) {
                 }
                 case PC_DIAG_TAB:
                     for (int j = 0; j < 8; ++j)
-                        E.line("cmul2(re[%d], im[%d], pk(scoef[%u].x, scoef[%u].x), pk(scoef[%u].y, scoef[%u].y));", j, j,
-                               c + j, c + j + 8, c + j, c + j + 8);
+                        E.line("cmul2(re[%d], im[%d], stab[%u], stab[%u]);", j, j, 16 * tab_at[oi] + j, 16 * tab_at[oi] + 8 + j);
                     break;
                 case PC_FLUSH:
                     E.line("{ const u64p cr = bc(pend.x), ci = bc(pend.y);");
@@ -457,7 +479,6 @@ std::string jit_pass32_body(const PassParams& P) {
         E.line("const u64p cr = bc(pend.x), ci = bc(pend.y);");
         E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
                ostride(m.warp[0]), ostride(m.warp[1]));
-        E.line("double ss = 0.0;");
         const unsigned long long r3 = ostride(m.reg[3]);
         for (int j = 0; j < 8; ++j) {
             unsigned long long off = 0;
@@ -465,10 +486,9 @@ std::string jit_pass32_body(const PassParams& P) {
                 if ((j >> k) & 1) off += ostride(m.reg[k]);
             E.line("{ cmul2(re[%d], im[%d], cr, ci); const float2 a = make_float2(lo(re[%d]), lo(im[%d])), b = make_float2(hi(re[%d]), hi(im[%d]));",
                    j, j, j, j, j, j);
-            E.line("  __stcs(amps + (tb + 0x%llxull), a); __stcs(amps + (tb + 0x%llxull), b);", off, off + r3);
-            E.line("  ss += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y; }");
+            E.line("  __stcs(amps + (tb + 0x%llxull), a); __stcs(amps + (tb + 0x%llxull), b); }", off, off + r3);
         }
-        E.line("block_norm_partial(ss, red, partials + blk);");
+        E.line("block_norm_partial(norm2_p(re, im), red, partials + blk);");
         E.line("}");
     }
     E.line("}");

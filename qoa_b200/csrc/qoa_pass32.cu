@@ -268,8 +268,8 @@ __device__ __forceinline__ void pass_tile_p32(float2* __restrict__ amps, const P
             const float2 a = make_float2(lo(re[j]), lo(im[j])), b = make_float2(hi(re[j]), hi(im[j]));
             __stcs(amps + g, a);
             __stcs(amps + g + rst[3], b);
-            ss += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
         }
+        ss = norm2_p(re, im);
     }
     if (!partial_out) return;
 #pragma unroll
@@ -555,8 +555,8 @@ __device__ __forceinline__ void pass_tile_p32x2(float2* __restrict__ amps, const
                 const float2 b = make_float2(hi(re[h][j]), hi(im[h][j]));
                 __stcs(amps + g, a);
                 __stcs(amps + g + rst[3], b);
-                ss[h] += (double)a.x * a.x + (double)a.y * a.y + (double)b.x * b.x + (double)b.y * b.y;
             }
+            ss[h] = norm2_p(re[h], im[h]);
         }
     }
     if (!partials) return;

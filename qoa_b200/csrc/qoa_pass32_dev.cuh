@@ -181,5 +181,17 @@ __device__ __forceinline__ void diag_p(u64p (&re)[8], u64p (&im)[8], bool tp, ui
         if (((uint32_t)j & cl) == cl) cmul2(re[j], im[j], cr, ci);
 }
 
+// Squared norm of a thread's 16 amplitudes: packed FP32 products summed per
+// half (8 amplitudes each), the two halves added in FP64.
+__device__ __forceinline__ double norm2_p(const u64p (&re)[8], const u64p (&im)[8]) {
+    u64p s = 0ull;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        s = fma2(re[j], re[j], s);
+        s = fma2(im[j], im[j], s);
+    }
+    return (double)lo(s) + (double)hi(s);
+}
+
 }  // namespace p32
 }  // namespace qoa
