@@ -628,7 +628,11 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
 // Diagonal factors that are constant over a thread's registers accumulate in
 // a per-thread pending factor, flushed only before an exchange that moves
 // amplitudes between threads whose factors may differ.
-int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParams& P) {
+// pair_pin (complex64 passes): register bit 3, along which the packed FP32
+// kernels pair amplitudes, holds one tile bit for the whole pass (one that
+// no 2x2 gate of the pass targets where there is one), so that every
+// exchange moves whole packed pairs.
+int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParams& P, bool pair_pin) {
     // thread conditions are 32-bit words: lane, warp and tile-number bits
     if (n > 32 - (LANE_BITS + WARP_BITS) + TILE_BITS) return -1;
     memset(&P, 0, sizeof P);
@@ -654,6 +658,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     // register demand per gate (tile bit of each 2x2 target)
     const int ng = (int)st.gates.size();
     std::vector<int> need(ng, -1);
+    int final_q[TILE_BITS];  // qubit each tile bit is stored to
     {
         int tb_sim[64];
         std::memcpy(tb_sim, tb_of, sizeof tb_of);
@@ -661,6 +666,23 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             const Gate& g = G[st.gates[i]];
             if (g.kind == K_G1) need[i] = tb_sim[g.t];
             else if (g.kind == K_SWAP) relabel(tb_sim, g);
+        }
+        for (int q = 0; q < 64; ++q)
+            if (tb_sim[q] >= 0) final_q[tb_sim[q]] = q;
+    }
+    // the pinned pairing bit: a high tile bit stored outside the lanes, the
+    // least used as a 2x2 target (ties: first used latest)
+    int pin = -1;
+    if (pair_pin) {
+        int best_uses = 1 << 30, best_first = -1;
+        for (int t = LANE_BITS; t < TILE_BITS; ++t) {
+            if (final_q[t] < LANE_BITS) continue;
+            int uses = 0, first = 1 << 30;
+            for (int i = 0; i < ng; ++i)
+                if (need[i] == t) { ++uses; first = std::min(first, i); }
+            if (uses < best_uses || (uses == best_uses && first > best_first)) {
+                best_uses = uses; best_first = first; pin = t;
+            }
         }
     }
     auto next_use = [&](int from, int t) {
@@ -675,10 +697,14 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     {
         for (int i = 0; i < LANE_BITS; ++i) m.lane[i] = (uint8_t)i;
         std::vector<std::pair<int, int>> c;
-        for (int t = LANE_BITS; t < TILE_BITS; ++t) c.push_back({next_use(0, t), t});
+        for (int t = LANE_BITS; t < TILE_BITS; ++t) c.push_back({t == pin ? -1 : next_use(0, t), t});
         std::sort(c.begin(), c.end());
         for (int k = 0; k < REG_BITS; ++k) m.reg[k] = (uint8_t)c[k].second;
         for (int k = 0; k < WARP_BITS; ++k) m.warp[k] = (uint8_t)c[REG_BITS + k].second;
+        if (pin >= 0) {  // the pinned bit on register bit 3
+            for (int k = 0; k < REG_BITS - 1; ++k)
+                if (m.reg[k] == pin) std::swap(m.reg[k], m.reg[REG_BITS - 1]);
+        }
     }
     P.map0 = m;
 
@@ -856,7 +882,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     // bring tile bit `must` into the registers
     auto make_reg = [&](int i, int must) -> bool {
         std::vector<std::pair<int, int>> c;
-        for (int t = 0; t < TILE_BITS; ++t) c.push_back({t == must ? -1 : next_use(i, t), t});
+        for (int t = 0; t < TILE_BITS; ++t) c.push_back({t == must ? -1 : (t == pin ? -2 : next_use(i, t)), t});
         std::sort(c.begin(), c.end());
         bool want[TILE_BITS] = {};
         for (int k = 0; k < REG_BITS; ++k) want[c[k].second] = true;
@@ -884,9 +910,8 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         }
         // register positions by next use: the last register bit goes to the
         // tile bit needed last (the complex64 pass pairs amplitudes along it)
-        std::stable_sort(nm.reg, nm.reg + REG_BITS, [&](uint8_t x, uint8_t y) {
-            return (x == must ? -1 : next_use(i, x)) < (y == must ? -1 : next_use(i, y));
-        });
+        auto key = [&](uint8_t x) { return x == pin ? (1 << 30) + 1 : (x == must ? -1 : next_use(i, x)); };
+        std::stable_sort(nm.reg, nm.reg + REG_BITS, [&](uint8_t x, uint8_t y) { return key(x) < key(y); });
         order_lanes(nm);
         return exchange_to(nm);
     };
@@ -1059,6 +1084,10 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             if (!is_lane[m.warp[k]]) high.push_back(m.warp[k]);
         for (int k = 0; k < LANE_BITS; ++k)
             if (!is_lane[m.lane[k]]) high.push_back(m.lane[k]);
+        if (pin >= 0 && !is_lane[pin]) {  // the pinned bit stays on register bit 3
+            high.erase(std::find(high.begin(), high.end(), pin));
+            high.insert(high.begin() + (REG_BITS - 1), pin);
+        }
         for (int k = 0; k < REG_BITS; ++k) nm.reg[k] = (uint8_t)high[k];
         for (int k = 0; k < WARP_BITS; ++k) nm.warp[k] = (uint8_t)high[REG_BITS + k];
         if (!exchange_to(nm)) return -1;
@@ -1374,7 +1403,7 @@ int run_gate(qoa_state_t s, const Gate& g) {
 
 int run_pass(qoa_state_t s, const std::vector<Gate>& G, const Step& st) {
     static thread_local PassParams P;
-    if (build_pass(G, st, s->n, P) != 0) {
+    if (build_pass(G, st, s->n, P, s->precision == QOA_PREC_F32) != 0) {
         // op stream too long for one launch: fall back to per-gate kernels
         for (int gi : st.gates) {
             int rc = run_gate(s, G[gi]);
@@ -1655,7 +1684,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
             std::vector<std::string> bodies;
             size_t b = 0;
             for (size_t k = 0; k < steps.size(); ++k) {
-                if (!steps[k].pass || build_pass(seg, steps[k], s->n, built[b]) != 0) continue;
+                if (!steps[k].pass || build_pass(seg, steps[k], s->n, built[b], c64) != 0) continue;
                 built_of[k] = (int)b;
                 bodies.push_back(c64 ? jit_pass32_body(built[b]) : jit_pass_body(built[b]));
                 ++b;
@@ -1979,7 +2008,8 @@ int batch_prepare(qoa_batch_t b) {
         std::vector<char> step_ok(jobs.size(), 0);
         parallel_for(jobs.size(), [&](size_t x) {
             const size_t i = jobs[x].first, k = jobs[x].second;
-            step_ok[x] = build_pass(b->circs[i].gates, steps_of[i][k], b->circs[i].n, p64[pbase[i] + k]) == 0;
+            step_ok[x] = build_pass(b->circs[i].gates, steps_of[i][k], b->circs[i].n, p64[pbase[i] + k],
+                                    b->precision == QOA_PREC_F32) == 0;
         });
         for (size_t i = 0; i < NC; ++i) built_ok[i] = all_pass[i];
         for (size_t x = 0; x < jobs.size(); ++x)
@@ -2588,7 +2618,7 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
         }
         if (steps[si].pass) {  // make sure the kernel op stream builds
             static thread_local PassParams P;
-            if (build_pass(G, steps[si], ex.n, P) != 0)
+            if (build_pass(G, steps[si], ex.n, P, false) != 0)
                 return set_err(nullptr, QOA_E_ARG, "pass %zu does not fit one launch", si);
             if (getenv("QOA_PLAN_STATS")) {  // op mix of each pass, for tuning
                 int cnt[PC_NCODES] = {};
@@ -2950,7 +2980,8 @@ int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* o
     static thread_local PassParams P;
     for (const Step& st : steps) {
         if (!st.pass) continue;
-        if (build_pass(G, st, n, P) != 0) return set_err(nullptr, QOA_E_ARG, "a pass does not fit one launch");
+        if (build_pass(G, st, n, P, precision == QOA_PREC_F32) != 0)
+            return set_err(nullptr, QOA_E_ARG, "a pass does not fit one launch");
         bodies.push_back(precision == QOA_PREC_F32 ? jit_pass32_body(P) : jit_pass_body(P));
     }
     if (npasses) *npasses = bodies.size();

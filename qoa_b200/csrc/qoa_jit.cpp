@@ -128,6 +128,31 @@ uint32_t reg_part(const TileMap& m, int v) {
     return spos_host(j);
 }
 
+// Pair exchanges (complex64, pairing bit r3 fixed): a tile bit t sits at
+// position t (t < r3) or t - 1 (t > r3) of the 10-bit pair index.
+int pair_pos(int t, int r3) { return t < r3 ? t : t - 1; }
+
+std::string pair_base(const TileMap& m, int r3) {
+    std::string e = "0u";
+    char b[96];
+    for (int i = 0; i < LANE_BITS; ++i) {
+        snprintf(b, sizeof b, " | ((((uint32_t)lane >> %d) & 1u) << %d)", i, pair_pos(m.lane[i], r3));
+        e += b;
+    }
+    for (int i = 0; i < WARP_BITS; ++i) {
+        snprintf(b, sizeof b, " | ((((uint32_t)wid >> %d) & 1u) << %d)", i, pair_pos(m.warp[i], r3));
+        e += b;
+    }
+    return e;
+}
+
+uint32_t pair_part(const TileMap& m, int r3, int j) {
+    uint32_t q = 0;
+    for (int k = 0; k < REG_BITS - 1; ++k)
+        if ((j >> k) & 1) q |= 1u << pair_pos(m.reg[k], r3);
+    return spos_host(q);
+}
+
 }  // namespace
 
 std::string jit_pass_body(const PassParams& P) {
@@ -453,6 +478,26 @@ std::string jit_pass32_body(const PassParams& P) {
                 case PC_XCHG: {
                     const TileMap& mo = *cur;
                     const TileMap& mn = P.xmap[c];
+                    if (mo.reg[REG_BITS - 1] == mn.reg[REG_BITS - 1]) {
+                        // the pairing bit stays on register bit 3: whole
+                        // packed pairs (re[j], im[j]) move as 16-byte units,
+                        // indexed by the tile index without that bit
+                        const int r3 = mo.reg[REG_BITS - 1];
+                        E.line("__syncthreads();");
+                        E.line("{ ulonglong2* pt = reinterpret_cast<ulonglong2*>(tile); const uint32_t pb = spos(%s);",
+                               pair_base(mo, r3).c_str());
+                        for (int j = 0; j < 8; ++j)
+                            E.line("pt[pb ^ %uu] = make_ulonglong2(re[%d], im[%d]);", pair_part(mo, r3, j), j, j);
+                        E.line("}");
+                        E.line("__syncthreads();");
+                        E.line("{ const ulonglong2* pt = reinterpret_cast<const ulonglong2*>(tile); const uint32_t pb = spos(%s);",
+                               pair_base(mn, r3).c_str());
+                        for (int j = 0; j < 8; ++j)
+                            E.line("{ const ulonglong2 u = pt[pb ^ %uu]; re[%d] = u.x; im[%d] = u.y; }", pair_part(mn, r3, j), j, j);
+                        E.line("}");
+                        cur = &mn;
+                        break;
+                    }
                     E.line("__syncthreads();");
                     E.line("{ const uint32_t pb = spos(%s);", tile_base(mo).c_str());
                     for (int j = 0; j < 8; ++j)
