@@ -225,6 +225,9 @@ typedef struct qoa_batch_tuning {
     uint32_t streams;           /* streams the larger circuits spread over */
     uint32_t pass_gate_budget;  /* max gates per tile pass (fusion width); 0 = default */
     uint32_t f32_tensor;        /* complex64 batches: 1 = dense tensor-core blocks, 0 = tile passes */
+    uint32_t jit;               /* tile passes as generated kernels, one per pass structure:
+                                   QOA_JIT_OFF, QOA_JIT_ASYNC (default: compiled in the background,
+                                   the graph is captured again once they are loaded), QOA_JIT_SYNC */
 } qoa_batch_tuning;
 int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out);
 int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, const uint64_t* zmasks, size_t nmasks,
@@ -238,6 +241,9 @@ int qoa_batch_launch(qoa_batch_t b);
 int qoa_batch_stream(qoa_batch_t b, void** stream);
 int qoa_batch_results(qoa_batch_t b, double* out, size_t count);
 int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t* large, uint32_t* graph_ready);
+/* Generated arena kernels: distinct pass structures, how many are loaded,
+ * and whether the captured graph launches them (1) or the interpreter (0). */
+int qoa_batch_jit_info(qoa_batch_t b, uint32_t* structures, uint32_t* ready, uint32_t* graph_uses);
 /* Algorithmic bytes of one run's arena tile passes (each pass reads and
  * writes its circuit's state once) and the number of pass rounds. */
 int qoa_batch_traffic(qoa_batch_t b, double* arena_pass_bytes, uint32_t* rounds);
@@ -398,9 +404,10 @@ int qoa_jit_stats_get(qoa_state_t s, qoa_jit_stats* out);
 /* Host only, no GPU needed: plans an op list for an n-qubit state of the
  * given precision (QOA_PREC_F64 / QOA_PREC_F32 tile passes) and writes the
  * generated source of each pass's kernel (concatenated, NUL terminated,
- * truncated to cap; *len = full length) and the pass count. compile != 0
- * also compiles it with NVRTC (nothing is loaded) and fails with QOA_E_ARG
- * and the compiler log when it does not compile. */
+ * truncated to cap; *len = full length) and the pass count. compile bit 0:
+ * also compile it with NVRTC (nothing is loaded; QOA_E_ARG and the compiler
+ * log when it does not compile); bit 1: the batch (arena) form of each
+ * kernel instead of the single-state form. */
 int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* ops, size_t nops, int compile,
                       char* out, size_t cap, size_t* len, size_t* npasses);
 

@@ -54,7 +54,7 @@ class JitStats(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("small_max_n", ctypes.c_uint32), ("small_threads", ctypes.c_uint32),
                 ("small_ctas_per_sm", ctypes.c_uint32), ("streams", ctypes.c_uint32),
-                ("pass_gate_budget", ctypes.c_uint32), ("f32_tensor", ctypes.c_uint32)]
+                ("pass_gate_budget", ctypes.c_uint32), ("f32_tensor", ctypes.c_uint32), ("jit", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -124,6 +124,7 @@ def _load() -> ctypes.CDLL:
         "qoa_batch_stream": (i32, [vp, P(vp)]),
         "qoa_batch_info": (i32, [vp, P(u32), P(u32), P(u32), P(u32)]),
         "qoa_batch_traffic": (i32, [vp, P(dbl), P(u32)]),
+        "qoa_batch_jit_info": (i32, [vp, P(u32), P(u32), P(u32)]),
         "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
         "qoa_batch_destroy": (i32, [vp]),
         "qoa_server_create": (i32, [P(ServerConfig), P(vp)]),
@@ -502,7 +503,7 @@ def jit_stats() -> dict:
     return {f: getattr(st, f) for f, _ in JitStats._fields_}
 
 
-def jit_translate(n: int, ops, flags: int = 0, compile: bool = False, precision: str = "f64"):
+def jit_translate(n: int, ops, flags: int = 0, compile: bool = False, precision: str = "f64", arena: bool = False):
     """Host only: the generated CUDA source of every tile pass of `ops` on an
     n-qubit state (precision "f64" or "f32"), and the pass count;
     compile=True also compiles it with NVRTC (raises QoaError with the log
@@ -510,10 +511,11 @@ def jit_translate(n: int, ops, flags: int = 0, compile: bool = False, precision:
     arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
     prec = QOA_PREC_F32 if precision == "f32" else QOA_PREC_F64
     ln, npasses = ctypes.c_size_t(), ctypes.c_size_t()
-    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), 0, None, 0, ctypes.byref(ln),
+    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), 2 if arena else 0, None, 0, ctypes.byref(ln),
                                  ctypes.byref(npasses)))
     buf = ctypes.create_string_buffer(ln.value + 1)
-    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), 1 if compile else 0, buf, ln.value + 1,
+    mode = (1 if compile else 0) | (2 if arena else 0)
+    _check(lib.qoa_jit_translate(n, prec, flags, _ptr(arr), len(arr), mode, buf, ln.value + 1,
                                  ctypes.byref(ln), ctypes.byref(npasses)))
     return buf.value.decode(), npasses.value
 
@@ -603,6 +605,13 @@ class Batch:
         by, rounds = ctypes.c_double(), ctypes.c_uint32()
         self._check(lib.qoa_batch_traffic(self._h, ctypes.byref(by), ctypes.byref(rounds)))
         return {"arena_pass_bytes": by.value, "rounds": rounds.value}
+
+    def jit_info(self) -> dict:
+        """Generated arena kernels: pass structures, loaded kernels, and
+        whether the captured graph launches them."""
+        a, r, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(lib.qoa_batch_jit_info(self._h, ctypes.byref(a), ctypes.byref(r), ctypes.byref(g)))
+        return {"structures": a.value, "ready": r.value, "graph_uses_generated": bool(g.value)}
 
     def close(self):
         if getattr(self, "_h", None):

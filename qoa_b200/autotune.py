@@ -50,12 +50,14 @@ def candidates(precision: str) -> List[Dict[str, int]]:
 
 def _time_batch(circuits, precision, tuning, reps=3) -> float:
     import torch
-    from . import Batch
+    from . import Batch, jit_wait
     with Batch(precision) as b:
         b.set_tuning(**tuning)
         for c in circuits:
             b.add(c["n"], c["ops"], c["masks"])
         b.run()
+        b.run()
+        jit_wait()  # generated arena kernels; the next run captures the graph again
         b.run()
         dev = torch.device("cuda", torch.cuda.current_device())
         s = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)

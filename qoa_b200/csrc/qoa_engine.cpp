@@ -14,6 +14,7 @@
 #include <thread>
 #include <functional>
 #include <atomic>
+#include <unordered_map>
 #include <complex>
 #include <cmath>
 #include <cstdarg>
@@ -1689,7 +1690,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
                 bodies.push_back(c64 ? jit_pass32_body(built[b]) : jit_pass_body(built[b]));
                 ++b;
             }
-            jk = jit_request(bodies, s->jit_mode == QOA_JIT_SYNC);
+            jk = jit_request(bodies, s->jit_mode == QOA_JIT_SYNC ? JitWhen::WAIT : JitWhen::SECOND_SIGHTING);
         }
         for (size_t k = 0; k < steps.size(); ++k) {
             const Step& st = steps[k];
@@ -1848,8 +1849,13 @@ struct qoa_batch_s {
     size_t f32_off[5] = {};
     ArenaJob* d_jobs = nullptr;
     uint32_t* d_tstart = nullptr;
-    struct Round { uint32_t job_off, njobs, tiles; int max_nops, max_ncoef; };
+    // one launch of a generated arena kernel: njobs jobs of one structure
+    // from job_off, 2^lt tiles each
+    struct Group { uint32_t job_off, njobs, lt; int kernel; };
+    struct Round { uint32_t job_off, njobs, tiles; int max_nops, max_ncoef; std::vector<Group> groups; };
     std::vector<Round> rounds;
+    std::vector<JitKernel> jit_kernels;  // by structure
+    bool graph_jit = false;              // the captured graph launches the generated kernels
     double arena_pass_bytes = 0;   // algorithmic bytes of one run's arena passes
     uint32_t narena = 0;
     // expectation values of arena and view circuits
@@ -1927,6 +1933,8 @@ void batch_free_device(qoa_batch_t b) {
     dfree(b->arena); dfree(b->d_small); dfree(b->d_ops); dfree(b->d_masks); dfree(b->d_out); dfree(b->d_counter);
     dfree(b->d_params); dfree(b->d_f32); dfree(b->d_jobs); dfree(b->d_tstart); dfree(b->d_ejobs); dfree(b->d_epart);
     b->rounds.clear();
+    b->jit_kernels.clear();
+    b->graph_jit = false;
     b->arena_pass_bytes = 0;
     b->nsmall = b->narena = b->n_ejobs = b->e_chunks = 0;
     b->prepared = false;
@@ -1939,6 +1947,48 @@ int upload(qoa_batch_t b, T*& dst, const std::vector<T>& src) {
     if (!src.empty()) BCK(cudaMemcpy((void*)dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
     return QOA_OK;
 }
+
+// fn(0) .. fn(count - 1) on all host cores
+void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
+    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+        pool.emplace_back([&] {
+            for (size_t k; (k = next.fetch_add(1)) < count;) fn(k);
+        });
+    for (auto& th : pool) th.join();
+}
+
+// The parts of a PassParams that its generated kernel depends on (all but
+// the coefficient values, the global phase and the angle values): passes
+// that agree here share one generated kernel. build_pass zeroes unused
+// fields, so whole arrays compare.
+struct PassShape {
+    const PassParams* P;
+    size_t nangles() const { return P->nang ? P->ang_start[P->nang] : 0; }
+    uint64_t hash() const {
+        uint64_t h = 1469598103934665603ull;
+        auto mix = [&](const void* p, size_t nb) {
+            const unsigned char* c = (const unsigned char*)p;
+            for (size_t i = 0; i < nb; ++i) { h ^= c[i]; h *= 1099511628211ull; }
+        };
+        mix(&P->n, 3 * sizeof(uint32_t));
+        mix(P->slot_qubit, offsetof(PassParams, ops) - offsetof(PassParams, slot_qubit));
+        mix(P->ops, P->nops * sizeof(PassOp));
+        for (size_t e = 0; e < nangles(); ++e) mix(&P->angles[e].omask, sizeof(uint64_t));
+        return h;
+    }
+    bool operator==(const PassShape& o) const {
+        const PassParams &a = *P, &b = *o.P;
+        if (a.n != b.n || a.nops != b.nops || a.ncoef != b.ncoef) return false;
+        if (memcmp(a.slot_qubit, b.slot_qubit, offsetof(PassParams, ops) - offsetof(PassParams, slot_qubit))) return false;
+        if (memcmp(a.ops, b.ops, a.nops * sizeof(PassOp))) return false;
+        for (size_t e = 0; e < nangles(); ++e)
+            if (a.angles[e].omask != b.angles[e].omask) return false;
+        return true;
+    }
+};
 
 int batch_prepare(qoa_batch_t b) {
     const bool f32 = b->precision == QOA_PREC_F32;
@@ -1978,16 +2028,6 @@ int batch_prepare(qoa_batch_t b) {
     std::vector<char> all_pass(NC, 0), built_ok(NC, 0);
     std::vector<size_t> pbase(NC, 0);
     if (!tensor) {
-        auto parallel_for = [](size_t count, const std::function<void(size_t)>& fn) {
-            const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
-            std::atomic<size_t> next{0};
-            std::vector<std::thread> pool;
-            for (unsigned t = 0; t < nt; ++t)
-                pool.emplace_back([&] {
-                    for (size_t k; (k = next.fetch_add(1)) < count;) fn(k);
-                });
-            for (auto& th : pool) th.join();
-        };
         parallel_for(NC, [&](size_t i) {
             const auto& c = b->circs[i];
             if (is_small[i] || c.n < (uint32_t)TILE_BITS || c.gates.empty()) return;
@@ -2098,12 +2138,52 @@ int batch_prepare(qoa_batch_t b) {
     std::vector<uint32_t> tstart;
     size_t maxp = 0;
     for (auto& v : pass_idx) maxp = std::max(maxp, v.size());
+    // generated arena kernels: every distinct pass structure gets one; a
+    // round's jobs are ordered by structure so that each structure's jobs
+    // are one contiguous launch
+    const bool jit = !tensor && b->tune.jit != QOA_JIT_OFF && !p64.empty();
+    std::vector<int> shape_of(p64.size(), -1);
+    std::vector<uint32_t> reps;  // representative pass of each structure
+    if (jit) {
+        std::vector<uint64_t> hs(p64.size());
+        parallel_for(p64.size(), [&](size_t k) { hs[k] = PassShape{&p64[k]}.hash(); });
+        std::unordered_map<uint64_t, std::vector<int>> by_hash;
+        for (auto& v : pass_idx)
+            for (uint32_t pi : v) {
+                auto& cands = by_hash[hs[pi]];
+                int found = -1;
+                for (int sid : cands)
+                    if (PassShape{&p64[reps[sid]]} == PassShape{&p64[pi]}) { found = sid; break; }
+                if (found < 0) {
+                    found = (int)reps.size();
+                    reps.push_back(pi);
+                    cands.push_back(found);
+                }
+                shape_of[pi] = found;
+            }
+        std::vector<std::string> bodies(reps.size());
+        parallel_for(reps.size(), [&](size_t k) {
+            bodies[k] = f32 ? jit_pass32_body(p64[reps[k]], true) : jit_pass_body(p64[reps[k]], true);
+        });
+        b->jit_kernels = jit_request(bodies, b->tune.jit == QOA_JIT_SYNC ? JitWhen::WAIT : JitWhen::NOW);
+    }
     for (size_t r = 0; r < maxp; ++r) {
-        qoa_batch_s::Round R{(uint32_t)jobs.size(), 0, 0, 0, 0};
-        for (size_t i = 0; i < b->circs.size(); ++i) {
-            if (pass_idx[i].size() <= r) continue;
+        qoa_batch_s::Round R{(uint32_t)jobs.size(), 0, 0, 0, 0, {}};
+        std::vector<size_t> order;
+        for (size_t i = 0; i < b->circs.size(); ++i)
+            if (pass_idx[i].size() > r) order.push_back(i);
+        if (jit)
+            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+                return shape_of[pass_idx[x][r]] < shape_of[pass_idx[y][r]];
+            });
+        for (size_t i : order) {
             const auto& c = b->circs[i];
             const uint32_t pi = pass_idx[i][r];
+            if (jit) {
+                if (R.groups.empty() || R.groups.back().kernel != shape_of[pi])
+                    R.groups.push_back({(uint32_t)jobs.size(), 0, c.n - (uint32_t)TILE_BITS, shape_of[pi]});
+                R.groups.back().njobs++;
+            }
             ArenaJob J;
             J.amps = arena + c.state_off;
             J.params = (const unsigned char*)b->d_params + (size_t)pi * psz;
@@ -2224,7 +2304,14 @@ int batch_enqueue(qoa_batch_t b) {
     }
     const unsigned char* fb = (const unsigned char*)b->d_f32;
     const bool tensor = f32 && b->tune.f32_tensor;
+    bool all_ready = !b->jit_kernels.empty();
+    for (const auto& k : b->jit_kernels) all_ready = all_ready && k.ready();
     for (const auto& R : b->rounds) {
+        if (all_ready && !R.groups.empty()) {
+            for (const auto& Gp : R.groups)
+                BCK(b->jit_kernels[Gp.kernel].launch_arena(b->d_jobs + Gp.job_off, Gp.njobs, Gp.lt, s0));
+            continue;
+        }
         if (tensor)
             BCK(launch_f32_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                       (const float*)(fb + b->f32_off[0]), (const F32PhaseOp*)(fb + b->f32_off[1]),
@@ -2242,6 +2329,26 @@ int batch_enqueue(qoa_batch_t b) {
         BCK(cudaStreamWaitEvent(s0, b->events[i], 0));
     }
     BCK(launch_arena_expz(f32, b->d_ejobs, b->n_ejobs, b->e_chunks, b->d_masks, b->d_epart, b->d_out, s0));
+    b->graph_jit = all_ready;
+    return QOA_OK;
+}
+
+bool batch_jit_all_ready(qoa_batch_t b) {
+    if (b->jit_kernels.empty()) return false;
+    for (const auto& k : b->jit_kernels)
+        if (!k.ready()) return false;
+    return true;
+}
+
+// Drops a graph captured with interpreter passes once the generated kernels
+// are all loaded (the next run captures again).
+int batch_refresh_graph(qoa_batch_t b) {
+    if (!b->exec || b->graph_jit || !batch_jit_all_ready(b)) return QOA_OK;
+    BCK(cudaStreamSynchronize(b->streams[0]));
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
     return QOA_OK;
 }
 
@@ -2670,6 +2777,7 @@ int qoa_batch_create(int precision, uint32_t flags, qoa_batch_t* out) {
     b->tune.streams = 8;
     b->tune.pass_gate_budget = 0;
     b->tune.f32_tensor = 0;
+    b->tune.jit = QOA_JIT_ASYNC;
     *out = b;
     return QOA_OK;
 }
@@ -2707,7 +2815,7 @@ int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, con
 int qoa_batch_set_tuning(qoa_batch_t b, const qoa_batch_tuning* t) {
     if (!b || !t) return bset_err(b, QOA_E_ARG, "null argument");
     if (t->small_threads < 32 || t->small_threads > 1024 || (t->small_threads & 31) || t->small_ctas_per_sm < 1 ||
-        t->streams < 1 || t->streams > 64)
+        t->streams < 1 || t->streams > 64 || t->jit > QOA_JIT_SYNC)
         return bset_err(b, QOA_E_ARG, "bad tuning values");
     if (b->prepared) {
         cudaSetDevice(b->device);
@@ -2739,6 +2847,8 @@ int qoa_batch_run(qoa_batch_t b) {
         b->runs++;
         return QOA_OK;
     }
+    int rrc = batch_refresh_graph(b);
+    if (rrc) return rrc;
     if (!b->exec) {
         // second run: capture the same launches into a graph, then replay it
         BCK(cudaStreamBeginCapture(b->streams[0], cudaStreamCaptureModeThreadLocal));
@@ -2760,6 +2870,19 @@ int qoa_batch_launch(qoa_batch_t b) {
     if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
     if (!b->exec) return bset_err(b, QOA_E_ARG, "qoa_batch_launch replays the graph that the second qoa_batch_run makes");
     if (cudaSetDevice(b->device) != cudaSuccess) return bset_err(b, QOA_E_CUDA, "cudaSetDevice failed");
+    if (!b->graph_jit && batch_jit_all_ready(b)) {
+        // the generated kernels arrived after the capture: capture again
+        int rc = batch_refresh_graph(b);
+        if (rc) return rc;
+        BCK(cudaStreamBeginCapture(b->streams[0], cudaStreamCaptureModeThreadLocal));
+        rc = batch_enqueue(b);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->streams[0], &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        BCK(e);
+        b->graph = g;
+        BCK(cudaGraphInstantiate(&b->exec, g, 0));
+    }
     BCK(cudaGraphLaunch(b->exec, b->streams[0]));
     return QOA_OK;
 }
@@ -2787,6 +2910,16 @@ int qoa_batch_info(qoa_batch_t b, uint32_t* circuits, uint32_t* small, uint32_t*
     if (small) *small = b->nsmall;
     if (large) *large = b->narena + (uint32_t)b->views.size();
     if (graph_ready) *graph_ready = b->exec ? 1u : 0u;
+    return QOA_OK;
+}
+
+int qoa_batch_jit_info(qoa_batch_t b, uint32_t* structures, uint32_t* ready, uint32_t* graph_uses) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    uint32_t r = 0;
+    for (const auto& k : b->jit_kernels) r += k.ready() ? 1u : 0u;
+    if (structures) *structures = (uint32_t)b->jit_kernels.size();
+    if (ready) *ready = r;
+    if (graph_uses) *graph_uses = (b->exec && b->graph_jit) ? 1u : 0u;
     return QOA_OK;
 }
 
@@ -2982,7 +3115,8 @@ int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* o
         if (!st.pass) continue;
         if (build_pass(G, st, n, P, precision == QOA_PREC_F32) != 0)
             return set_err(nullptr, QOA_E_ARG, "a pass does not fit one launch");
-        bodies.push_back(precision == QOA_PREC_F32 ? jit_pass32_body(P) : jit_pass_body(P));
+        const bool arena = (compile & 2) != 0;
+        bodies.push_back(precision == QOA_PREC_F32 ? jit_pass32_body(P, arena) : jit_pass_body(P, arena));
     }
     if (npasses) *npasses = bodies.size();
     const std::string text = jit_program(bodies);
@@ -2992,7 +3126,7 @@ int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* o
         memcpy(out, text.data(), k);
         out[k] = '\0';
     }
-    if (compile && !bodies.empty()) {
+    if ((compile & 1) && !bodies.empty()) {
         std::string err;
         if (!jit_compile_only(bodies, err)) return set_err(nullptr, QOA_E_ARG, "%s", err.c_str());
     }

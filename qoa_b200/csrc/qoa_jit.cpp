@@ -155,18 +155,41 @@ uint32_t pair_part(const TileMap& m, int r3, int j) {
 
 }  // namespace
 
-std::string jit_pass_body(const PassParams& P) {
-    Emit E;
-    E.line("(double2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
-    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials) {");
+// Kernel head shared by both precisions: the signature, shared memory, the
+// thread's lane / warp / tile number, the amplitude pointer, the pass
+// parameters P and the input's squared norm nrm. Single-state form: P is the
+// __grid_constant__ parameter, one CTA per tile. Arena form: CTA b runs tile
+// b % 2^(n - 11) of job b / 2^(n - 11) (every job of the launch has this
+// structure), P is the job's PassParams in global memory and its
+// coefficients are staged in shared memory (scoef).
+void emit_head(Emit& E, const PassParams& P, bool c64, bool arena) {
+    const char* T = c64 ? "float2" : "double2";
+    if (arena) {
+        E.line("(const qoa::ArenaJob* __restrict__ jobs) {");
+    } else {
+        E.line("(%s* __restrict__ amps, const __grid_constant__ qoa::PassParams P,", T);
+        E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials) {");
+    }
     E.line("using namespace qoa;");
-    E.line("typedef double2 T;");
+    if (c64) E.line("using namespace qoa::p32;");
+    E.line("typedef %s T;", T);
     E.line("__shared__ __align__(16) T tile[1 << TILE_BITS];");
-    E.line("__shared__ double red[PASS_THREADS / 32];");
+    if (!arena) E.line("__shared__ double red[PASS_THREADS / 32];");
+    if (c64 || arena) E.line("__shared__ __align__(16) T scoef[%u];", P.ncoef ? P.ncoef : 1);
     if (P.nang) E.line("__shared__ T sang[%u];", P.nang);
     E.line("const int lane = threadIdx.x & 31;");
     E.line("const int wid = threadIdx.x >> 5;");
-    E.line("const uint64_t blk = blockIdx.x;");
+    if (arena) {
+        const int lt = (int)P.n - TILE_BITS;
+        E.line("const qoa::ArenaJob J = jobs[blockIdx.x >> %d];", lt);
+        E.line("const uint64_t blk = blockIdx.x & 0x%xu;", (1u << lt) - 1);
+        E.line("T* __restrict__ amps = reinterpret_cast<T*>(J.amps);");
+        E.line("const PassParams& P = *reinterpret_cast<const PassParams*>(J.params);");
+        E.line("const double nrm = J.fresh ? 0.0 : 1.0;");
+    } else {
+        E.line("const uint64_t blk = blockIdx.x;");
+        E.line("const double nrm = *norm2_in;");
+    }
     E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
            LANE_BITS + WARP_BITS);
     // tile origin: the tile number's bits deposited into the outer qubits,
@@ -185,8 +208,19 @@ std::string jit_pass_body(const PassParams& P) {
         }
         E.line("const uint64_t g0 = %s;", g.c_str());
     }
-    E.line("const double nrm = *norm2_in;");
+    if (c64)
+        E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);",
+               P.ncoef);
+    else if (arena)
+        E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = P.coef[i];", P.ncoef);
     if (P.nang) E.line("pass_angles(P, blk, sang);");
+}
+
+std::string jit_pass_body(const PassParams& P, bool arena) {
+    Emit E;
+    // complex128 coefficients: the parameter's constant bank, or the staged copy
+    const char* cf = arena ? "scoef" : "P.coef";
+    emit_head(E, P, false, arena);
     E.line("const bool valid = nrm > 1e-12;");
     E.line("T pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;");
     E.line("T a[REGS];");
@@ -211,7 +245,7 @@ std::string jit_pass_body(const PassParams& P) {
         E.line("}");
         E.line("}");
     }
-    if (P.nang) E.line("__syncthreads();");
+    if (P.nang || arena) E.line("__syncthreads();");
 
     const TileMap* cur = &P.map0;
     const uint32_t* ow = reinterpret_cast<const uint32_t*>(P.ops);
@@ -222,20 +256,20 @@ std::string jit_pass_body(const PassParams& P) {
         const uint32_t cr = op.cond_reg;
         const uint32_t tm = ow[4 * oi + 2];
         if (code >= PC_HF && code < PC_XC) {
-            E.line("g1r<%s, %d>(a, P.coef + %u);", g1_name(code), code & 3, c);
+            E.line("g1r<%s, %d>(a, %s + %u);", g1_name(code), code & 3, cf, c);
         } else if (code >= PC_RXB && code < PC_DIAG_TA) {
-            E.line("g1r<%s, %d>(a, P.coef + %u);", g1_name(code), code & 3, c);
+            E.line("g1r<%s, %d>(a, %s + %u);", g1_name(code), code & 3, cf, c);
         } else if (code >= PC_XC && code < PC_RXB) {
             E.line("g1rc<%s, %d>(a, %s, 0x%xu);", (code & ~3) == PC_XC ? "G1_X" : "G1_Y", code & 3,
                    tcond(tm).c_str(), cr);
         } else {
             switch (code) {
                 case PC_DIAG_T:
-                    if (tm) E.line("if (%s) pend = c_mul(pend, P.coef[%u]);", tcond(tm).c_str(), c);
-                    else E.line("pend = c_mul(pend, P.coef[%u]);", c);
+                    if (tm) E.line("if (%s) pend = c_mul(pend, %s[%u]);", tcond(tm).c_str(), cf, c);
+                    else E.line("pend = c_mul(pend, %s[%u]);", cf, c);
                     break;
                 case PC_DIAG_M:
-                    E.line("diag_m(a, %s, 0x%xu, P.coef[%u]);", tcond(tm).c_str(), cr, c);
+                    E.line("diag_m(a, %s, 0x%xu, %s[%u]);", tcond(tm).c_str(), cr, cf, c);
                     break;
                 case PC_DIAG_TA:
                     if (tm) E.line("if (%s) pend = c_mul(pend, sang[%u]);", tcond(tm).c_str(), c);
@@ -254,10 +288,10 @@ std::string jit_pass_body(const PassParams& P) {
                     for (uint32_t e = 1; e <= cnt; ++e) {
                         const PassOp& r = P.ops[oi + e];
                         const uint32_t rtm = ow[4 * (oi + e) + 2];
-                        if (!rtm && one) E.line("f = P.coef[%u];", (unsigned)r.coef);
-                        else if (one) E.line("f = %s ? P.coef[%u] : make_double2(1.0, 0.0);", tcond(rtm).c_str(), (unsigned)r.coef);
-                        else if (!rtm) E.line("f = c_mul(f, P.coef[%u]);", (unsigned)r.coef);
-                        else E.line("if (%s) f = c_mul(f, P.coef[%u]);", tcond(rtm).c_str(), (unsigned)r.coef);
+                        if (!rtm && one) E.line("f = %s[%u];", cf, (unsigned)r.coef);
+                        else if (one) E.line("f = %s ? %s[%u] : make_double2(1.0, 0.0);", tcond(rtm).c_str(), cf, (unsigned)r.coef);
+                        else if (!rtm) E.line("f = c_mul(f, %s[%u]);", cf, (unsigned)r.coef);
+                        else E.line("if (%s) f = c_mul(f, %s[%u]);", tcond(rtm).c_str(), cf, (unsigned)r.coef);
                         one = false;
                         if (code == PC_DIAG_MX && (e == cnt || ((r.has_tp >> 1) & 1u))) {
                             E.line("diag_m(a, true, 0x%xu, f);", (unsigned)r.cond_reg);
@@ -271,7 +305,7 @@ std::string jit_pass_body(const PassParams& P) {
                     break;
                 }
                 case PC_DIAG_TAB:
-                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], P.coef[%u]);", v, v, c + v);
+                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], %s[%u]);", v, v, cf, c + v);
                     break;
                 case PC_FLUSH:
                     for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], pend);", v, v);
@@ -303,14 +337,15 @@ std::string jit_pass_body(const PassParams& P) {
         E.line("{");
         E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
                ostride(m.warp[0]), ostride(m.warp[1]));
-        E.line("double ss = 0.0;");
+        if (!arena) E.line("double ss = 0.0;");
         for (int v = 0; v < REGS; ++v) {
             unsigned long long off = 0;
             for (int k = 0; k < REG_BITS; ++k)
                 if ((v >> k) & 1) off += ostride(m.reg[k]);
-            E.line("{ const T x = c_mul(a[%d], pend); __stcs(amps + (tb + 0x%llxull), x); ss += c_abs2(x); }", v, off);
+            E.line("{ const T x = c_mul(a[%d], pend); __stcs(amps + (tb + 0x%llxull), x);%s }", v, off,
+                   arena ? "" : " ss += c_abs2(x);");
         }
-        E.line("block_norm_partial(ss, red, partials + blk);");
+        if (!arena) E.line("block_norm_partial(ss, red, partials + blk);");
         E.line("}");
     }
     E.line("}");
@@ -321,38 +356,9 @@ std::string jit_pass_body(const PassParams& P) {
 // (pass_tile_p32) for the same PassParams. Registers hold re[j] / im[j] =
 // packed (amplitude j, amplitude j + 8); coefficients are rounded to float
 // once per CTA into shared memory, as the interpreter stages them.
-std::string jit_pass32_body(const PassParams& P) {
+std::string jit_pass32_body(const PassParams& P, bool arena) {
     Emit E;
-    E.line("(float2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
-    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials) {");
-    E.line("using namespace qoa;");
-    E.line("using namespace qoa::p32;");
-    E.line("__shared__ __align__(16) float2 tile[1 << TILE_BITS];");
-    E.line("__shared__ double red[PASS_THREADS / 32];");
-    const uint32_t ncoef = P.ncoef ? P.ncoef : 1;
-    E.line("__shared__ float2 scoef[%u];", ncoef);
-    if (P.nang) E.line("__shared__ float2 sang[%u];", P.nang);
-    E.line("const int lane = threadIdx.x & 31;");
-    E.line("const int wid = threadIdx.x >> 5;");
-    E.line("const uint64_t blk = blockIdx.x;");
-    E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
-           LANE_BITS + WARP_BITS);
-    {
-        std::string g = "0ull";
-        const int nout = (int)P.n - TILE_BITS;
-        char b[128];
-        for (int k = 0; k < nout;) {
-            int len = 1;
-            while (k + len < nout && P.outer_qubits[k + len] == P.outer_qubits[k] + len) ++len;
-            snprintf(b, sizeof b, " | (((blk >> %d) & 0x%llxull) << %d)", k,
-                     (unsigned long long)((len >= 64) ? ~0ull : ((1ull << len) - 1)), P.outer_qubits[k]);
-            g += b;
-            k += len;
-        }
-        E.line("const uint64_t g0 = %s;", g.c_str());
-    }
-    E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);",
-           P.ncoef);
+    emit_head(E, P, true, arena);
     // register tables (PC_DIAG_TAB): staged once per CTA already packed as
     // (factor j, factor j + 8) pairs, real parts then imaginary parts
     std::vector<uint32_t> tab_at(P.nops, 0);
@@ -376,8 +382,6 @@ std::string jit_pass32_body(const PassParams& P) {
             }
         }
     }
-    if (P.nang) E.line("pass_angles(P, blk, sang);");
-    E.line("const double nrm = *norm2_in;");
     E.line("const bool valid = nrm > 1e-12;");
     E.line("float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))");
     E.line("                    : make_float2((float)P.phase.x, (float)P.phase.y);");
@@ -533,7 +537,7 @@ std::string jit_pass32_body(const PassParams& P) {
                    j, j, j, j, j, j);
             E.line("  __stcs(amps + (tb + 0x%llxull), a); __stcs(amps + (tb + 0x%llxull), b); }", off, off + r3);
         }
-        E.line("block_norm_partial(norm2_p(re, im), red, partials + blk);");
+        if (!arena) E.line("block_norm_partial(norm2_p(re, im), red, partials + blk);");
         E.line("}");
     }
     E.line("}");
@@ -558,6 +562,14 @@ cudaError_t JitKernel::launch(void* amps, const PassParams& P, const double* nor
     return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(blocks), dim3(PASS_THREADS), args, 0, st);
 }
 
+cudaError_t JitKernel::launch_arena(const ArenaJob* jobs, uint32_t njobs, uint32_t lt, cudaStream_t st) const {
+    if (!ready()) return cudaErrorNotReady;
+    if (!njobs) return cudaSuccess;
+    void* args[] = {&jobs};
+    return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(njobs << lt), dim3(PASS_THREADS), args, 0,
+                            st);
+}
+
 namespace {
 
 uint64_t fnv64(const std::string& s) {
@@ -569,11 +581,15 @@ uint64_t fnv64(const std::string& s) {
     return h;
 }
 
+bool body_is_c64(const std::string& body) {
+    return body.find("using namespace qoa::p32;") < 200;
+}
+
 std::string program_text(const std::vector<std::string>& names, const std::vector<std::string>& bodies) {
     std::string src = kPrelude;
     char head[160];
     for (size_t i = 0; i < names.size(); ++i) {
-        const bool c64 = bodies[i].compare(0, 7, "(float2") == 0;
+        const bool c64 = body_is_c64(bodies[i]);
         snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS,
                  occ_target(c64), names[i].c_str());
         src += head;
@@ -614,7 +630,8 @@ bool build_cubin(const std::vector<std::string>& names, const std::vector<std::s
 
 std::string kernel_name(const std::string& body) {
     char nm[48];
-    snprintf(nm, sizeof nm, "%s_%016llx", body.compare(0, 7, "(float2") == 0 ? "qoa_jit_pass32" : "qoa_jit_pass",
+    const bool arena = body.compare(0, 20, "(const qoa::ArenaJob") == 0;
+    snprintf(nm, sizeof nm, "qoa_jit_%s%s_%016llx", arena ? "arena" : "pass", body_is_c64(body) ? "32" : "",
              (unsigned long long)fnv64(body));
     return nm;
 }
@@ -638,7 +655,8 @@ public:
             if (t.joinable()) t.join();
     }
 
-    std::vector<JitKernel> request(const std::vector<std::string>& bodies, bool wait) {
+    std::vector<JitKernel> request(const std::vector<std::string>& bodies, JitWhen when) {
+        const bool wait = when == JitWhen::WAIT;
         std::vector<JitKernel> out;
         std::vector<std::shared_ptr<JitEntry>> mine;
         out.reserve(bodies.size());
@@ -653,7 +671,7 @@ public:
                     mine.push_back(it->second);
                     continue;
                 }
-                if (!wait) {
+                if (when == JitWhen::SECOND_SIGHTING) {
                     // a structure is compiled the second time it is seen:
                     // one-off passes (a noisy trajectory's Pauli draws, a
                     // program run once) never pay for a compile
@@ -816,8 +834,8 @@ bool jit_compile_only(const std::vector<std::string>& bodies, std::string& err) 
     return ok;
 }
 
-std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, bool wait) {
-    return compiler().request(bodies, wait);
+std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, JitWhen when) {
+    return compiler().request(bodies, when);
 }
 void jit_wait_all() { compiler().wait_all(); }
 JitStats jit_stats() { return compiler().stats(); }

@@ -33,6 +33,8 @@ public:
     // amps: double2* (complex128 kernels) or float2* (complex64 kernels).
     cudaError_t launch(void* amps, const PassParams& P, const double* norm2_in, double* partials,
                        cudaStream_t st) const;
+    // Arena form: njobs device ArenaJob records from `jobs`, 2^lt tiles each.
+    cudaError_t launch_arena(const ArenaJob* jobs, uint32_t njobs, uint32_t lt, cudaStream_t st) const;
 
 private:
     std::shared_ptr<JitEntry> e_;
@@ -41,14 +43,19 @@ private:
 // The kernel body (everything after the kernel's name) for a pass:
 // complex128 (the k_pass form) or complex64 (the packed FP32 form of
 // k_pass_p32).
-std::string jit_pass_body(const PassParams& P);
-std::string jit_pass32_body(const PassParams& P);
+// arena: the batch form, one launch over many jobs of this structure
+// (ArenaJob list; CTA b runs tile b % 2^(n-11) of job b / 2^(n-11)).
+std::string jit_pass_body(const PassParams& P, bool arena = false);
+std::string jit_pass32_body(const PassParams& P, bool arena = false);
 
-// Looks each body up in the process-wide cache. wait: the missing ones are
-// compiled now and the call returns when they are loaded. Otherwise a
-// missing body is queued for the compile threads the second time it is
-// requested (the first request returns an empty, never-ready kernel).
-std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, bool wait);
+// Looks each body up in the process-wide cache; a missing one is compiled
+// on the compile threads:
+//   SECOND_SIGHTING  the second time it is requested (the first request
+//                    returns an empty, never-ready kernel)
+//   NOW              now, without waiting
+//   WAIT             now, and the call returns when they are loaded
+enum class JitWhen { SECOND_SIGHTING, NOW, WAIT };
+std::vector<JitKernel> jit_request(const std::vector<std::string>& bodies, JitWhen when);
 
 // The whole NVRTC program text for these bodies (prelude, kernels).
 std::string jit_program(const std::vector<std::string>& bodies);

@@ -138,3 +138,53 @@ def test_autotune_picks_a_valid_tuning(tmp_path, circs, ref):
     assert autotune.tune(circs, "f64", sample=12, cache=cache) == best     # served from the cache
     first, _, _ = run_batch(circs, "f64", **best)
     np.testing.assert_allclose(first, ref, rtol=0, atol=F64_TOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_batch_generated_arena_kernels(circs, ref, precision):
+    """Arena passes as generated kernels (one per pass structure, compiled
+    before the first run) give the interpreter's results bit for bit, and the
+    oracle's within tolerance; the graph launches the generated kernels."""
+    big = [c for c in circs if c["n"] >= 11] + C.variational_batch(count=6, nmin=13, nmax=15, lmin=2, lmax=3,
+                                                                    nmasks=4, seed=12)
+    with qb.Batch(precision) as b:
+        b.set_tuning(jit=qb.QOA_JIT_SYNC, small_max_n=10, f32_tensor=0)
+        for c in big:
+            b.add(c["n"], c["ops"], c["masks"])
+        b.run()
+        gen = b.results()
+        b.run()
+        b.run()
+        info = b.jit_info()
+        again = b.results()
+    with qb.Batch(precision) as b:
+        b.set_tuning(jit=qb.QOA_JIT_OFF, small_max_n=10, f32_tensor=0)
+        for c in big:
+            b.add(c["n"], c["ops"], c["masks"])
+        b.run()
+        interp = b.results()
+    assert info["structures"] > 0 and info["ready"] == info["structures"]
+    assert info["graph_uses_generated"]
+    assert np.array_equal(gen, interp)
+    assert np.array_equal(gen, again)
+    exp = expected(big)
+    tol = F64_TOL if precision == "f64" else F32_TOL
+    assert np.max(np.abs(gen - exp)) < tol
+
+
+@pytest.mark.gpu
+def test_batch_graph_recaptured_when_kernels_arrive(circs):
+    big = [c for c in circs if c["n"] >= 11]
+    with qb.Batch("f64") as b:
+        b.set_tuning(jit=qb.QOA_JIT_ASYNC, small_max_n=10)
+        for c in big:
+            b.add(c["n"], c["ops"], c["masks"])
+        b.run()
+        first = b.results()
+        b.run()
+        qb.jit_wait()
+        b.launch()          # replays, capturing again with the generated kernels
+        qb_sync = b.results()
+        assert b.jit_info()["graph_uses_generated"]
+    assert np.array_equal(first, qb_sync)
