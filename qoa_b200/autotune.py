@@ -50,14 +50,14 @@ def candidates(precision: str) -> List[Dict[str, int]]:
 
 def _time_batch(circuits, precision, tuning, reps=3) -> float:
     import torch
-    from . import Batch, jit_wait
+    from . import Batch
     with Batch(precision) as b:
-        b.set_tuning(**tuning)
+        # the candidates are timed on the interpreted passes: generated
+        # kernels would make every candidate pay for its compiles
+        b.set_tuning(**dict(tuning, jit=0))
         for c in circuits:
             b.add(c["n"], c["ops"], c["masks"])
         b.run()
-        b.run()
-        jit_wait()  # generated arena kernels; the next run captures the graph again
         b.run()
         dev = torch.device("cuda", torch.cuda.current_device())
         s = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)

@@ -1967,6 +1967,12 @@ void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
 struct PassShape {
     const PassParams* P;
     size_t nangles() const { return P->nang ? P->ang_start[P->nang] : 0; }
+    // the factored form of a rotation follows its angle: one shape for both
+    static PassOp canon(PassOp o) {
+        if (o.code >= PC_RXB && o.code < PC_RXB + 4) o.code = (uint8_t)(PC_RX + (o.code - PC_RXB));
+        else if (o.code >= PC_RYB && o.code < PC_RYB + 4) o.code = (uint8_t)(PC_RY + (o.code - PC_RYB));
+        return o;
+    }
     uint64_t hash() const {
         uint64_t h = 1469598103934665603ull;
         auto mix = [&](const void* p, size_t nb) {
@@ -1975,7 +1981,10 @@ struct PassShape {
         };
         mix(&P->n, 3 * sizeof(uint32_t));
         mix(P->slot_qubit, offsetof(PassParams, ops) - offsetof(PassParams, slot_qubit));
-        mix(P->ops, P->nops * sizeof(PassOp));
+        for (uint32_t k = 0; k < P->nops; ++k) {
+            const PassOp o = canon(P->ops[k]);
+            mix(&o, sizeof o);
+        }
         for (size_t e = 0; e < nangles(); ++e) mix(&P->angles[e].omask, sizeof(uint64_t));
         return h;
     }
@@ -1983,7 +1992,10 @@ struct PassShape {
         const PassParams &a = *P, &b = *o.P;
         if (a.n != b.n || a.nops != b.nops || a.ncoef != b.ncoef) return false;
         if (memcmp(a.slot_qubit, b.slot_qubit, offsetof(PassParams, ops) - offsetof(PassParams, slot_qubit))) return false;
-        if (memcmp(a.ops, b.ops, a.nops * sizeof(PassOp))) return false;
+        for (uint32_t k = 0; k < a.nops; ++k) {
+            const PassOp x = canon(a.ops[k]), y = canon(b.ops[k]);
+            if (memcmp(&x, &y, sizeof x)) return false;
+        }
         for (size_t e = 0; e < nangles(); ++e)
             if (a.angles[e].omask != b.angles[e].omask) return false;
         return true;
@@ -2141,7 +2153,7 @@ int batch_prepare(qoa_batch_t b) {
     // generated arena kernels: every distinct pass structure gets one; a
     // round's jobs are ordered by structure so that each structure's jobs
     // are one contiguous launch
-    const bool jit = !tensor && b->tune.jit != QOA_JIT_OFF && !p64.empty();
+    bool jit = !tensor && b->tune.jit != QOA_JIT_OFF && !p64.empty();
     std::vector<int> shape_of(p64.size(), -1);
     std::vector<uint32_t> reps;  // representative pass of each structure
     if (jit) {
@@ -2161,6 +2173,13 @@ int batch_prepare(qoa_batch_t b) {
                 }
                 shape_of[pi] = found;
             }
+        // in the default mode a structure must serve at least 8 passes of
+        // the batch to be worth its compile (~0.3 s of host time)
+        size_t npass = 0;
+        for (auto& v : pass_idx) npass += v.size();
+        if (b->tune.jit == QOA_JIT_ASYNC && reps.size() * 8 > npass) jit = false;
+    }
+    if (jit) {
         std::vector<std::string> bodies(reps.size());
         parallel_for(reps.size(), [&](size_t k) {
             bodies[k] = f32 ? jit_pass32_body(p64[reps[k]], true) : jit_pass_body(p64[reps[k]], true);

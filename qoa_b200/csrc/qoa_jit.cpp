@@ -95,6 +95,16 @@ const char* g1_name(int code) {
     }
 }
 
+// RX / RY ops in either factored form (A: cos factored out, B: sin)
+bool rotation(int code) {
+    const int b = code & ~3;
+    return b == PC_RX || b == PC_RY || b == PC_RXB || b == PC_RYB;
+}
+bool rot_x(int code) {
+    const int b = code & ~3;
+    return b == PC_RX || b == PC_RXB;
+}
+
 // "(tw & m) == m" or "true"
 std::string tcond(uint32_t tm) {
     if (!tm) return "true";
@@ -255,7 +265,15 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
         const uint32_t c = op.coef;
         const uint32_t cr = op.cond_reg;
         const uint32_t tm = ow[4 * oi + 2];
-        if (code >= PC_HF && code < PC_XC) {
+        if (rotation(code)) {
+            // RX / RY: which of |cos|, |sin| was factored out is a property
+            // of the angle, read from the op at run time, so that the text
+            // (and the compiled kernel) does not depend on angle values
+            const bool x = rot_x(code);
+            E.line("if (P.ops[%u].code >= %d) g1r<%s, %d>(a, %s + %u); else g1r<%s, %d>(a, %s + %u);", oi,
+                   x ? PC_RXB : PC_RYB, x ? "G1_RXB" : "G1_RYB", code & 3, cf, c, x ? "G1_RXA" : "G1_RYA", code & 3,
+                   cf, c);
+        } else if (code >= PC_HF && code < PC_XC) {
             E.line("g1r<%s, %d>(a, %s + %u);", g1_name(code), code & 3, cf, c);
         } else if (code >= PC_RXB && code < PC_DIAG_TA) {
             E.line("g1r<%s, %d>(a, %s + %u);", g1_name(code), code & 3, cf, c);
@@ -424,7 +442,17 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
         const uint32_t cr = op.cond_reg;
         const uint32_t tm = ow[4 * oi + 2];
         const bool g1 = (code >= PC_HF && code < PC_XC) || (code >= PC_RXB && code < PC_DIAG_TA);
-        if (g1) {
+        if (rotation(code)) {
+            const bool x = rot_x(code);
+            const char* fb = x ? "G1_RXB" : "G1_RYB";
+            const char* fa = x ? "G1_RXA" : "G1_RYA";
+            if ((code & 3) == 3)
+                E.line("if (P.ops[%u].code >= %d) g1_bit3<%s>(re, im, scoef + %u); else g1_bit3<%s>(re, im, scoef + %u);",
+                       oi, x ? PC_RXB : PC_RYB, fb, c, fa, c);
+            else
+                E.line("if (P.ops[%u].code >= %d) g1p<%s, %d>(re, im, scoef + %u); else g1p<%s, %d>(re, im, scoef + %u);",
+                       oi, x ? PC_RXB : PC_RYB, fb, code & 3, c, fa, code & 3, c);
+        } else if (g1) {
             if ((code & 3) == 3) E.line("g1_bit3<%s>(re, im, scoef + %u);", g1_name(code), c);
             else E.line("g1p<%s, %d>(re, im, scoef + %u);", g1_name(code), code & 3, c);
         } else if (code >= PC_XC && code < PC_RXB) {
