@@ -175,7 +175,8 @@ def test_batch_generated_arena_kernels(circs, ref, precision):
 
 @pytest.mark.gpu
 def test_batch_graph_recaptured_when_kernels_arrive(circs):
-    big = [c for c in circs if c["n"] >= 11]
+    # each structure repeated ten times: shared enough for the default mode
+    big = [c for c in circs if c["n"] >= 11] * 10
     with qb.Batch("f64") as b:
         b.set_tuning(jit=qb.QOA_JIT_ASYNC, small_max_n=10)
         for c in big:
@@ -185,6 +186,6 @@ def test_batch_graph_recaptured_when_kernels_arrive(circs):
         b.run()
         qb.jit_wait()
         b.launch()          # replays, capturing again with the generated kernels
-        qb_sync = b.results()
+        replay = b.results()
         assert b.jit_info()["graph_uses_generated"]
-    assert np.array_equal(first, qb_sync)
+    assert np.array_equal(first, replay)
