@@ -538,7 +538,8 @@ def run_batch(args):
     out["e2e"] = {"value": count / e2e_s, "unit": "circuits/s",
                   "h2d_bytes_per_step": int(sum(c["ops"].nbytes + 8 * len(c["masks"]) for c in circs)),
                   "d2h_bytes_per_step": int(r.nbytes), "steps": k,
-                  "note": "wall clock: host planning + upload + eager launches + results"}
+                  "note": "wall clock: host planning + upload + eager launches + results; the generated "
+                          "arena kernels of these circuits' pass structures are already in the process cache"}
     if not args.no_cpu:
         from oracle import pyoracle as po
         po.set_fast(False)

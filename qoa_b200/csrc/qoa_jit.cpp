@@ -265,10 +265,11 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
         const uint32_t c = op.coef;
         const uint32_t cr = op.cond_reg;
         const uint32_t tm = ow[4 * oi + 2];
-        if (rotation(code)) {
-            // RX / RY: which of |cos|, |sin| was factored out is a property
-            // of the angle, read from the op at run time, so that the text
-            // (and the compiled kernel) does not depend on angle values
+        if (arena && rotation(code)) {
+            // RX / RY in the batch form: which of |cos|, |sin| was factored
+            // out is a property of the angle, read from the op at run time,
+            // so that circuits differing only in angles share the kernel
+            // (the single-state form keeps the branch out of the code)
             const bool x = rot_x(code);
             E.line("if (P.ops[%u].code >= %d) g1r<%s, %d>(a, %s + %u); else g1r<%s, %d>(a, %s + %u);", oi,
                    x ? PC_RXB : PC_RYB, x ? "G1_RXB" : "G1_RYB", code & 3, cf, c, x ? "G1_RXA" : "G1_RYA", code & 3,
@@ -442,7 +443,7 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
         const uint32_t cr = op.cond_reg;
         const uint32_t tm = ow[4 * oi + 2];
         const bool g1 = (code >= PC_HF && code < PC_XC) || (code >= PC_RXB && code < PC_DIAG_TA);
-        if (rotation(code)) {
+        if (arena && rotation(code)) {
             const bool x = rot_x(code);
             const char* fb = x ? "G1_RXB" : "G1_RYB";
             const char* fa = x ? "G1_RXA" : "G1_RYA";
