@@ -29,6 +29,7 @@
 #include <thread>
 #include <unordered_map>
 #include <algorithm>
+#include <functional>
 
 namespace qoa {
 
@@ -693,7 +694,8 @@ public:
         {
             std::lock_guard<std::mutex> lk(mu_);
             for (const std::string& b : bodies) {
-                auto it = cache_.find(b);
+                const Key key{fnv64(b), std::hash<std::string>()(b)};
+                auto it = cache_.find(key);
                 if (it != cache_.end()) {
                     ++hits_;
                     out.emplace_back(it->second);
@@ -705,15 +707,20 @@ public:
                     // one-off passes (a noisy trajectory's Pauli draws, a
                     // program run once) never pay for a compile
                     if (seen_.size() > (1u << 20)) seen_.clear();
-                    if (++seen_[fnv64(b)] < 2) {
+                    if (++seen_[key.a] < 2) {
                         out.emplace_back();
                         continue;
                     }
                 }
+                if (cache_.size() >= max_kernels_) {
+                    // the cache is full: this structure stays interpreted
+                    out.emplace_back();
+                    continue;
+                }
                 ++misses_;
                 auto e = std::make_shared<JitEntry>();
                 e->name = kernel_name(b);
-                cache_.emplace(b, e);
+                cache_.emplace(key, e);
                 queue_.push_back(JitJob{e, b});
                 ++pending_;
                 queued = true;
@@ -817,7 +824,23 @@ private:
 
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
-    std::unordered_map<std::string, std::shared_ptr<JitEntry>> cache_;
+    // Cache key: two independent 64-bit hashes of the kernel text (the text
+    // itself is dropped once compiled).
+    struct Key {
+        uint64_t a, b;
+        bool operator==(const Key& o) const { return a == o.a && b == o.b; }
+    };
+    struct KeyHash {
+        size_t operator()(const Key& k) const { return (size_t)(k.a ^ (k.b * 0x9e3779b97f4a7c15ull)); }
+    };
+    std::unordered_map<Key, std::shared_ptr<JitEntry>, KeyHash> cache_;
+    // At most this many kernels are loaded per process (QOA_JIT_MAX_KERNELS,
+    // default 8192): beyond it new structures stay on the interpreter.
+    const size_t max_kernels_ = [] {
+        const char* v = getenv("QOA_JIT_MAX_KERNELS");
+        const long k = v ? atol(v) : 0;
+        return k > 0 ? (size_t)k : (size_t)8192;
+    }();
     std::unordered_map<uint64_t, uint32_t> seen_;  // sightings of structures not yet compiled
     std::deque<JitJob> queue_;
     std::vector<std::thread> workers_;
