@@ -385,7 +385,9 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
  *                  their kernel is ready (one-off structures, such as a
  *                  noisy trajectory's Pauli draws, are never compiled)
  *   QOA_JIT_SYNC   compile before the first launch
- * States below min_qubits (default 20) always interpret. */
+ * States below min_qubits (default 20) always interpret. At most 8192
+ * kernels are loaded per process (environment QOA_JIT_MAX_KERNELS); further
+ * structures interpret. */
 #define QOA_JIT_OFF   0
 #define QOA_JIT_ASYNC 1
 #define QOA_JIT_SYNC  2
