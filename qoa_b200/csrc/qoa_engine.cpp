@@ -848,14 +848,16 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         return emit_group(mx, PC_DIAG_MX);
     };
     // lane positions 0..2 carry a quarter-warp: give them tile bits with
-    // distinct residues mod 3 where the lane set allows (bank-conflict-free)
+    // distinct residues mod 3 where the lane set allows (bank-conflict-free).
+    // With a pinned pairing bit the exchanges index the tile without that
+    // bit, so a tile bit above it counts one position lower.
     auto order_lanes = [&](TileMap& t) {
         int best[LANE_BITS];
         for (int i = 0; i < LANE_BITS; ++i) best[i] = t.lane[i];
         int seen[3] = {-1, -1, -1};
         std::vector<int> first, rest;
         for (int i = 0; i < LANE_BITS; ++i) {
-            const int r = best[i] % 3;
+            const int r = (pin >= 0 && best[i] > pin ? best[i] - 1 : best[i]) % 3;
             if (seen[r] < 0) { seen[r] = best[i]; first.push_back(best[i]); }
             else rest.push_back(best[i]);
         }
