@@ -143,25 +143,76 @@ uint32_t reg_part(const TileMap& m, int v) {
 // position t (t < r3) or t - 1 (t > r3) of the 10-bit pair index.
 int pair_pos(int t, int r3) { return t < r3 ? t : t - 1; }
 
-std::string pair_base(const TileMap& m, int r3) {
+// Shared-memory layout of one exchange: index bit t of a 16-byte unit's
+// index keeps its place, except that the low three bits are XORed with A[t]
+// for every set bit t >= 3 (a linear bijection, like spos). A quarter-warp
+// (lanes 0..7) touches 8 units that differ in the index bits of lane bits
+// 0..2; they fall in 8 distinct bank groups when those three bits' low-3
+// images are linearly independent. Each exchange picks its own A so that
+// this holds for the mapping it stores under and the one it loads under.
+struct Swizzle {
+    int nbits = TILE_BITS;
+    uint32_t A[16] = {};
+    uint32_t img(int t) const { return t < 3 ? 1u << t : A[t]; }
+    uint32_t f(uint32_t j) const {
+        uint32_t g = 0;
+        for (int t = 3; t < nbits; ++t)
+            if ((j >> t) & 1) g ^= A[t];
+        return j ^ g;
+    }
+};
+
+bool independent3(uint32_t a, uint32_t b, uint32_t c) {
+    return a && b && c && a != b && c != a && c != b && c != (a ^ b);
+}
+
+// so[i] / sn[i]: index positions of lane bits 0..2 under the store and the
+// load mapping
+Swizzle make_swizzle(const int (&so)[3], const int (&sn)[3], int nbits) {
+    Swizzle z;
+    z.nbits = nbits;
+    for (int t = 3; t < nbits; ++t) z.A[t] = 1u << (t % 3);  // the spos choice
+    std::vector<int> vars;
+    for (int i = 0; i < 3; ++i) {
+        if (so[i] >= 3 && std::find(vars.begin(), vars.end(), so[i]) == vars.end()) vars.push_back(so[i]);
+        if (sn[i] >= 3 && std::find(vars.begin(), vars.end(), sn[i]) == vars.end()) vars.push_back(sn[i]);
+    }
+    auto ok = [&]() {
+        return independent3(z.img(so[0]), z.img(so[1]), z.img(so[2])) &&
+               independent3(z.img(sn[0]), z.img(sn[1]), z.img(sn[2]));
+    };
+    if (ok()) return z;
+    // at most six free images of 7 values each: exhaustive, spos-like first
+    std::function<bool(size_t)> search = [&](size_t k) -> bool {
+        if (k == vars.size()) return ok();
+        const int t = vars[k];
+        const uint32_t first = 1u << (t % 3);
+        for (uint32_t d = 0; d < 7; ++d) {
+            z.A[t] = ((first - 1 + d) % 7) + 1;
+            if (search(k + 1)) return true;
+        }
+        z.A[t] = first;
+        return false;
+    };
+    if (!search(0))
+        for (int t = 3; t < nbits; ++t) z.A[t] = 1u << (t % 3);  // no such layout: keep spos
+    return z;
+}
+
+// f(index of this thread's unit 0) as an XOR of constants selected by the
+// lane and warp bits (pos[t]: index position of tile bit t)
+std::string swz_base(const Swizzle& z, const TileMap& m, const int* pos) {
     std::string e = "0u";
-    char b[96];
+    char b[112];
     for (int i = 0; i < LANE_BITS; ++i) {
-        snprintf(b, sizeof b, " | ((((uint32_t)lane >> %d) & 1u) << %d)", i, pair_pos(m.lane[i], r3));
+        snprintf(b, sizeof b, " ^ ((0u - (((uint32_t)lane >> %d) & 1u)) & 0x%xu)", i, z.f(1u << pos[m.lane[i]]));
         e += b;
     }
     for (int i = 0; i < WARP_BITS; ++i) {
-        snprintf(b, sizeof b, " | ((((uint32_t)wid >> %d) & 1u) << %d)", i, pair_pos(m.warp[i], r3));
+        snprintf(b, sizeof b, " ^ ((0u - (((uint32_t)wid >> %d) & 1u)) & 0x%xu)", i, z.f(1u << pos[m.warp[i]]));
         e += b;
     }
     return e;
-}
-
-uint32_t pair_part(const TileMap& m, int r3, int j) {
-    uint32_t q = 0;
-    for (int k = 0; k < REG_BITS - 1; ++k)
-        if ((j >> k) & 1) q |= 1u << pair_pos(m.reg[k], r3);
-    return spos_host(q);
 }
 
 }  // namespace
@@ -335,12 +386,23 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
                     const TileMap& mo = *cur;
                     const TileMap& mn = P.xmap[c];
                     E.line("__syncthreads();");
-                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mo).c_str());
-                    for (int v = 0; v < REGS; ++v) E.line("tile[pb ^ %uu] = a[%d];", reg_part(mo, v), v);
+                    int pos[TILE_BITS];
+                    for (int t = 0; t < TILE_BITS; ++t) pos[t] = t;
+                    const int so[3] = {mo.lane[0], mo.lane[1], mo.lane[2]};
+                    const int sn[3] = {mn.lane[0], mn.lane[1], mn.lane[2]};
+                    const Swizzle z = make_swizzle(so, sn, TILE_BITS);
+                    auto off = [&](const TileMap& m, int v) {
+                        uint32_t j = 0;
+                        for (int k = 0; k < REG_BITS; ++k)
+                            if ((v >> k) & 1) j |= 1u << m.reg[k];
+                        return z.f(j);
+                    };
+                    E.line("{ const uint32_t pb = %s;", swz_base(z, mo, pos).c_str());
+                    for (int v = 0; v < REGS; ++v) E.line("tile[pb ^ %uu] = a[%d];", off(mo, v), v);
                     E.line("}");
                     E.line("__syncthreads();");
-                    E.line("{ const uint32_t pb = spos(%s);", tile_base(mn).c_str());
-                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[pb ^ %uu];", v, reg_part(mn, v));
+                    E.line("{ const uint32_t pb = %s;", swz_base(z, mn, pos).c_str());
+                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[pb ^ %uu];", v, off(mn, v));
                     E.line("}");
                     cur = &mn;
                     break;
@@ -517,17 +579,28 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
                         // packed pairs (re[j], im[j]) move as 16-byte units,
                         // indexed by the tile index without that bit
                         const int r3 = mo.reg[REG_BITS - 1];
+                        int pos[TILE_BITS];
+                        for (int t = 0; t < TILE_BITS; ++t) pos[t] = pair_pos(t, r3);
+                        const int so[3] = {pos[mo.lane[0]], pos[mo.lane[1]], pos[mo.lane[2]]};
+                        const int sn[3] = {pos[mn.lane[0]], pos[mn.lane[1]], pos[mn.lane[2]]};
+                        const Swizzle z = make_swizzle(so, sn, TILE_BITS - 1);
+                        auto off = [&](const TileMap& m, int j) {
+                            uint32_t q = 0;
+                            for (int k = 0; k < REG_BITS - 1; ++k)
+                                if ((j >> k) & 1) q |= 1u << pos[m.reg[k]];
+                            return z.f(q);
+                        };
                         E.line("__syncthreads();");
-                        E.line("{ ulonglong2* pt = reinterpret_cast<ulonglong2*>(tile); const uint32_t pb = spos(%s);",
-                               pair_base(mo, r3).c_str());
+                        E.line("{ ulonglong2* pt = reinterpret_cast<ulonglong2*>(tile); const uint32_t pb = %s;",
+                               swz_base(z, mo, pos).c_str());
                         for (int j = 0; j < 8; ++j)
-                            E.line("pt[pb ^ %uu] = make_ulonglong2(re[%d], im[%d]);", pair_part(mo, r3, j), j, j);
+                            E.line("pt[pb ^ %uu] = make_ulonglong2(re[%d], im[%d]);", off(mo, j), j, j);
                         E.line("}");
                         E.line("__syncthreads();");
-                        E.line("{ const ulonglong2* pt = reinterpret_cast<const ulonglong2*>(tile); const uint32_t pb = spos(%s);",
-                               pair_base(mn, r3).c_str());
+                        E.line("{ const ulonglong2* pt = reinterpret_cast<const ulonglong2*>(tile); const uint32_t pb = %s;",
+                               swz_base(z, mn, pos).c_str());
                         for (int j = 0; j < 8; ++j)
-                            E.line("{ const ulonglong2 u = pt[pb ^ %uu]; re[%d] = u.x; im[%d] = u.y; }", pair_part(mn, r3, j), j, j);
+                            E.line("{ const ulonglong2 u = pt[pb ^ %uu]; re[%d] = u.x; im[%d] = u.y; }", off(mn, j), j, j);
                         E.line("}");
                         cur = &mn;
                         break;
