@@ -396,12 +396,15 @@ def run_qft(args):
     with qb.QuantumState(n, precision="f32", profile=True) as st:
         st.set_random_state(2)
         ms, passes, bw, avg = timed(st, ops_n, args.steps, args.warmup, 3)
+        generated = st.jit_stats()["launches"] > 0
     peak, src = measured_peaks()
     out.update(value=len(ops_n) / (ms / 1e3), dtype="complex64 (FP32 tile passes, FP64-built coefficients)",
                config={"workload": f"QFT n={n}", "gates": len(ops_n), "state_bytes": 8 << n},
                ms_per_step=ms, fp32_passes=passes,
                roofline={"bound": "hbm", "achieved": bw, "peak": peak, "unit": "GB/s",
-                         "frac": bw / peak if bw else None, "kernel": "k_pass_p32", "avg_launch_ms": avg,
+                         "frac": bw / peak if bw else None,
+                         "kernel": "qoa_jit_pass32_* (generated complex64 tile pass)" if generated
+                         else "k_pass_p32x2 (interpreter)", "avg_launch_ms": avg,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({src})"})
     m = n - 1
     ops_m = C.ops_to_array(C.qft(m))
