@@ -29,6 +29,7 @@
 #include <thread>
 #include <unordered_map>
 #include <algorithm>
+#include <array>
 #include <functional>
 
 namespace qoa {
@@ -199,6 +200,59 @@ Swizzle make_swizzle(const int (&so)[3], const int (&sn)[3], int nbits) {
     return z;
 }
 
+// One layout for every exchange of a pass: each lane triple (index
+// positions of lane bits 0..2 under a mapping the pass stores or loads
+// under) must get independent low-3 images. With one layout, a thread
+// stores each exchange's data exactly where it loaded the previous
+// exchange's, so the barrier that otherwise separates the previous loads
+// from the next stores is not needed. False when no layout is found within
+// a bounded search.
+bool pass_swizzle(const std::vector<std::array<int, 3>>& triples, int nbits, Swizzle& z) {
+    z = Swizzle();
+    z.nbits = nbits;
+    for (int t = 3; t < nbits; ++t) z.A[t] = 1u << (t % 3);
+    int freq[16] = {};
+    for (const auto& tr : triples)
+        for (int p : tr)
+            if (p >= 3) freq[p]++;
+    std::vector<int> vars;
+    for (int t = 3; t < nbits; ++t)
+        if (freq[t]) vars.push_back(t);
+    std::sort(vars.begin(), vars.end(), [&](int a, int b) { return freq[a] > freq[b]; });
+    int rank[16];
+    for (int t = 0; t < 16; ++t) rank[t] = -1;
+    for (size_t k = 0; k < vars.size(); ++k) rank[vars[k]] = (int)k;
+    // a triple is checked once its last variable is assigned
+    std::vector<std::vector<int>> due(vars.size() + 1);
+    for (size_t i = 0; i < triples.size(); ++i) {
+        int last = -1;
+        for (int p : triples[i]) last = std::max(last, p >= 3 ? rank[p] : -1);
+        due[last + 1].push_back((int)i);
+    }
+    auto holds = [&](int i) {
+        const auto& tr = triples[i];
+        return independent3(z.img(tr[0]), z.img(tr[1]), z.img(tr[2]));
+    };
+    for (int i : due[0])
+        if (!holds(i)) return false;
+    long nodes = 0;
+    std::function<bool(size_t)> search = [&](size_t k) -> bool {
+        if (k == vars.size()) return true;
+        if (++nodes > 200000) return false;
+        const int t = vars[k];
+        const uint32_t first = 1u << (t % 3);
+        for (uint32_t d = 0; d < 7; ++d) {
+            z.A[t] = ((first - 1 + d) % 7) + 1;
+            bool good = true;
+            for (int i : due[k + 1]) good = good && holds(i);
+            if (good && search(k + 1)) return true;
+        }
+        z.A[t] = first;
+        return false;
+    };
+    return search(0);
+}
+
 // f(index of this thread's unit 0) as an XOR of constants selected by the
 // lane and warp bits (pos[t]: index position of tile bit t)
 std::string swz_base(const Swizzle& z, const TileMap& m, const int* pos) {
@@ -309,6 +363,25 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
     }
     if (P.nang || arena) E.line("__syncthreads();");
 
+    // one exchange layout for the whole pass where one exists
+    Swizzle zp;
+    bool shared_layout = false;
+    {
+        std::vector<std::array<int, 3>> tr;
+        const TileMap* m = &P.map0;
+        for (uint32_t oi = 0; oi < P.nops; ++oi) {
+            const PassOp& op = P.ops[oi];
+            if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) { oi += op.k; continue; }
+            if (op.code != PC_XCHG) continue;
+            const TileMap& mn = P.xmap[op.coef];
+            tr.push_back({m->lane[0], m->lane[1], m->lane[2]});
+            tr.push_back({mn.lane[0], mn.lane[1], mn.lane[2]});
+            m = &mn;
+        }
+        shared_layout = !tr.empty() && pass_swizzle(tr, TILE_BITS, zp);
+    }
+    int nxchg = 0;
+
     const TileMap* cur = &P.map0;
     const uint32_t* ow = reinterpret_cast<const uint32_t*>(P.ops);
     for (uint32_t oi = 0; oi < P.nops; ++oi) {
@@ -385,12 +458,15 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
                 case PC_XCHG: {
                     const TileMap& mo = *cur;
                     const TileMap& mn = P.xmap[c];
-                    E.line("__syncthreads();");
+                    // with the pass's one layout each thread stores where it
+                    // last loaded: only the first exchange waits before storing
+                    if (!shared_layout || nxchg == 0) E.line("__syncthreads();");
+                    ++nxchg;
                     int pos[TILE_BITS];
                     for (int t = 0; t < TILE_BITS; ++t) pos[t] = t;
                     const int so[3] = {mo.lane[0], mo.lane[1], mo.lane[2]};
                     const int sn[3] = {mn.lane[0], mn.lane[1], mn.lane[2]};
-                    const Swizzle z = make_swizzle(so, sn, TILE_BITS);
+                    const Swizzle z = shared_layout ? zp : make_swizzle(so, sn, TILE_BITS);
                     auto off = [&](const TileMap& m, int v) {
                         uint32_t j = 0;
                         for (int k = 0; k < REG_BITS; ++k)
@@ -497,6 +573,29 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
     }
     E.line("__syncthreads();");
 
+    // one pair-exchange layout for the whole pass, when every exchange keeps
+    // the same pairing bit and one layout serves all of them
+    Swizzle zp;
+    bool shared_layout = false;
+    {
+        std::vector<std::array<int, 3>> tr;
+        const TileMap* m = &P.map0;
+        const int r3 = P.map0.reg[REG_BITS - 1];
+        bool all_pair = true;
+        for (uint32_t oi = 0; oi < P.nops; ++oi) {
+            const PassOp& op = P.ops[oi];
+            if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) { oi += op.k; continue; }
+            if (op.code != PC_XCHG) continue;
+            const TileMap& mn = P.xmap[op.coef];
+            all_pair = all_pair && m->reg[REG_BITS - 1] == r3 && mn.reg[REG_BITS - 1] == r3;
+            tr.push_back({pair_pos(m->lane[0], r3), pair_pos(m->lane[1], r3), pair_pos(m->lane[2], r3)});
+            tr.push_back({pair_pos(mn.lane[0], r3), pair_pos(mn.lane[1], r3), pair_pos(mn.lane[2], r3)});
+            m = &mn;
+        }
+        shared_layout = all_pair && !tr.empty() && pass_swizzle(tr, TILE_BITS - 1, zp);
+    }
+    int nxchg = 0;
+
     const TileMap* cur = &P.map0;
     const uint32_t* ow = reinterpret_cast<const uint32_t*>(P.ops);
     for (uint32_t oi = 0; oi < P.nops; ++oi) {
@@ -583,14 +682,17 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
                         for (int t = 0; t < TILE_BITS; ++t) pos[t] = pair_pos(t, r3);
                         const int so[3] = {pos[mo.lane[0]], pos[mo.lane[1]], pos[mo.lane[2]]};
                         const int sn[3] = {pos[mn.lane[0]], pos[mn.lane[1]], pos[mn.lane[2]]};
-                        const Swizzle z = make_swizzle(so, sn, TILE_BITS - 1);
+                        const Swizzle z = shared_layout ? zp : make_swizzle(so, sn, TILE_BITS - 1);
                         auto off = [&](const TileMap& m, int j) {
                             uint32_t q = 0;
                             for (int k = 0; k < REG_BITS - 1; ++k)
                                 if ((j >> k) & 1) q |= 1u << pos[m.reg[k]];
                             return z.f(q);
                         };
-                        E.line("__syncthreads();");
+                        // with the pass's one layout each thread stores where
+                        // it last loaded: only the first exchange waits first
+                        if (!shared_layout || nxchg == 0) E.line("__syncthreads();");
+                        ++nxchg;
                         E.line("{ ulonglong2* pt = reinterpret_cast<ulonglong2*>(tile); const uint32_t pb = %s;",
                                swz_base(z, mo, pos).c_str());
                         for (int j = 0; j < 8; ++j)
