@@ -1816,6 +1816,7 @@ inline bool shim_bit_ok(size_t b) { return b < 64; }
 // launches over the arena. The first run executes eagerly and captures
 // everything into a CUDA graph; later runs replay it.
 enum BatchRoute { R_SMALL = 0, R_ARENA = 1, R_VIEW = 2 };
+constexpr int kRoundStreams = 4;  // extra streams of a round's generated launches
 
 struct qoa_batch_s {
     int precision = QOA_PREC_F64;
@@ -1853,10 +1854,14 @@ struct qoa_batch_s {
     uint32_t* d_tstart = nullptr;
     // one launch of a generated arena kernel: njobs jobs of one structure
     // from job_off, 2^lt tiles each
-    struct Group { uint32_t job_off, njobs, lt; int kernel; };
+    struct Group { uint32_t job_off, njobs, lt; int kernel; int stream; };
     struct Round { uint32_t job_off, njobs, tiles; int max_nops, max_ncoef; std::vector<Group> groups; };
     std::vector<Round> rounds;
     std::vector<JitKernel> jit_kernels;  // by structure
+    // a round's generated launches spread over stream 0 and these
+    // (small groups would leave most SMs idle one after another)
+    std::vector<cudaStream_t> rstreams;
+    std::vector<cudaEvent_t> revents;    // [0] fork, [1 + i] join of rstreams[i]
     bool graph_jit = false;              // the captured graph launches the generated kernels
     double arena_pass_bytes = 0;   // algorithmic bytes of one run's arena passes
     uint32_t narena = 0;
@@ -2202,7 +2207,7 @@ int batch_prepare(qoa_batch_t b) {
             const uint32_t pi = pass_idx[i][r];
             if (jit) {
                 if (R.groups.empty() || R.groups.back().kernel != shape_of[pi])
-                    R.groups.push_back({(uint32_t)jobs.size(), 0, c.n - (uint32_t)TILE_BITS, shape_of[pi]});
+                    R.groups.push_back({(uint32_t)jobs.size(), 0, c.n - (uint32_t)TILE_BITS, shape_of[pi], 0});
                 R.groups.back().njobs++;
             }
             ArenaJob J;
@@ -2218,6 +2223,21 @@ int batch_prepare(qoa_batch_t b) {
             if (!tensor) {
                 R.max_nops = std::max(R.max_nops, (int)p64[pi].nops);
                 R.max_ncoef = std::max(R.max_ncoef, (int)p64[pi].ncoef);
+            }
+        }
+        if (R.groups.size() > 1) {
+            // longest-processing-time-first over 1 + kRoundStreams streams
+            std::vector<size_t> idx(R.groups.size());
+            for (size_t g = 0; g < idx.size(); ++g) idx[g] = g;
+            auto work = [&](size_t g) { return (double)R.groups[g].njobs * std::ldexp(1.0, (int)R.groups[g].lt); };
+            std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return work(x) > work(y); });
+            double load[1 + kRoundStreams] = {};
+            for (size_t g : idx) {
+                int best = 0;
+                for (int k = 1; k <= kRoundStreams; ++k)
+                    if (load[k] < load[best]) best = k;
+                R.groups[g].stream = best;
+                load[best] += work(g);
             }
         }
         b->rounds.push_back(R);
@@ -2255,6 +2275,19 @@ int batch_prepare(qoa_batch_t b) {
     if (!ej.empty()) {
         if ((rc = upload(b, b->d_ejobs, ej))) return rc;
         BCK(cudaMalloc(&b->d_epart, parts * sizeof(double)));
+    }
+
+    if (jit && b->rstreams.empty()) {
+        cudaEvent_t ev;
+        BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->revents.push_back(ev);
+        for (int k = 0; k < kRoundStreams; ++k) {
+            cudaStream_t st;
+            BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            b->rstreams.push_back(st);
+            BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            b->revents.push_back(ev);
+        }
     }
 
     // streams
@@ -2329,8 +2362,20 @@ int batch_enqueue(qoa_batch_t b) {
     for (const auto& k : b->jit_kernels) all_ready = all_ready && k.ready();
     for (const auto& R : b->rounds) {
         if (all_ready && !R.groups.empty()) {
-            for (const auto& Gp : R.groups)
-                BCK(b->jit_kernels[Gp.kernel].launch_arena(b->d_jobs + Gp.job_off, Gp.njobs, Gp.lt, s0));
+            const bool fork = R.groups.size() > 1 && !b->rstreams.empty();
+            if (fork) {
+                BCK(cudaEventRecord(b->revents[0], s0));
+                for (cudaStream_t st : b->rstreams) BCK(cudaStreamWaitEvent(st, b->revents[0], 0));
+            }
+            for (const auto& Gp : R.groups) {
+                cudaStream_t st = (fork && Gp.stream > 0) ? b->rstreams[Gp.stream - 1] : s0;
+                BCK(b->jit_kernels[Gp.kernel].launch_arena(b->d_jobs + Gp.job_off, Gp.njobs, Gp.lt, st));
+            }
+            if (fork)
+                for (size_t k = 0; k < b->rstreams.size(); ++k) {
+                    BCK(cudaEventRecord(b->revents[1 + k], b->rstreams[k]));
+                    BCK(cudaStreamWaitEvent(s0, b->revents[1 + k], 0));
+                }
             continue;
         }
         if (tensor)
@@ -2841,6 +2886,7 @@ int qoa_batch_set_tuning(qoa_batch_t b, const qoa_batch_tuning* t) {
     if (b->prepared) {
         cudaSetDevice(b->device);
         for (cudaStream_t st : b->streams) cudaStreamSynchronize(st);
+        for (cudaStream_t st : b->rstreams) cudaStreamSynchronize(st);
         batch_free_device(b);
     }
     b->tune = *t;
@@ -3160,9 +3206,12 @@ int qoa_batch_destroy(qoa_batch_t b) {
     if (!b) return QOA_OK;
     cudaSetDevice(b->device);
     for (cudaStream_t st : b->streams) cudaStreamSynchronize(st);
+    for (cudaStream_t st : b->rstreams) cudaStreamSynchronize(st);
     batch_free_device(b);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
     for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
+    for (cudaEvent_t e : b->revents) cudaEventDestroy(e);
+    for (cudaStream_t st : b->rstreams) cudaStreamDestroy(st);
     delete b;
     return QOA_OK;
 }
