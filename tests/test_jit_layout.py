@@ -1,0 +1,80 @@
+"""Shared-memory exchanges of the generated pass kernels, checked on the
+host from the generated source (no GPU): every exchange's layout is a
+bijection onto the tile's 16-byte units, a quarter-warp's accesses fall in
+eight distinct bank groups, and where an exchange skips the barrier before
+its stores, every thread stores exactly the units it loaded in the previous
+exchange (so no thread overwrites data another thread has yet to load)."""
+import re
+
+import pytest
+
+import qoa_b200 as qb
+from qoa_b200 import circuits as C
+from tests.test_plan import mixed_circuit
+
+TERM = re.compile(r"\(\(0u - \(\(\(uint32_t\)(lane|wid) >> (\d)\) & 1u\)\) & 0x([0-9a-f]+)u\)")
+
+
+def exchanges(kernel, precision):
+    """[(barrier_before_store, store_units[thread][k], load_units[thread][k])]"""
+    if precision == "f64":
+        pat = re.compile(r"(__syncthreads\(\);\n)?\{ const uint32_t pb = (0u[^;]*);\n((?:tile\[pb \^ \d+u\] = a\[\d+\];\n){16})\}\n"
+                         r"__syncthreads\(\);\n\{ const uint32_t pb = (0u[^;]*);\n((?:a\[\d+\] = tile\[pb \^ \d+u\];\n){16})")
+    else:
+        pat = re.compile(r"(__syncthreads\(\);\n)?\{ ulonglong2\* pt = reinterpret_cast<ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
+                         r"((?:pt\[pb \^ \d+u\] = .*\n){8})\}\n__syncthreads\(\);\n"
+                         r"\{ const ulonglong2\* pt = reinterpret_cast<const ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
+                         r"((?:\{ const ulonglong2 u = pt\[pb \^ \d+u\].*\n){8})")
+    out = []
+    for m in pat.finditer(kernel):
+        def units(expr, body):
+            terms = [(w, int(i), int(c, 16)) for w, i, c in TERM.findall(expr)]
+            assert len(terms) == 7
+            offs = [int(x) for x in re.findall(r"pb \^ (\d+)u", body)]
+            res = []
+            for t in range(128):
+                lane, wid = t & 31, t >> 5
+                base = 0
+                for w, i, c in terms:
+                    if ((lane if w == "lane" else wid) >> i) & 1:
+                        base ^= c
+                res.append([base ^ o for o in offs])
+            return res
+        out.append((m.group(1) is not None, units(m.group(2), m.group(3)), units(m.group(4), m.group(5))))
+    return out
+
+
+CASES = [
+    ("layered", 20, lambda: C.random_layered(20, 6, 3, initial_h=True), 1),
+    ("qft", 20, lambda: C.qft(20), 0),
+    ("mixed", 16, lambda: mixed_circuit(16, 200, 8), 0),
+]
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("name,n,make,flags", CASES, ids=[c[0] for c in CASES])
+def test_generated_exchanges(name, n, make, flags, precision):
+    src, npasses = qb.jit_translate(n, make(), flags=flags, precision=precision)
+    kernels = src.split('extern "C"')[1:]
+    assert len(kernels) == npasses
+    nunits = 2048 if precision == "f64" else 1024
+    seen = 0
+    for k in kernels:
+        xs = exchanges(k, precision)
+        # every exchange of the kernel was recognised
+        assert len(xs) == (k.count("tile[pb ^") // 32 if precision == "f64" else k.count("make_ulonglong2") // 8)
+        prev_load = None
+        for i, (barrier, st, ld) in enumerate(xs):
+            for side in (st, ld):
+                flat = [u for t in side for u in t]
+                assert sorted(flat) == list(range(nunits)), "layout is not a bijection"
+                for t0 in range(0, 128, 8):   # quarter-warps: 8 distinct bank groups per access
+                    for j in range(len(side[0])):
+                        assert len({side[t][j] % 8 for t in range(t0, t0 + 8)}) == 8
+            if not barrier:
+                assert i > 0 and prev_load is not None
+                for t in range(128):
+                    assert sorted(st[t]) == sorted(prev_load[t]), "store without barrier touches other units"
+            prev_load = ld
+            seen += 1
+    assert seen > 0
