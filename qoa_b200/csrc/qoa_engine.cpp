@@ -553,8 +553,8 @@ uint64_t tile_need(const Gate& g, bool f32) {
     return g.kind == K_DIAG ? 0 : (g.nmask | g.dmask);
 }
 
-std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false,
-                           int gate_budget = 0) {
+std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32,
+                                      int gate_budget, bool slot_search) {
     std::vector<Step> steps;
     const size_t N = G.size();
     std::vector<char> done(N, 0);
@@ -573,39 +573,78 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
         }
         Step st;
         st.pass = true;
-        uint64_t tile = 0x1Full;  // lane qubits
-        int nslots = 0;
-        uint64_t bN = 0, bD = 0;  // qubits blocked by waiting gates (non-diagonal / diagonal action)
-        int budget_ops = MAX_PASS_OPS / 3;  // room for the exchanges and flushes
-        if (gate_budget > 0 && gate_budget < budget_ops) budget_ops = gate_budget;
-        int budget_coef = MAX_PASS_COEF - 8;
-        for (size_t i = first; i < N; ++i) {
-            if (done[i]) continue;
-            const Gate& g = G[i];
-            if (is_barrier(g)) break;
-            bool ok = (f32 ? is_pass_gate_f32(g) : is_pass_gate(g)) && !(g.nmask & (bN | bD)) && !(g.dmask & bN);
-            if (ok) {
-                const uint64_t need = tile_need(g, f32) & ~tile;
-                const int k = __builtin_popcountll(need);
-                const int nc = g.kind == K_G1 ? 4 : 2;  // a selector diagonal becomes two phase ops
-                if (nslots + k > HIGH_SLOTS || budget_ops < 1 || budget_coef < nc) ok = false;
-                else {
-                    tile |= need;
-                    nslots += k;
-                    budget_ops -= 1;
-                    budget_coef -= nc;
+        // Gates of the pass from `first` on, in order, each joining when its
+        // qubits are not blocked by a waiting gate and its non-diagonal
+        // qubits are in the tile (claiming free high slots as needed, unless
+        // the tile is given whole). Returns the tile.
+        auto fill = [&](uint64_t tile, int nslots, std::vector<int>& out) -> uint64_t {
+            uint64_t bN = 0, bD = 0;  // qubits blocked by waiting gates (non-diagonal / diagonal action)
+            int budget_ops = MAX_PASS_OPS / 3;  // room for the exchanges and flushes
+            if (gate_budget > 0 && gate_budget < budget_ops) budget_ops = gate_budget;
+            int budget_coef = MAX_PASS_COEF - 8;
+            for (size_t i = first; i < N; ++i) {
+                if (done[i]) continue;
+                const Gate& g = G[i];
+                if (is_barrier(g)) break;
+                bool ok = (f32 ? is_pass_gate_f32(g) : is_pass_gate(g)) && !(g.nmask & (bN | bD)) && !(g.dmask & bN);
+                if (ok) {
+                    const uint64_t need = tile_need(g, f32) & ~tile;
+                    const int k = __builtin_popcountll(need);
+                    const int nc = g.kind == K_G1 ? 4 : 2;  // a selector diagonal becomes two phase ops
+                    if (nslots + k > HIGH_SLOTS || budget_ops < 1 || budget_coef < nc) ok = false;
+                    else {
+                        tile |= need;
+                        nslots += k;
+                        budget_ops -= 1;
+                        budget_coef -= nc;
+                    }
+                }
+                if (ok) {
+                    out.push_back((int)i);
+                } else {
+                    bN |= g.nmask;
+                    bD |= g.dmask;
+                    const uint64_t full = (n >= 64) ? ~0ull : ((1ull << n) - 1);
+                    if ((bN & full) == full) break;  // every qubit blocked: nothing else can join
                 }
             }
-            if (ok) {
-                st.gates.push_back((int)i);
-                done[i] = 1;
-            } else {
-                bN |= g.nmask;
-                bD |= g.dmask;
-                const uint64_t full = (n >= 64) ? ~0ull : ((1ull << n) - 1);
-                if ((bN & full) == full) break;  // every qubit blocked: nothing else can join
+            return tile;
+        };
+        uint64_t tile = fill(0x1Full, 0, st.gates);
+        // Slot search: the greedy claims slots for the first gates that need
+        // them; swapping one slot qubit for another, with the tile then
+        // fixed, often admits more gates. Hill-climb while it does.
+        if (slot_search && n > (uint32_t)TILE_BITS && __builtin_popcountll(tile) == TILE_BITS) {
+            std::vector<int> best_gates = st.gates, trial;
+            uint64_t best_tile = tile;
+            for (int round = 0; round < 4; ++round) {
+                bool improved = false;
+                uint64_t cand_tile = best_tile;
+                std::vector<int> cand_gates;
+                for (uint32_t a = LANE_BITS; a < n; ++a) {
+                    if (!((best_tile >> a) & 1)) continue;
+                    for (uint32_t q = LANE_BITS; q < n; ++q) {
+                        if ((best_tile >> q) & 1) continue;
+                        const uint64_t t2 = (best_tile & ~(1ull << a)) | (1ull << q);
+                        trial.clear();
+                        fill(t2, HIGH_SLOTS, trial);
+                        if (trial.size() > std::max(best_gates.size(), cand_gates.size())) {
+                            cand_gates = trial;
+                            cand_tile = t2;
+                        }
+                    }
+                }
+                if (cand_gates.size() > best_gates.size()) {
+                    best_gates = cand_gates;
+                    best_tile = cand_tile;
+                    improved = true;
+                }
+                if (!improved) break;
             }
+            st.gates = best_gates;
+            tile = best_tile;
         }
+        for (int gi : st.gates) done[gi] = 1;
         // the tile's high slots: claimed qubits, padded with unused ones >= 5
         for (uint32_t q = LANE_BITS; q < n; ++q)
             if ((tile >> q) & 1) st.slots.push_back((int)q);
@@ -614,6 +653,21 @@ std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate
         steps.push_back(st);
     }
     return steps;
+}
+
+// The pass plan of a gate list: the in-order greedy, and the same with the
+// slot search; the one with fewer steps (the search is per pass, so on some
+// circuits it loses overall). QOA_SCHED_SEARCH=0 keeps the greedy alone.
+std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false,
+                           int gate_budget = 0) {
+    static const bool search = [] {
+        const char* v = getenv("QOA_SCHED_SEARCH");
+        return !(v && v[0] == '0');
+    }();
+    std::vector<Step> a = schedule_pass_order(G, n, per_gate, f32, gate_budget, false);
+    if (!search || per_gate || n <= (uint32_t)TILE_BITS || a.size() < 2) return a;
+    std::vector<Step> b = schedule_pass_order(G, n, per_gate, f32, gate_budget, true);
+    return b.size() < a.size() ? b : a;
 }
 
 // Builds the kernel op stream of a pass. The tile's TILE_BITS index bits
