@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <memory>
+#include <deque>
 #include <thread>
 #include <functional>
 #include <atomic>
@@ -196,6 +198,7 @@ struct qoa_state_s {
     double noise_p = 0.0;
     uint64_t launches = 0;
     uint32_t host_resets = 0;     // normalize() resets decided on the host
+    std::shared_ptr<void> plans;    // PlanCache: plans of repeated op lists
     int jit_mode = QOA_JIT_ASYNC;   // generated complex128 pass kernels (qoa_jit.cpp)
     uint32_t jit_min_qubits = 20;   // smaller states interpret their passes
     uint64_t jit_launches = 0;
@@ -540,6 +543,51 @@ struct Step {
     std::vector<int> slots;        // pass: high qubits of the tile (HIGH_SLOTS)
 };
 
+// Plans of repeated op lists (per state): a list seen for the second time
+// keeps its schedule, its built pass parameters and its generated kernel
+// texts, so that a circuit executed again (benchmark steps, shot or
+// trajectory loops, a VM loop body) skips the host planning. Keyed by two
+// independent hashes of every gate field the plan depends on.
+struct PlanEntry {
+    uint64_t h1 = 0, h2 = 0;
+    std::vector<Step> steps;
+    bool prebuilt = false;
+    std::vector<PassParams> built;
+    std::vector<int> built_of;
+    std::vector<std::string> bodies;
+};
+struct PlanCache {
+    static constexpr size_t kEntries = 8;
+    std::deque<PlanEntry> entries;                 // most recent last
+    std::unordered_map<uint64_t, uint8_t> seen;    // op lists seen once
+};
+
+void plan_hash(const std::vector<Gate>& G, uint64_t key, uint64_t& h1, uint64_t& h2) {
+    h1 = 1469598103934665603ull ^ key;
+    h2 = 0x9e3779b97f4a7c15ull ^ (key * 0xff51afd7ed558ccdull);
+    auto mix = [&](const void* p, size_t nb) {
+        const unsigned char* c = (const unsigned char*)p;
+        for (size_t i = 0; i < nb; ++i) {
+            h1 = (h1 ^ c[i]) * 1099511628211ull;
+            h2 = (h2 ^ c[i]) * 0x100000001b3ull + (h2 >> 29);
+        }
+    };
+    for (const Gate& g : G) {
+        mix(&g.kind, sizeof g.kind);
+        mix(&g.sub, sizeof g.sub);
+        mix(&g.t, sizeof g.t);
+        mix(&g.t2, sizeof g.t2);
+        mix(&g.cmask, sizeof g.cmask);
+        const uint8_t neg = g.neg;
+        mix(&neg, 1);
+        mix(g.m, sizeof g.m);
+        mix(&g.nmask, sizeof g.nmask);
+        mix(&g.dmask, sizeof g.dmask);
+        mix(&g.u, sizeof g.u);
+        if (g.kind == K_PERM) mix(g.pi, sizeof g.pi);
+    }
+}
+
 // Greedy list scheduling. Gate g may run in the current pass when every
 // earlier gate still waiting commutes with it: for each shared qubit both act
 // diagonally (controls, phases). Non-diagonal targets must be in the tile:
@@ -553,8 +601,11 @@ uint64_t tile_need(const Gate& g, bool f32) {
     return g.kind == K_DIAG ? 0 : (g.nmask | g.dmask);
 }
 
+// slot_weight 0: in-order greedy only; w > 0: slot search scoring a
+// diagonal gate 1 and any other gate w.
 std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32,
-                                      int gate_budget, bool slot_search) {
+                                      int gate_budget, int slot_weight) {
+    const bool slot_search = slot_weight > 0;
     std::vector<Step> steps;
     const size_t N = G.size();
     std::vector<char> done(N, 0);
@@ -615,9 +666,14 @@ std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bo
         // them; swapping one slot qubit for another, with the tile then
         // fixed, often admits more gates. Hill-climb while it does.
         if (slot_search && n > (uint32_t)TILE_BITS && __builtin_popcountll(tile) == TILE_BITS) {
+            auto score = [&](const std::vector<int>& v) {
+                long sc = 0;
+                for (int gi : v) sc += G[gi].kind == K_DIAG ? 1 : slot_weight;
+                return sc;
+            };
             std::vector<int> best_gates = st.gates, trial;
             uint64_t best_tile = tile;
-            for (int round = 0; round < 4; ++round) {
+            for (int round = 0; round < 6; ++round) {
                 bool improved = false;
                 uint64_t cand_tile = best_tile;
                 std::vector<int> cand_gates;
@@ -628,13 +684,13 @@ std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bo
                         const uint64_t t2 = (best_tile & ~(1ull << a)) | (1ull << q);
                         trial.clear();
                         fill(t2, HIGH_SLOTS, trial);
-                        if (trial.size() > std::max(best_gates.size(), cand_gates.size())) {
+                        if (score(trial) > std::max(score(best_gates), score(cand_gates))) {
                             cand_gates = trial;
                             cand_tile = t2;
                         }
                     }
                 }
-                if (cand_gates.size() > best_gates.size()) {
+                if (score(cand_gates) > score(best_gates)) {
                     best_gates = cand_gates;
                     best_tile = cand_tile;
                     improved = true;
@@ -656,18 +712,22 @@ std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bo
 }
 
 // The pass plan of a gate list: the in-order greedy, and the same with the
-// slot search; the one with fewer steps (the search is per pass, so on some
-// circuits it loses overall). QOA_SCHED_SEARCH=0 keeps the greedy alone.
+// slot search scoring all gates alike or non-diagonal ones double; the one
+// with the fewest steps (the search is per pass, so any of them can win
+// overall). QOA_SCHED_SEARCH=0 keeps the greedy alone.
 std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false,
                            int gate_budget = 0) {
     static const bool search = [] {
         const char* v = getenv("QOA_SCHED_SEARCH");
         return !(v && v[0] == '0');
     }();
-    std::vector<Step> a = schedule_pass_order(G, n, per_gate, f32, gate_budget, false);
-    if (!search || per_gate || n <= (uint32_t)TILE_BITS || a.size() < 2) return a;
-    std::vector<Step> b = schedule_pass_order(G, n, per_gate, f32, gate_budget, true);
-    return b.size() < a.size() ? b : a;
+    std::vector<Step> best = schedule_pass_order(G, n, per_gate, f32, gate_budget, 0);
+    if (!search || per_gate || n <= (uint32_t)TILE_BITS || best.size() < 2) return best;
+    for (int w : {1, 2}) {
+        std::vector<Step> t = schedule_pass_order(G, n, per_gate, f32, gate_budget, w);
+        if (t.size() < best.size()) best.swap(t);
+    }
+    return best;
 }
 
 // Builds the kernel op stream of a pass. The tile's TILE_BITS index bits
@@ -1728,26 +1788,56 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         while (j < G.size() && G[j].kind != K_QINIT) ++j;
         std::vector<Gate> seg(G.begin() + i, G.begin() + j);
         if (!per_gate) merge_swap_blocks(seg);
-        std::vector<Step> steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
-        // tile passes of a large state: built ahead, and their generated
-        // kernels requested from the compile cache
-        std::vector<PassParams> built;
-        std::vector<int> built_of(steps.size(), -1);
-        std::vector<JitKernel> jk;
-        if (!per_gate && s->jit_mode != QOA_JIT_OFF && s->n >= s->jit_min_qubits) {
-            size_t np = 0;
-            for (const Step& st : steps) np += st.pass ? 1 : 0;
-            built.resize(np);
-            std::vector<std::string> bodies;
-            size_t b = 0;
-            for (size_t k = 0; k < steps.size(); ++k) {
-                if (!steps[k].pass || build_pass(seg, steps[k], s->n, built[b], c64) != 0) continue;
-                built_of[k] = (int)b;
-                bodies.push_back(c64 ? jit_pass32_body(built[b]) : jit_pass_body(built[b]));
-                ++b;
+        const bool prebuild = !per_gate && s->jit_mode != QOA_JIT_OFF && s->n >= s->jit_min_qubits;
+        // a repeated op list reuses its plan
+        PlanEntry local;
+        PlanEntry* pe = &local;
+        bool cache_it = false;
+        if (!per_gate && s->n > (uint32_t)TILE_BITS) {
+            if (!s->plans) s->plans = std::make_shared<PlanCache>();
+            PlanCache& pc = *static_cast<PlanCache*>(s->plans.get());
+            const uint64_t key = (uint64_t)s->n | ((uint64_t)c64 << 8) | ((uint64_t)prebuild << 9) |
+                                 ((uint64_t)(uint32_t)s->pass_budget << 16);
+            plan_hash(seg, key, local.h1, local.h2);
+            for (auto& e : pc.entries)
+                if (e.h1 == local.h1 && e.h2 == local.h2) pe = &e;
+            if (pe == &local) {
+                if (pc.seen.size() > 4096) pc.seen.clear();
+                cache_it = pc.seen[local.h1]++ > 0;
             }
-            jk = jit_request(bodies, s->jit_mode == QOA_JIT_SYNC ? JitWhen::WAIT : JitWhen::SECOND_SIGHTING);
         }
+        const bool fresh = pe == &local;
+        if (fresh) {
+            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
+            pe->built_of.assign(pe->steps.size(), -1);
+            // tile passes of a large state: built ahead, and their generated
+            // kernels requested from the compile cache
+            if (prebuild) {
+                size_t np = 0;
+                for (const Step& st : pe->steps) np += st.pass ? 1 : 0;
+                pe->built.resize(np);
+                size_t b = 0;
+                for (size_t k = 0; k < pe->steps.size(); ++k) {
+                    if (!pe->steps[k].pass || build_pass(seg, pe->steps[k], s->n, pe->built[b], c64) != 0) continue;
+                    pe->built_of[k] = (int)b;
+                    pe->bodies.push_back(c64 ? jit_pass32_body(pe->built[b]) : jit_pass_body(pe->built[b]));
+                    ++b;
+                }
+                pe->prebuilt = true;
+            }
+            if (cache_it) {
+                PlanCache& pc = *static_cast<PlanCache*>(s->plans.get());
+                if (pc.entries.size() >= PlanCache::kEntries) pc.entries.pop_front();
+                pc.entries.push_back(std::move(local));
+                pe = &pc.entries.back();
+            }
+        }
+        const std::vector<Step>& steps = pe->steps;
+        const std::vector<PassParams>& built = pe->built;
+        const std::vector<int>& built_of = pe->built_of;
+        std::vector<JitKernel> jk;
+        if (pe->prebuilt)
+            jk = jit_request(pe->bodies, s->jit_mode == QOA_JIT_SYNC ? JitWhen::WAIT : JitWhen::SECOND_SIGHTING);
         for (size_t k = 0; k < steps.size(); ++k) {
             const Step& st = steps[k];
             int rc;
