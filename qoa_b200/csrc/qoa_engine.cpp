@@ -711,18 +711,24 @@ std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bo
     return steps;
 }
 
-// The pass plan of a gate list: the in-order greedy, and the same with the
-// slot search scoring all gates alike or non-diagonal ones double; the one
-// with the fewest steps (the search is per pass, so any of them can win
-// overall). QOA_SCHED_SEARCH=0 keeps the greedy alone.
+// The pass plan of a gate list: the in-order greedy, and (when `search`)
+// the same with the slot search scoring all gates alike or non-diagonal
+// ones double; the one with the fewest steps (the search is per pass, so
+// any of them can win overall). The search costs ~5x the host time of the
+// greedy (~25 us per gate at 28 qubits) and saves about a quarter of the
+// passes, which pays for itself from ~26 qubits on (a pass over 2^26
+// complex128 amplitudes takes ~0.5 ms) or when the plan is kept for reuse.
+// QOA_SCHED_SEARCH=0 keeps the greedy alone.
+bool slot_search_pays(uint32_t n) { return n >= 26; }
+
 std::vector<Step> schedule(const std::vector<Gate>& G, uint32_t n, bool per_gate, bool f32 = false,
-                           int gate_budget = 0) {
-    static const bool search = [] {
+                           int gate_budget = 0, bool search_wanted = false) {
+    static const bool search_on = [] {
         const char* v = getenv("QOA_SCHED_SEARCH");
         return !(v && v[0] == '0');
     }();
     std::vector<Step> best = schedule_pass_order(G, n, per_gate, f32, gate_budget, 0);
-    if (!search || per_gate || n <= (uint32_t)TILE_BITS || best.size() < 2) return best;
+    if (!search_wanted || !search_on || per_gate || n <= (uint32_t)TILE_BITS || best.size() < 2) return best;
     for (int w : {1, 2}) {
         std::vector<Step> t = schedule_pass_order(G, n, per_gate, f32, gate_budget, w);
         if (t.size() < best.size()) best.swap(t);
@@ -1808,7 +1814,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         }
         const bool fresh = pe == &local;
         if (fresh) {
-            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget);
+            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget, cache_it || slot_search_pays(s->n));
             pe->built_of.assign(pe->steps.size(), -1);
             // tile passes of a large state: built ahead, and their generated
             // kernels requested from the compile cache
@@ -2923,7 +2929,7 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
     const std::vector<Gate>& G = ex.out;
     for (const Gate& g : G)
         if (g.kind == K_QINIT) return set_err(nullptr, QOA_E_ARG, "qoa_plan does not take QINIT");
-    std::vector<Step> steps = schedule(G, ex.n, (flags & QOA_FLAG_PER_GATE) != 0);
+    std::vector<Step> steps = schedule(G, ex.n, (flags & QOA_FLAG_PER_GATE) != 0, false, 0, slot_search_pays(ex.n));
     *ngates = G.size();
     *npasses = steps.size();
     if (G.size() > cap) return set_err(nullptr, QOA_E_ARG, "cap too small: %zu gates", G.size());
@@ -3319,7 +3325,7 @@ int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* o
     for (const Gate& g : G)
         if (g.kind == K_QINIT) return set_err(nullptr, QOA_E_ARG, "qoa_jit_translate does not take QINIT");
     merge_swap_blocks(G);
-    std::vector<Step> steps = schedule(G, n, false);
+    std::vector<Step> steps = schedule(G, n, false, false, 0, slot_search_pays(n));
     std::vector<std::string> bodies;
     static thread_local PassParams P;
     for (const Step& st : steps) {
