@@ -134,3 +134,28 @@ def test_generated_complex64_passes_match_interpreter(name, n, quirk, make):
     assert np.array_equal(got_jit.view(np.float32), got_int.view(np.float32)), "generated != interpreter"
     ref = oracle_run(n, ops, 1 if quirk else 0)
     assert rel_l2(got_jit.astype(np.complex128), ref) < 1e-5
+
+
+@pytest.mark.gpu
+def test_repeated_op_lists_reuse_their_plans():
+    """An op list executed again reuses its kept plan (schedule, built passes,
+    kernel texts); results stay bit-identical across repeats and another
+    list in between does not disturb them."""
+    n = 26   # the slot search runs from the first sighting at this size
+    a_ops = C.ops_to_array(C.random_layered(n, 3, 61, initial_h=True))
+    b_ops = C.ops_to_array(C.qft(n))
+    outs = []
+    with qb.QuantumState(n, compat_mask_quirk=True) as st:
+        for k in range(4):
+            st.apply_reset_all()
+            st.execute(a_ops)
+            outs.append(st.get_state_vector())
+            if k == 1:
+                st.apply_reset_all()
+                st.execute(b_ops)
+            if k == 2:
+                qb.jit_wait()
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.float64), outs[0].view(np.float64))
+    ref = oracle_run(n, C.random_layered(n, 3, 61, initial_h=True), 1)
+    assert rel_l2(outs[0], ref) < TOL
