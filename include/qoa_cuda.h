@@ -365,6 +365,9 @@ int qoa_get_precision(qoa_state_t s, int* precision);
  * each expanded gate in submission order, the index of the pass that applies
  * it (pass_of[i]) and the order within the pass (order[i]); *npasses receives
  * the pass count and *ngates the expanded gate count (<= cap). */
+/* Plans with the scheduler's slot search at any size (states of 26 or more
+ * qubits always plan with it); for tests of the plans. */
+#define QOA_PLAN_SLOT_SEARCH 0x100u
 int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t cap,
              int32_t* pass_of, int32_t* order, int32_t* gate_kind, uint32_t* gate_qubits,
              double* gate_matrix, size_t* ngates, size_t* npasses);

@@ -717,7 +717,7 @@ std::vector<Step> schedule_pass_order(const std::vector<Gate>& G, uint32_t n, bo
 // any of them can win overall). The search costs ~5x the host time of the
 // greedy (~25 us per gate at 28 qubits) and saves about a quarter of the
 // passes, which pays for itself from ~26 qubits on (a pass over 2^26
-// complex128 amplitudes takes ~0.5 ms) or when the plan is kept for reuse.
+// complex128 amplitudes takes ~0.5 ms).
 // QOA_SCHED_SEARCH=0 keeps the greedy alone.
 bool slot_search_pays(uint32_t n) { return n >= 26; }
 
@@ -1814,7 +1814,9 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         }
         const bool fresh = pe == &local;
         if (fresh) {
-            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget, cache_it || slot_search_pays(s->n));
+            // the plan depends on the op list and the size only, so a list
+            // executed again gives bit-identical results
+            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget, slot_search_pays(s->n));
             pe->built_of.assign(pe->steps.size(), -1);
             // tile passes of a large state: built ahead, and their generated
             // kernels requested from the compile cache
@@ -2929,7 +2931,8 @@ int qoa_plan(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, size_t 
     const std::vector<Gate>& G = ex.out;
     for (const Gate& g : G)
         if (g.kind == K_QINIT) return set_err(nullptr, QOA_E_ARG, "qoa_plan does not take QINIT");
-    std::vector<Step> steps = schedule(G, ex.n, (flags & QOA_FLAG_PER_GATE) != 0, false, 0, slot_search_pays(ex.n));
+    std::vector<Step> steps = schedule(G, ex.n, (flags & QOA_FLAG_PER_GATE) != 0, false, 0,
+                                       slot_search_pays(ex.n) || (flags & QOA_PLAN_SLOT_SEARCH));
     *ngates = G.size();
     *npasses = steps.size();
     if (G.size() > cap) return set_err(nullptr, QOA_E_ARG, "cap too small: %zu gates", G.size());

@@ -141,7 +141,7 @@ def test_repeated_op_lists_reuse_their_plans():
     """An op list executed again reuses its kept plan (schedule, built passes,
     kernel texts); results stay bit-identical across repeats and another
     list in between does not disturb them."""
-    n = 26   # the slot search runs from the first sighting at this size
+    n = 22
     a_ops = C.ops_to_array(C.random_layered(n, 3, 61, initial_h=True))
     b_ops = C.ops_to_array(C.qft(n))
     outs = []

@@ -11,6 +11,8 @@ from qoa_b200 import circuits as C
 from oracle import pyoracle as po
 from tests.plan_emulator import replay
 
+QOA_PLAN_SLOT_SEARCH = 0x100
+
 
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
@@ -65,11 +67,13 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("search", [0, 1])
 @pytest.mark.parametrize("quirk", [0, 1])
 @pytest.mark.parametrize("name,n,make", CASES, ids=[c[0] for c in CASES])
-def test_plan_replay_matches_oracle(name, n, make, quirk):
+def test_plan_replay_matches_oracle(name, n, make, quirk, search):
+    """search=1: the slot search (used from 26 qubits on) forced at this size."""
     ops = make()
-    flags = qb.QOA_FLAG_COMPAT_MASK_QUIRK if quirk else 0
+    flags = (qb.QOA_FLAG_COMPAT_MASK_QUIRK if quirk else 0) | (QOA_PLAN_SLOT_SEARCH if search else 0)
     plan = qb.plan(n, C.ops_to_array(ops), flags)
     assert plan["npasses"] >= 1
     # each expanded gate is in exactly one step, at a distinct slot
@@ -81,11 +85,12 @@ def test_plan_replay_matches_oracle(name, n, make, quirk):
 
 
 def test_layered_30_pass_count():
-    """The 930-gate 30-qubit workload packs into far fewer sweeps than gates."""
+    """The 930-gate 30-qubit workload packs into far fewer sweeps than gates;
+    the slot search (on at this size) packs it into 13."""
     ops = C.layered_h_workload()
     plan = qb.plan(30, C.ops_to_array(ops), qb.QOA_FLAG_COMPAT_MASK_QUIRK)
     assert len(plan["pass_of"]) == 930
-    assert plan["npasses"] <= 40
+    assert plan["npasses"] <= 14
 
 
 def test_per_gate_flag_gives_one_step_per_gate():
