@@ -898,10 +898,12 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         for (int k = 0; k < REG_BITS; ++k) c += ang_reg[k].empty() ? 0 : 1;
         return c;
     };
+    uint32_t tab_touched = 0;  // registers whose table factor is not exactly 1
     auto tab_reset = [&]() {
         for (int v = 0; v < REGS; ++v) tab[v] = d2(1, 0);
         tab_bits = 0;
         tab_count = 0;
+        tab_touched = 0;
     };
     tab_reset();
     auto flush_tab = [&]() -> bool {
@@ -917,6 +919,9 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             if (ncoef + REGS > MAX_PASS_COEF) return false;
             o->code = PC_DIAG_TAB;
             o->coef = (uint16_t)ncoef;
+            // the registers whose factor is not exactly 1 (the generated
+            // kernels multiply only those; the interpreter multiplies all)
+            o->tmask = tab_touched;
             for (int v = 0; v < REGS; ++v) P.coef[ncoef++] = tab[v];
         }
         tab_reset();
@@ -1096,8 +1101,10 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         }
         if (!o.has_tp) {  // register-only: joins the table
             for (int v = 0; v < REGS; ++v)
-                if (((uint32_t)v & o.cond_reg) == o.cond_reg)
+                if (((uint32_t)v & o.cond_reg) == o.cond_reg) {
                     tab[v] = d2(tab[v].x * d.x - tab[v].y * d.y, tab[v].x * d.y + tab[v].y * d.x);
+                    tab_touched |= 1u << v;
+                }
             tab_bits |= o.cond_reg;
             o.code = PC_DIAG_M;
             tab_last = o;

@@ -449,7 +449,9 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
                     break;
                 }
                 case PC_DIAG_TAB:
-                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], %s[%u]);", v, v, cf, c + v);
+                    // registers whose factor is exactly 1 are left alone
+                    for (int v = 0; v < REGS; ++v)
+                        if ((tm >> v) & 1) E.line("a[%d] = c_mul(a[%d], %s[%u]);", v, v, cf, c + v);
                     break;
                 case PC_FLUSH:
                     for (int v = 0; v < REGS; ++v) E.line("a[%d] = c_mul(a[%d], pend);", v, v);
@@ -662,8 +664,11 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
                     break;
                 }
                 case PC_DIAG_TAB:
+                    // a pair whose two factors are exactly 1 is left alone
                     for (int j = 0; j < 8; ++j)
-                        E.line("cmul2(re[%d], im[%d], stab[%u], stab[%u]);", j, j, 16 * tab_at[oi] + j, 16 * tab_at[oi] + 8 + j);
+                        if (((tm >> j) | (tm >> (j + 8))) & 1)
+                            E.line("cmul2(re[%d], im[%d], stab[%u], stab[%u]);", j, j, 16 * tab_at[oi] + j,
+                                   16 * tab_at[oi] + 8 + j);
                     break;
                 case PC_FLUSH:
                     E.line("{ const u64p cr = bc(pend.x), ci = bc(pend.y);");
