@@ -1786,6 +1786,16 @@ int run_perm(qoa_state_t s, const Gate& g) {
     return QOA_OK;
 }
 
+// Max gates per tile pass of a state: its own setting, else QOA_PASS_GATES
+// (tuning), else the scheduler's default.
+int state_pass_budget(qoa_state_t s) {
+    static const int env = [] {
+        const char* v = getenv("QOA_PASS_GATES");
+        return v ? std::max(0, atoi(v)) : 0;
+    }();
+    return s->pass_budget ? s->pass_budget : env;
+}
+
 int execute(qoa_state_t s, std::vector<Gate>& G) {
     const bool c64 = s->precision == QOA_PREC_F32;
     if (c64 && (s->flags & QOA_FLAG_F32_TENSOR)) return execute_f32(s, G);
@@ -1810,7 +1820,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
             if (!s->plans) s->plans = std::make_shared<PlanCache>();
             PlanCache& pc = *static_cast<PlanCache*>(s->plans.get());
             const uint64_t key = (uint64_t)s->n | ((uint64_t)c64 << 8) | ((uint64_t)prebuild << 9) |
-                                 ((uint64_t)(uint32_t)s->pass_budget << 16);
+                                 ((uint64_t)(uint32_t)state_pass_budget(s) << 16);
             plan_hash(seg, key, local.h1, local.h2);
             for (auto& e : pc.entries)
                 if (e.h1 == local.h1 && e.h2 == local.h2) pe = &e;
@@ -1823,7 +1833,7 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         if (fresh) {
             // the plan depends on the op list and the size only, so a list
             // executed again gives bit-identical results
-            pe->steps = schedule(seg, s->n, per_gate, false, s->pass_budget, slot_search_pays(s->n));
+            pe->steps = schedule(seg, s->n, per_gate, false, state_pass_budget(s), slot_search_pays(s->n));
             pe->built_of.assign(pe->steps.size(), -1);
             // tile passes of a large state: built ahead, and their generated
             // kernels requested from the compile cache
