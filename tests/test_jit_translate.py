@@ -67,3 +67,19 @@ def test_bad_sizes_fail_cleanly():
         qb.jit_translate(8, C.qft(8))
     with pytest.raises(qb.QoaError):
         qb.jit_translate(40, C.qft(4))
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_batch_form_compiles(precision):
+    """The batch (arena) form: one kernel per pass over a job list, the
+    rotation form read at run time; it compiles and its text does not
+    depend on rotation angles."""
+    n = 13
+    def circ(a):
+        return [C.Op(C.H, [q]) for q in range(n)] + [C.Op(C.RY, [q], a * (q + 1)) for q in range(n)] + \
+               [C.Op(C.CZ, [q, (q + 1) % n]) for q in range(n)] + [C.Op(C.RX, [q], 2.9 - a * q) for q in range(n)]
+    src1, np1 = qb.jit_translate(n, circ(0.21), compile=True, precision=precision, arena=True)
+    src2, np2 = qb.jit_translate(n, circ(1.37), precision=precision, arena=True)
+    assert np1 == np2 and np1 > 0
+    assert src1 == src2
+    assert "const qoa::ArenaJob J = jobs[blockIdx.x >> 2];" in src1
