@@ -14,6 +14,7 @@
 // run-time mappings — disappears, and the compiler schedules across gates.
 #include "qoa_jit.h"
 
+#include <dlfcn.h>
 #include <nvrtc.h>
 
 #include <atomic>
@@ -27,6 +28,7 @@
 #include <deque>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <unordered_map>
 #include <algorithm>
 #include <array>
@@ -808,33 +810,90 @@ std::string program_text(const std::vector<std::string>& names, const std::vecto
     return src;
 }
 
+// NVRTC is loaded at first use (dlopen), so that the library loads, and
+// runs every pass on the interpreter kernels, where the toolkit's
+// libnvrtc is absent.
+struct NvrtcApi {
+    decltype(&nvrtcCreateProgram) create = nullptr;
+    decltype(&nvrtcCompileProgram) compile = nullptr;
+    decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+    decltype(&nvrtcGetProgramLog) log = nullptr;
+    decltype(&nvrtcGetErrorString) error_string = nullptr;
+    decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+    decltype(&nvrtcGetCUBIN) cubin = nullptr;
+    decltype(&nvrtcDestroyProgram) destroy = nullptr;
+    std::string why;  // set when unavailable
+};
+
+const NvrtcApi& nvrtc() {
+    static const NvrtcApi api = [] {
+        NvrtcApi a;
+        const char* paths[] = {"libnvrtc.so.12", "libnvrtc.so",
+#ifdef QOA_NVRTC_PATH
+                               QOA_NVRTC_PATH,
+#endif
+        };
+        void* h = nullptr;
+        for (const char* p : paths)
+            if ((h = dlopen(p, RTLD_NOW | RTLD_LOCAL)) != nullptr) break;
+        if (!h) {
+            a.why = "libnvrtc could not be loaded: passes run on the interpreter kernels";
+            return a;
+        }
+        bool ok = true;
+        auto sym = [&](auto& f, const char* name) {
+            f = reinterpret_cast<std::remove_reference_t<decltype(f)>>(dlsym(h, name));
+            ok = ok && f != nullptr;
+        };
+        sym(a.create, "nvrtcCreateProgram");
+        sym(a.compile, "nvrtcCompileProgram");
+        sym(a.log_size, "nvrtcGetProgramLogSize");
+        sym(a.log, "nvrtcGetProgramLog");
+        sym(a.error_string, "nvrtcGetErrorString");
+        sym(a.cubin_size, "nvrtcGetCUBINSize");
+        sym(a.cubin, "nvrtcGetCUBIN");
+        sym(a.destroy, "nvrtcDestroyProgram");
+        if (!ok) {
+            a = NvrtcApi();
+            a.why = "libnvrtc lacks an entry point the engine needs: passes run on the interpreter kernels";
+        }
+        return a;
+    }();
+    return api;
+}
+
 // NVRTC: the kernels named names[i] with bodies[i], as one sm_100a cubin.
 bool build_cubin(const std::vector<std::string>& names, const std::vector<std::string>& bodies,
                  std::vector<char>& cubin, std::string& err) {
+    const NvrtcApi& nv = nvrtc();
+    if (!nv.create) {
+        err = nv.why;
+        return false;
+    }
     const std::string src = program_text(names, bodies);
     const char* hdrs[] = {kTypesHeader, kDevHeader, kDev32Header};
     const char* hnames[] = {"qoa_kernels.cuh", "qoa_pass_dev.cuh", "qoa_pass32_dev.cuh"};
     nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src.c_str(), "qoa_jit_pass.cu", 3, hdrs, hnames) != NVRTC_SUCCESS) {
+    if (nv.create(&prog, src.c_str(), "qoa_jit_pass.cu", 3, hdrs, hnames) != NVRTC_SUCCESS) {
         err = "nvrtcCreateProgram failed";
         return false;
     }
     const char* opts[] = {"-arch=sm_100a", "-std=c++17", "--fmad=true"};
-    const nvrtcResult rc = nvrtcCompileProgram(prog, 3, opts);
+    const nvrtcResult rc = nv.compile(prog, 3, opts);
     if (rc != NVRTC_SUCCESS) {
         size_t n = 0;
-        nvrtcGetProgramLogSize(prog, &n);
+        nv.log_size(prog, &n);
         std::string log(n, '\0');
-        if (n) nvrtcGetProgramLog(prog, &log[0]);
-        err = std::string("NVRTC: ") + nvrtcGetErrorString(rc) + ": " + log.substr(0, 2000);
-        nvrtcDestroyProgram(&prog);
+        if (n) nv.log(prog, &log[0]);
+        err = std::string("NVRTC: ") + nv.error_string(rc) + ": " + log.substr(0, 2000);
+        nv.destroy(&prog);
         return false;
     }
     size_t cs = 0;
-    nvrtcGetCUBINSize(prog, &cs);
+    nv.cubin_size(prog, &cs);
     cubin.resize(cs);
-    nvrtcGetCUBIN(prog, cubin.data());
-    nvrtcDestroyProgram(&prog);
+    nv.cubin(prog, cubin.data());
+    nv.destroy(&prog);
     return true;
 }
 
