@@ -828,11 +828,15 @@ struct NvrtcApi {
 const NvrtcApi& nvrtc() {
     static const NvrtcApi api = [] {
         NvrtcApi a;
-        const char* paths[] = {"libnvrtc.so.12", "libnvrtc.so",
+        // the toolkit the library was built with first, by full path: a
+        // process may already hold another NVRTC under the same soname
+        // (PyTorch's wheels bring their own), whose code generation can
+        // differ in the last bit from the interpreter kernels'
+        const char* paths[] = {
 #ifdef QOA_NVRTC_PATH
-                               QOA_NVRTC_PATH,
+            QOA_NVRTC_PATH,
 #endif
-        };
+            "libnvrtc.so.12", "libnvrtc.so"};
         void* h = nullptr;
         for (const char* p : paths)
             if ((h = dlopen(p, RTLD_NOW | RTLD_LOCAL)) != nullptr) break;
