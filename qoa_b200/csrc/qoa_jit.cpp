@@ -78,11 +78,20 @@ struct Emit {
     std::string s;
     void line(const char* fmt, ...) __attribute__((format(printf, 2, 3))) {
         char buf[512];
-        va_list ap;
+        va_list ap, ap2;
         va_start(ap, fmt);
-        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_copy(ap2, ap);
+        const int k = vsnprintf(buf, sizeof buf, fmt, ap);
         va_end(ap);
-        s += buf;
+        if (k >= (int)sizeof buf) {  // a long line (e.g. many outer-qubit runs): format again in full
+            std::string big((size_t)k + 1, '\0');
+            vsnprintf(&big[0], big.size(), fmt, ap2);
+            big.resize((size_t)k);
+            s += big;
+        } else if (k > 0) {
+            s += buf;
+        }
+        va_end(ap2);
         s += '\n';
     }
 };
