@@ -48,6 +48,9 @@ CASES = [
     ("layered", 20, lambda: C.random_layered(20, 6, 3, initial_h=True), 1),
     ("qft", 20, lambda: C.qft(20), 0),
     ("mixed", 16, lambda: mixed_circuit(16, 200, 8), 0),
+    # 26+ qubits: the slot search makes deeper passes with more exchanges
+    ("layered26", 26, lambda: C.random_layered(26, 5, 9, initial_h=True), 1),
+    ("mixed28", 28, lambda: mixed_circuit(28, 150, 10), 0),
 ]
 
 
