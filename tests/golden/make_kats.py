@@ -8,8 +8,9 @@ Two levels:
   "vec"   — a src/vectorization.rs function applied to a raw slice (src/test.rs:62-472)
   "instr" — QuantumState::execute_arithmetic on a QuantumState (src/test.rs:2199-2667)
 
-Run with the reference checked out at QOA_REFERENCE (default /root/reference)
-to refresh the line numbers; without it the previous numbers are kept.
+Run as `python tests/golden/make_kats.py [path-to-qoa-checkout]`: with the
+path, the line numbers are refreshed from its src/test.rs; without it the
+previous numbers are kept.
 """
 import json
 import math
@@ -18,7 +19,6 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "reference_kats.json")
-REF = os.environ.get("QOA_REFERENCE", "/root/reference")
 
 R2 = 1.0 / math.sqrt(2.0)
 PI = math.pi
@@ -140,14 +140,14 @@ CASES = [
 ]
 
 
-def main():
+def main(ref=None):
     lines = {}
     old = {}
     if os.path.exists(OUT):
         for rec in json.load(open(OUT))["cases"]:
             old[rec["name"]] = rec.get("src")
-    path = os.path.join(REF, "src", "test.rs")
-    if os.path.exists(path):
+    path = os.path.join(ref, "src", "test.rs") if ref else None
+    if path and os.path.exists(path):
         for i, line in enumerate(open(path), start=1):
             m = re.match(r"\s*fn (test_\w+)\(", line)
             if m and m.group(1) not in lines:
@@ -161,4 +161,5 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -1,5 +1,5 @@
-"""Bytecode front-end on the GPU: the reference's compiled example programs
-run through qoa_exe_run on a complex128 state, compared with the oracle
+"""Bytecode front-end on the GPU: the reference's example programs (assembled
+from their .qoa sources by this repository's assembler) run through qoa_exe_run on a complex128 state, compared with the oracle
 applying the same instruction stream with the same measurement uniforms
 (the handle's seeded stream): final amplitudes within 1e-12 relative L2,
 and every measurement outcome identical (the collapse would differ otherwise).
@@ -15,14 +15,14 @@ from qoa_b200 import qexe
 from oracle import pyoracle as po
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-GOLDEN = json.load(open(os.path.join(HERE, "golden", "reference_qexe.json")))
+PROGRAMS = json.load(open(os.path.join(HERE, "golden", "qexe_programs.json")))
 MEAS_STREAM = 0x6D656173
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["teleport.qx", "shor.qx", "aes-decryption-16.qx", "fusion.qx", "hello.qx"])
+@pytest.mark.parametrize("name", ["teleport", "shor", "aes-decryption-16", "fusion-sim", "hello_world"])
 def test_reference_program_matches_oracle(name):
-    f = bytes.fromhex(GOLDEN[name]["hex"])
+    f = bytes.fromhex(PROGRAMS[name]["hex"])
     n = max(qexe.parse(f)["inferred_qubits"], 1)
     seed = 1234
     ops, tres, tout = qexe.trace(f)

@@ -1,10 +1,14 @@
 """Bytecode front-end (host side): .qexe header parsing and qubit inference,
 the run_exe interpreter traced without a GPU, and the assembler.
 
-The reference's own compiled example programs (tests/golden/
-reference_qexe.json, made by make_qexe_golden.py) must parse, run to HALT and
-infer the qubit counts `qoa run` would; small programs of our own pin the
-instruction semantics (jumps, registers, printing, the loop quirk)."""
+The fixtures (tests/golden/qexe_programs.json, made by make_qexe_fixtures.py)
+are the reference's example sources (qoa_files/*.qoa) assembled by this
+repository's own assembler; they must parse, run to HALT and infer the qubit
+counts `qoa run` would. The assembler itself is pinned instruction by
+instruction against bytes written out by hand from the encode rules of
+src/instructions.rs (Instruction::encode, 631-1489); small programs of our
+own pin the instruction semantics (jumps, registers, printing, the loop quirk).
+"""
 import json
 import os
 import struct
@@ -17,7 +21,7 @@ from qoa_b200 import circuits as C
 from qoa_b200 import qexe
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-GOLDEN = json.load(open(os.path.join(HERE, "golden", "reference_qexe.json")))
+PROGRAMS = json.load(open(os.path.join(HERE, "golden", "qexe_programs.json")))
 
 
 def prog(src: str, kind="qexe") -> bytes:
@@ -29,9 +33,9 @@ def ops_summary(ops):
     return [(int(o["opcode"]), tuple(int(x) for x in o["q"][:o["nq"]]), float(o["angle"])) for o in ops]
 
 
-@pytest.mark.parametrize("name", sorted(GOLDEN))
-def test_reference_binaries_parse_and_run_to_halt(name):
-    f = bytes.fromhex(GOLDEN[name]["hex"])
+@pytest.mark.parametrize("name", sorted(PROGRAMS))
+def test_example_programs_parse_and_run_to_halt(name):
+    f = bytes.fromhex(PROGRAMS[name]["hex"])
     info = qexe.parse(f)
     assert info["kind"] in qexe.MAGIC and info["payload_offset"] == 9
     assert info["payload_len"] == len(f) - 9
@@ -43,21 +47,58 @@ def test_reference_binaries_parse_and_run_to_halt(name):
     assert qmax < max(info["inferred_qubits"], 1)
 
 
-def test_reference_hello_prints():
-    ops, res, out = qexe.trace(bytes.fromhex(GOLDEN["hello.qx"]["hex"]))
+def test_fixtures_are_what_the_assembler_writes_now():
+    # a fixture that no longer matches the assembler's output means the
+    # assembler changed; regenerate with make_qexe_fixtures.py after review
+    for name, rec in PROGRAMS.items():
+        f = bytes.fromhex(rec["hex"])
+        assert f[:4] == b"QEXE" and f[4] == 1 and struct.unpack("<I", f[5:9])[0] == len(f) - 9, name
+
+
+def test_hello_world_prints():
+    ops, res, out = qexe.trace(bytes.fromhex(PROGRAMS["hello_world"]["hex"]))
     assert out == b"Hello, World!\n" and len(ops) == 0 and res["halted"] == 1
 
 
-def test_reference_qubit_inference():
-    got = {k: qexe.parse(bytes.fromhex(v["hex"]))["inferred_qubits"] for k, v in GOLDEN.items()}
-    assert got["teleport.qx"] == 25 and got["hello.qx"] == 1 and got["fusion.qx"] == 4
+def test_qubit_inference():
+    got = {k: qexe.parse(bytes.fromhex(v["hex"]))["inferred_qubits"] for k, v in PROGRAMS.items()}
+    assert got == {"teleport": 25, "hello_world": 1, "fusion-sim": 4, "shor": 13, "aes-decryption-16": 25}
 
 
-def test_assembler_pinned_against_reference_compiler():
-    # recorded when the fixture was made: our assembler reproduced these
-    # reference binaries byte for byte from their sources
-    matched = [k for k, v in GOLDEN.items() if v.get("assembler_matches_reference")]
-    assert {"hello.qx", "teleport.qx", "shor.qx", "aes.qx"} <= set(matched)
+# (source line, expected bytes written out from the encode rule, rule's line in src/instructions.rs)
+F05 = "000000000000e03f"   # 0.5 as f64, little endian
+F10 = "000000000000f03f"   # 1.0
+F025 = "000000000000d03f"  # 0.25
+F20 = "0000000000000040"   # 2.0
+ENCODINGS = [
+    ("QINIT 3", "0403", 634), ("QI 3", "0403", 634), ("MEASURE 2", "3202", 639), ("M 2", "3202", 639),
+    ("H 1", "0501", 644), ("HAD 1", "0501", 644), ("CNOT 0 1", "170001", 647), ("CN 2 0", "170200", 647),
+    ("Z 2", "0602", 650), ("X 2", "0702", 651), ("T 4", "0d04", 652), ("S 4", "0e04", 653),
+    ("P 1 0.5", "0801" + F05, 654), ("PHASESHIFT 1 0.5", "0801" + F05, 654),
+    ("RESET 1", "0a01", 664), ("RST 1", "0a01", 664), ("SWAP 0 1", "0b0001", 669),
+    ("CSWAP 0 1 2", "0c000102", 670), ("ENTANGLE 0 1", "110001", 673), ("EBELL 0 1", "120001", 674),
+    ("EMULTI 0 1 2", "1303000102", 677), ("ECLUSTER 0 1 2", "1403000102", 682),
+    ("ESWAP 0 1 2 3", "1500010203", 687), ("RESETALL", "1c", 723), ("SETPHASE 1 0.25", "1d01" + F025, 733),
+    ("CHARLOAD 2 'A'", "310241", 753), ("CHAROUT 2", "1802", 756),
+    ("RX 0 1.0", "2200" + F10, 761), ("RY 0 1.0", "2300" + F10, 766), ("RZ 0 1.0", "0f00" + F10, 771),
+    ("PHASE 2 0.5", "2402" + F05, 776), ("CZ 1 0", "1e0100", 781), ("REGSET 3 2.0", "2103" + F20, 790),
+    ("LOOPSTART 2", "0102", 799), ("LOOPEND", "10", 802), ("ROT 0 x 0.5", "330078" + F05, 805),
+    ("CPHASE 0 1 0.5", "350001" + F05, 822), ("APPLYCPHASE 0 1 0.5", "350001" + F05, 822),
+    ("JMP -3", "90fdffffffffffffff", 988), ("REGADD 0 1 2", "54000102", 1029), ("REGCOPY 4 5", "580405", 1041),
+    ("HALT", "ff", 1345), ("JMPABS 16", "911000000000000000", 1353),
+    ("IFLT 0 1 -4", "930001fcffffffffffffff", 1363),
+    ('PRINTF "x" 1 2', "98" + "0100000000000000" + "78" + "020102", 1387),
+    ('PRINT "a"', "99" + "0100000000000000" + "61", 1395),
+    ('PRINTLN "hi"', "9a" + "0200000000000000" + "6869", 1401),
+    ("SEEDRNG 7", "ad0700000000000000", 1476),
+]
+
+
+@pytest.mark.parametrize("line,expect,rule", ENCODINGS, ids=[e[0] for e in ENCODINGS])
+def test_assembler_matches_encode_rules(line, expect, rule):
+    payload, skipped = qexe.assemble(line)
+    assert not skipped
+    assert payload == bytes.fromhex(expect), f"src/instructions.rs:{rule}"
 
 
 def test_quantum_ops_and_run_exe_noops():
