@@ -141,62 +141,100 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_gates_per_s(ops_arr, n, max_gates, max_seconds):
-    """Times the oracle (faithful profile) gate by gate from the start of the
-    circuit; returns (gates/s, gates timed, threads)."""
-    from oracle import pyoracle as po
-    po.set_fast(False)
-    st = po.OracleState(n, 1)
-    t_total, k = 0.0, 0
-    for i in range(min(max_gates, len(ops_arr))):
+GATE_CLASS = {0x05: "H", 0x0D: "T", 0x0E: "S", 0x22: "RX", 0x23: "RY", 0x0F: "RZ", 0x08: "P", 0x17: "CNOT",
+              0x1E: "CZ", 0x35: "CPHASE"}
+CPU_FORMULA = ("gates/s = G / sum_c N_c * t_c: t_c = measured seconds of one class-c gate of the circuit on the "
+               "faithful oracle (single-thread gate loop + all-core normalize), N_c = class-c gates in the circuit, "
+               "G = sum_c N_c; every page of the state is written once, untimed, before the first timing")
+
+
+def gate_classes(ops_arr):
+    """(class -> count in the circuit, class -> index of its first gate)."""
+    counts, first = {}, {}
+    for i, op in enumerate(ops_arr):
+        c = GATE_CLASS.get(int(op["opcode"]), "other")
+        counts[c] = counts.get(c, 0) + 1
+        first.setdefault(c, i)
+    return counts, first
+
+
+def extrapolate(times: dict, counts: dict) -> float:
+    """Gates/s of the whole circuit from per-class mean gate times (a class
+    not timed yet takes the mean of all timed gates)."""
+    timed = [t for v in times.values() for t in v]
+    mean_all = sum(timed) / len(timed)
+    tot = sum(counts[c] * (sum(times[c]) / len(times[c]) if times.get(c) else mean_all) for c in counts)
+    return sum(counts.values()) / tot
+
+
+class CpuGateTimer:
+    """The oracle in the reference's time profile on an n-qubit state, timing
+    one gate at a time by class (the state is touched once, untimed)."""
+
+    def __init__(self, n, ops_arr):
+        from oracle import pyoracle as po
+        self.po = po
+        po.set_fast(False)
+        self.st = po.OracleState(n, 1)
+        self.st.touch()
+        self.ops = ops_arr
+        self.counts, self.first = gate_classes(ops_arr)
+        self.order = [c for c in GATE_CLASS.values() if c in self.counts]
+        self.times = {c: [] for c in self.order}
+        self.k = 0
+
+    def next(self) -> float:
+        """Times the first gate of the next class (round robin) once."""
+        c = self.order[self.k % len(self.order)]
+        self.k += 1
+        i = self.first[c]
         t0 = time.perf_counter()
-        st.apply(ops_arr[i:i + 1])
-        t_total += time.perf_counter() - t0
-        k += 1
-        if t_total > max_seconds:
-            break
-    st.close()
-    return k / t_total, k, int(po.lib.orc_get_max_threads())
+        self.st.apply(self.ops[i:i + 1])
+        dt = time.perf_counter() - t0
+        self.times[c].append(dt)
+        return dt
+
+    def value(self) -> float:
+        return extrapolate(self.times, {c: self.counts[c] for c in self.order})
+
+    def record(self) -> dict:
+        return {"per_class_s": {c: sum(v) / len(v) for c, v in self.times.items() if v},
+                "class_counts": {c: self.counts[c] for c in self.order}, "formula": CPU_FORMULA}
+
+    def threads(self) -> int:
+        return int(self.po.lib.orc_get_max_threads())
+
+    def close(self):
+        self.st.close()
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    import numpy as np  # noqa: F401
-    from qoa_b200 import circuits as C
-    from oracle import pyoracle as po
+    from qoa_b200 import circuits as C  # the generators only: no GPU library is opened
     n = WORKLOAD["n_qubits"]
     ops = C.ops_to_array(C.layered_h_workload(n, WORKLOAD["depth"], WORKLOAD["seed"]))
-    po.set_fast(False)
-    st = po.OracleState(n, 1)
-    per_step = args.ref_gates_per_step
-    pos = 0
-
-    def step():
-        nonlocal pos
-        for _ in range(per_step):
-            st.apply(ops[pos % len(ops): pos % len(ops) + 1])
-            pos += 1
-
+    timer = CpuGateTimer(n, ops)
     for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
+        timer.next()
+    timer.times = {c: [] for c in timer.order}
+    dt = 0.0
     for _ in range(args.steps):
-        step()
-    dt = time.perf_counter() - t0
-    value = args.steps * per_step / dt
-    threads = int(po.lib.orc_get_max_threads())
+        dt += timer.next()
+    value = timer.value()
+    threads = timer.threads()
     line = {"impl": "reference", "metric": "gates/s", "value": value, "unit": "gates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(WORKLOAD),
-            "cpu_baseline": {"value": value, "unit": "gates/s", "cores": threads, "kind": "port",
-                             "sample": f"{per_step} gate(s) per step of the {len(ops)}-gate circuit at n={n}, in "
-                                       "order, faithful oracle: single-thread gate loop + all-core normalize"},
+            "cpu_baseline": dict({"value": value, "unit": "gates/s", "cores": threads, "kind": "port",
+                                  "sample": f"one gate per step, gate classes in turn (first gate of each class "
+                                            f"of the {len(ops)}-gate circuit at n={n}), faithful oracle; "
+                                            "extrapolated to the circuit's class mix"}, **timer.record()),
             "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    st.close()
+    timer.close()
     return 0
 
 
@@ -329,19 +367,55 @@ def run_ours(args):
         st2.close()
         del host
 
+    # ---- parity at full size (untimed): the same circuit on the per-gate
+    # kernels (no passes, no scheduler), and the circuit followed by its
+    # inverse, which must give back |0..0>; the oracle itself is checked
+    # against these plans in the tests (26 and 28 qubits, and 30 in the slow test)
+    parity = None
+    if not args.no_parity:
+        with qb.QuantumState(n, compat_mask_quirk=True, per_gate=True) as pg:
+            pg.execute(ops)
+            st.apply_reset_all()
+            st.execute(ops)
+            r_pg, f_pg = st.compare(pg)
+        inv = C.ops_to_array(C.inverse(ops_list))
+        st.execute(inv)
+        with qb.QuantumState(n, compat_mask_quirk=True) as zero:
+            r_inv, f_inv = st.compare(zero)
+        parity = {"vs_per_gate_kernels_rel_l2": r_pg, "vs_per_gate_kernels_infidelity": f_pg,
+                  "inverse_roundtrip_rel_l2": r_inv, "inverse_roundtrip_infidelity": f_inv,
+                  "tolerance": 1e-12,
+                  "note": "full-size checks: the pass plan against the per-gate kernels, and circuit + inverse "
+                          "= identity; the oracle is compared on the same plans at 26 and 28 qubits (tests)"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        g, k, thr = cpu_gates_per_s(ops, n, args.cpu_gates, args.cpu_seconds)
-        cpu = {"value": g, "unit": "gates/s", "cores": thr, "kind": "port",
-               "sample": f"first {k} gates of the same {G}-gate circuit at n={n}, faithful oracle: "
-                         "single-thread gate loop + all-core normalize after each gate"}
+        timer = CpuGateTimer(n, ops)
+        spent = 0.0
+        while spent < args.cpu_seconds and timer.k < args.cpu_gates:
+            spent += timer.next()
+        cpu = dict({"value": timer.value(), "unit": "gates/s", "cores": timer.threads(), "kind": "port",
+                    "sample": f"{timer.k} gates, one per gate class in turn (the first gate of each class of the "
+                              f"same {G}-gate circuit at n={n}), faithful oracle; extrapolated to the circuit's "
+                              "class mix"}, **timer.record())
+        timer.close()
+
+    frm = None
+    if rank == 0 and ws == 1 and not args.no_forms:
+        st.close()
+        frm = forms(args, ops)
 
     if rank == 0:
         line = {"metric": "gates/s", "value": value, "unit": "gates/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD),
-                "effective_gbs": C.algorithmic_bytes(ops_list, n, quirk=True) * args.steps * ws / (tmax / 1e3) / 1e9,
+                "fusion": {"per_gate_algorithmic_bytes": C.algorithmic_bytes(ops_list, n, quirk=True),
+                           "pass_algorithmic_bytes": roofline["algorithmic_bytes_per_launch"] *
+                           roofline["launches_per_step"] if roofline["algorithmic_bytes_per_launch"] else None,
+                           "note": "bytes the reference's per-gate sweeps would move for one circuit, against "
+                                   "the bytes the fused tile passes move"},
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+                "parity": parity, "forms": frm,
                 "e2e": e2e, "impl": "qoa_b200",
                 "jit": {"mode": args.jit, "generated_pass_launches_timed": int(jit_timed),
                         "kernels_compiled": int(jit["kernels"]), "compile_ms_total": jit["compile_ms"],
@@ -441,6 +515,11 @@ def run_qft(args):
 
 
 def run_batch(args):
+    print(json.dumps(batch_form(args)), flush=True)
+    return 0
+
+
+def batch_form(args) -> dict:
     """Batching form: 4096 hardware-efficient variational circuits (n ~ U{8..22},
     L ~ U{2..12} layers of RY+RZ on every qubit then a CZ ladder, 8 random
     Z-strings each), all in one batch: shared-memory persistent kernel for the
@@ -564,15 +643,14 @@ def run_batch(args):
                                "sample": f"{done} circuits drawn at random from the same batch, faithful oracle "
                                          "(per-gate loops + normalize after every gate)"}
     out["generate_s"] = gen_s
-    print(json.dumps(out), flush=True)
-    return 0
+    return out
 
 
-def serve_requests(count: int, seed: int = 4, nmax: int = 28, dmax: int = 200):
+def serve_requests(count: int, seed: int = 4, nmax: int = 28, dmax: int = 200, rate: float = 2000.0):
     """Serving workload: random layered circuits (gate mix of the layered
     workload), n log-uniform in [10, nmax], depth uniform in [10, dmax],
     depolarising p = 1e-3 per gate, 64 trajectories x 16 shots, seeded per
-    request; Poisson arrival gaps with mean 1/2000 s."""
+    request; Poisson arrival gaps with mean 1/rate s."""
     import numpy as np
     from qoa_b200 import circuits as C
     rng = np.random.default_rng(seed)
@@ -582,63 +660,264 @@ def serve_requests(count: int, seed: int = 4, nmax: int = 28, dmax: int = 200):
         n = int(np.floor(np.exp(rng.uniform(np.log(10), np.log(nmax + 1)))))
         n = min(max(n, 10), nmax)
         depth = int(rng.integers(10, dmax + 1))
-        t += float(rng.exponential(1.0 / 2000.0))
+        t += float(rng.exponential(1.0 / rate))
         out.append(dict(n=n, depth=depth, ops=C.ops_to_array(C.random_layered(n, depth, 7000 + k)), noise_p=1e-3,
                         trajectories=64, shots=16, seed=90000 + k, arrival=t))
     return out
 
 
 def run_serve(args):
-    """Serving form: a bounded Poisson request stream through the continuous-
-    batching server, per precision. value = completed requests / (last
-    completion - first submission); p50 / p99 of submit-to-done latency."""
+    print(json.dumps(serve_form(args)), flush=True)
+    return 0
+
+
+def serve_stream(reqs, prec: str, workers: int) -> dict:
+    """One bounded request stream through the continuous-batching server:
+    completed circuits/s = requests / (last completion - first submission),
+    p50 / p99 of submit-to-done latency, overall and per qubit-count bucket."""
     import numpy as np
     import qoa_b200 as qb
-    reqs = serve_requests(args.serve_requests, nmax=args.serve_max_qubits, dmax=args.serve_max_depth)
+    with qb.Server(prec, hbm_budget_gb=150, workers=workers) as srv:
+        t0 = srv.now()
+        for r in reqs:
+            while srv.now() - t0 < r["arrival"]:
+                time.sleep(max(0.0, min(0.001, r["arrival"] - (srv.now() - t0))))
+            srv.submit(r["n"], r["ops"], r["noise_p"], r["trajectories"], r["shots"], r["seed"])
+        res = []
+        while len(res) < len(reqs):
+            res += srv.poll(timeout_ms=1000)
+        st = srv.stats()
+        for x in res:
+            if x["status"] == 0:
+                srv.take_shots(x["id"], int(x["shots"]))
+    lat = np.array([x["t_done"] - x["t_submit"] for x in res])
+    buckets = {}
+    for lo_n, hi_n in ((10, 14), (15, 19), (20, 24), (25, 28)):
+        sel = np.array([lo_n <= x["n"] <= hi_n for x in res])
+        if sel.any():
+            buckets[f"n{lo_n}-{hi_n}"] = {"requests": int(sel.sum()),
+                                          "p50_latency_s": float(np.percentile(lat[sel], 50)),
+                                          "p99_latency_s": float(np.percentile(lat[sel], 99))}
+    first = min(x["t_submit"] for x in res)
+    last = max(x["t_done"] for x in res)
+    return {"value": len(res) / (last - first), "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": last - first,
+            "failed": sum(1 for x in res if x["status"] != 0), "by_qubits": buckets,
+            "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": workers}
+
+
+def serve_cpu_baseline(reqs, seconds: float) -> dict:
+    """The oracle in the reference's time profile (single-thread gate loops,
+    all-core normalize, depolarising draws after every gate) on a sample of
+    the requests: the first gates of one trajectory per sampled request are
+    timed and extrapolated to the request's gates x 64 trajectories."""
+    import numpy as np
+    from oracle import pyoracle as po
+    po.set_fast(False)
+    rng = np.random.default_rng(11)
+    t_req, done, spent = [], 0, 0.0
+    for i in rng.permutation(len(reqs)):
+        r = reqs[i]
+        st = po.OracleState(r["n"], 0)
+        st.touch()
+        st.set_noise(1, r["noise_p"], r["seed"], 0)
+        k, tt = 0, 0.0
+        while k < len(r["ops"]) and tt < seconds / 4:
+            t0 = time.perf_counter()
+            st.apply(r["ops"][k:k + 1])
+            tt += time.perf_counter() - t0
+            k += 1
+        st.close()
+        t_req.append(tt / k * len(r["ops"]) * r["trajectories"])
+        spent += tt
+        done += 1
+        if spent > seconds:
+            break
+    return {"value": len(t_req) / sum(t_req), "unit": "circuits/s", "kind": "port",
+            "cores": int(po.lib.orc_get_max_threads()),
+            "sample": f"{done} requests drawn at random from the stream; per request the first gates of one "
+                      "noisy trajectory on the faithful oracle, extrapolated to its gates x 64 trajectories"}
+
+
+def serve_form(args) -> dict:
+    """Serving form: bounded Poisson request streams through the continuous-
+    batching server, one per offered rate in args.serve_rates and precision.
+    The line's value is the completed circuits/s at the highest offered rate
+    (the server saturated); `sustainable_rate` is the highest offered rate
+    whose stream completed at >= 90 % of that rate."""
+    import numpy as np
+    rates = [float(x) for x in str(getattr(args, "serve_rates", "2000")).split(",")]
+    base = serve_requests(args.serve_requests, nmax=args.serve_max_qubits, dmax=args.serve_max_depth)
     out = {"metric": "circuits/s (served, 64 trajectories x 16 shots each), p50/p99 latency", "unit": "circuits/s",
            "impl": "qoa_b200", "higher_is_better": True, "n_gpus": 1, "steps": 1, "warmup": 0, "scaling": "weak",
            "vs_baseline": None, "data": "synthetic (seeded random layered circuits, Poisson arrivals)",
-           "config": {"workload": f"{len(reqs)} requests, n log-uniform [10,{args.serve_max_qubits}], depth "
-                                  f"U[10,{args.serve_max_depth}], p=1e-3, 64 traj x 16 shots, mean arrival "
-                                  "2000 req/s, HBM budget 150 GB",
-                      "requests": len(reqs),
-                      "n_hist": np.bincount([r["n"] for r in reqs], minlength=41)[10:args.serve_max_qubits + 1].tolist(),
-                      "gates": int(sum(len(r["ops"]) for r in reqs))}}
+           "config": {"workload": f"{len(base)} requests per stream, n log-uniform [10,{args.serve_max_qubits}], "
+                                  f"depth U[10,{args.serve_max_depth}], p=1e-3, 64 traj x 16 shots, HBM budget "
+                                  f"150 GB, offered rates {rates} req/s", "requests": len(base),
+                      "n_hist": np.bincount([r["n"] for r in base], minlength=41)[10:args.serve_max_qubits + 1].tolist(),
+                      "gates": int(sum(len(r["ops"]) for r in base))}}
     for prec in args.precisions.split(","):
-        with qb.Server(prec, hbm_budget_gb=150, workers=args.serve_workers) as srv:
-            t0 = srv.now()
-            for r in reqs:
-                while srv.now() - t0 < r["arrival"]:
-                    time.sleep(max(0.0, min(0.001, r["arrival"] - (srv.now() - t0))))
-                srv.submit(r["n"], r["ops"], r["noise_p"], r["trajectories"], r["shots"], r["seed"])
-            res = []
-            while len(res) < len(reqs):
-                res += srv.poll(timeout_ms=1000)
-            st = srv.stats()
-            for x in res:
-                if x["status"] == 0:
-                    srv.take_shots(x["id"], int(x["shots"]))
-        lat = np.array([x["t_done"] - x["t_submit"] for x in res])
-        buckets = {}
-        for lo_n, hi_n in ((10, 14), (15, 19), (20, 24), (25, 28)):
-            sel = np.array([lo_n <= x["n"] <= hi_n for x in res])
-            if sel.any():
-                buckets[f"n{lo_n}-{hi_n}"] = {"requests": int(sel.sum()),
-                                              "p50_latency_s": float(np.percentile(lat[sel], 50)),
-                                              "p99_latency_s": float(np.percentile(lat[sel], 99))}
-        first = min(x["t_submit"] for x in res)
-        last = max(x["t_done"] for x in res)
-        out[prec] = {"value": len(res) / (last - first), "p50_latency_s": float(np.percentile(lat, 50)),
-                     "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": last - first,
-                     "failed": sum(1 for x in res if x["status"] != 0), "by_qubits": buckets,
-                     "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": args.serve_workers,
-                     "ran_in": {"f64": sum(1 for x in res if x["precision"] == 0),
-                                "f32": sum(1 for x in res if x["precision"] == 1)}}
+        sweep = []
+        for lam in rates:
+            reqs = serve_requests(args.serve_requests, nmax=args.serve_max_qubits, dmax=args.serve_max_depth,
+                                  rate=lam)
+            rec = serve_stream(reqs, prec, args.serve_workers)
+            rec["offered_rate"] = lam
+            sweep.append(rec)
+        top = max(sweep, key=lambda r: r["offered_rate"])
+        ok = [r["offered_rate"] for r in sweep if r["value"] >= 0.9 * r["offered_rate"]]
+        out[prec] = dict(top, sweep=[{k: r[k] for k in ("offered_rate", "value", "p50_latency_s", "p99_latency_s",
+                                                         "by_qubits", "failed")} for r in sweep],
+                         sustainable_rate=max(ok) if ok else None)
     prim = args.precisions.split(",")[0]
     out.update(value=out[prim]["value"], p50_latency_s=out[prim]["p50_latency_s"],
                p99_latency_s=out[prim]["p99_latency_s"], dtype=prim)
-    print(json.dumps(out), flush=True)
-    return 0
+    if not getattr(args, "no_cpu", True):
+        out["cpu_baseline"] = serve_cpu_baseline(base, getattr(args, "cpu_seconds", 10.0))
+    return out
+
+
+def per_gate_class_gbs(n: int, ops_arr, layer_ops: int):
+    """Config 1 per gate class: the first `layer_ops` gates (the H layer and
+    the first random layer) each as its own per-gate kernel (QOA_FLAG_PER_GATE)
+    with CUDA-event times; GB/s per class = per-gate algorithmic bytes (2S for
+    H / RX / RY / RZ, S for phase gates and CNOT, S/2 for CZ / CPHASE) over the
+    class's summed kernel time."""
+    import qoa_b200 as qb
+    sub = ops_arr[:layer_ops]
+    with qb.QuantumState(n, compat_mask_quirk=True, per_gate=True, profile=True) as st:
+        st.execute(sub)
+        st.sync()
+        st.launch_times()
+        st.apply_reset_all()
+        st.execute(sub)
+        st.sync()
+        ms, by, kind = st.launch_times()
+    gate_ms, gate_by = ms[kind == 1], by[kind == 1]
+    out = {}
+    if len(gate_ms) != len(sub):
+        return {"error": f"{len(gate_ms)} per-gate launches for {len(sub)} gates"}
+    peak, _ = measured_peaks()
+    for i, op in enumerate(sub):
+        c = GATE_CLASS.get(int(op["opcode"]), "other")
+        d = out.setdefault(c, {"gates": 0, "ms": 0.0, "bytes": 0.0})
+        d["gates"] += 1
+        d["ms"] += float(gate_ms[i])
+        d["bytes"] += float(gate_by[i])
+    for c, d in out.items():
+        d["gbs"] = d["bytes"] / (d["ms"] / 1e3) / 1e9
+        d["frac_of_peak"] = d["gbs"] / peak
+        d["ms_per_gate"] = d["ms"] / d["gates"]
+    return out
+
+
+def qft_form(n: int, steps: int, warmup: int, tensor: bool = True) -> dict:
+    """QFT (H + CPHASE(pi/2^k) ladder + swap network) from a seeded Gaussian
+    state at n qubits: FP64 plain and FP32-fused gates/s side by side, and
+    the FP32 result's relative L2 / 1 - F against the FP64 one."""
+    import torch
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+    dev = torch.device("cuda", 0)
+    ops = C.ops_to_array(C.qft(n))
+
+    def timed(st, kind):
+        stream = torch.cuda.ExternalStream(st.stream_ptr(), device=dev)
+        for _ in range(warmup):
+            st.execute(ops)
+        qb.jit_wait()
+        st.execute(ops)
+        st.sync()
+        st.launch_times()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            st.execute(ops)
+        e1.record(stream)
+        st.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        lm, lb, lk = st.launch_times()
+        sel = lk == kind
+        bw = float(lb[sel].sum() / (lm[sel].sum() / 1e3) / 1e9) if sel.any() else None
+        return ms, int(sel.sum() // steps), bw
+
+    out = {"workload": f"QFT n={n} from a seeded Gaussian state", "gates": len(ops)}
+    with qb.QuantumState(n, profile=True) as s64:
+        s64.set_random_state(2)
+        ms64, p64, bw64 = timed(s64, 0)
+    with qb.QuantumState(n, precision="f32", profile=True) as s32:
+        s32.set_random_state(2)
+        ms32, p32, bw32 = timed(s32, 3)
+    out.update(fp64_gates_s=len(ops) / (ms64 / 1e3), fp32_gates_s=len(ops) / (ms32 / 1e3),
+               fp32_over_fp64=ms64 / ms32, fp64_ms=ms64, fp32_ms=ms32, fp64_passes=p64, fp32_passes=p32,
+               fp64_pass_gbs=bw64, fp32_pass_gbs=bw32)
+    if tensor:
+        with qb.QuantumState(n, precision="f32", profile=True, f32_tensor=True) as s32t:
+            s32t.set_random_state(2)
+            ms32t, p32t, _ = timed(s32t, 2)
+        out.update(fp32_tensor_gates_s=len(ops) / (ms32t / 1e3), fp32_tensor_over_fp64=ms64 / ms32t)
+    for tens in ((False, True) if tensor else (False,)):
+        with qb.QuantumState(n) as a, qb.QuantumState(n, precision="f32", f32_tensor=tens) as b:
+            a.set_random_state(2)
+            b.set_random_state(2)
+            a.execute(ops)
+            b.execute(ops)
+            r, f = b.compare(a)
+        key = "fp32_tensor" if tens else "fp32"
+        out[key + "_rel_l2_vs_fp64"] = r
+        out[key + "_infidelity_vs_fp64"] = f
+    return out
+
+
+def qft33_fp32(steps: int, warmup: int) -> dict:
+    """FP32-fused QFT throughput at 33 qubits (64 GiB complex64)."""
+    import torch
+    import qoa_b200 as qb
+    from qoa_b200 import circuits as C
+    ops = C.ops_to_array(C.qft(33))
+    with qb.QuantumState(33, precision="f32") as st:
+        st.set_random_state(2)
+        stream = torch.cuda.ExternalStream(st.stream_ptr(), device=torch.device("cuda", 0))
+        for _ in range(warmup):
+            st.execute(ops)
+        qb.jit_wait()
+        st.execute(ops)
+        st.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            st.execute(ops)
+        e1.record(stream)
+        st.sync()
+        ms = e0.elapsed_time(e1) / steps
+    return {"n": 33, "gates": len(ops), "ms": ms, "gates_s": len(ops) / (ms / 1e3)}
+
+
+def forms(args, ops_arr) -> dict:
+    """The further forms on the default run, each bounded to finish in well
+    under a minute: config 1 per gate class, the precision form (QFT), the
+    batching form and the serving form (see each function)."""
+    out = {}
+    t0 = time.perf_counter()
+    out["config1_per_gate_class"] = per_gate_class_gbs(WORKLOAD["n_qubits"], ops_arr,
+                                                       WORKLOAD["n_qubits"] + WORKLOAD["n_qubits"] * 3 // 2)
+    out["precision_qft"] = qft_form(args.forms_qft_qubits, steps=3, warmup=2, tensor=True)
+    out["precision_qft"]["fp32_n33"] = qft33_fp32(steps=3, warmup=2)
+    bargs = argparse.Namespace(batch_count=4096, precisions="f64,f32", tune_sample=0, tune_seconds=0.0,
+                               steps=5, warmup=2, e2e_steps=1, no_cpu=False, cpu_seconds=10.0)
+    b = batch_form(bargs)
+    out["batch"] = {k: b[k] for k in ("config", "value", "ms_per_step", "roofline", "e2e", "cpu_baseline",
+                                      "f32_vs_f64_max_abs_diff") if k in b}
+    for prec in ("f64", "f32"):
+        if prec in b:
+            out["batch"][prec] = {k: b[prec][k] for k in ("value", "ms_per_step", "roofline", "jit", "routes")}
+    sargs = argparse.Namespace(serve_requests=args.forms_serve_requests, serve_max_qubits=args.forms_serve_max_qubits,
+                               serve_max_depth=200, serve_workers=16, precisions="f64,f32",
+                               serve_rates=args.forms_serve_rates, cpu_seconds=10.0, no_cpu=False)
+    out["serve"] = serve_form(sargs)
+    out["forms_wall_s"] = time.perf_counter() - t0
+    return out
 
 
 JIT_MODES = {"off": 0, "async": 1, "sync": 2}
@@ -673,8 +952,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-gates", type=int, default=12)
-    ap.add_argument("--cpu-seconds", type=float, default=25.0)
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision / batch / serving forms")
+    ap.add_argument("--forms-qft-qubits", type=int, default=32)
+    ap.add_argument("--forms-serve-requests", type=int, default=200)
+    ap.add_argument("--forms-serve-max-qubits", type=int, default=20)
+    ap.add_argument("--forms-serve-rates", default="50,100,200,2000",
+                    help="offered request rates (req/s) of the serving sweep")
+    ap.add_argument("--cpu-gates", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=60.0)
     ap.add_argument("--ref-gates-per-step", type=int, default=1)
     ap.add_argument("--qubits", type=int, default=30, help="smaller instances for profiling captures")
     ap.add_argument("--depth", type=int, default=20)
@@ -685,6 +971,7 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=16)
     ap.add_argument("--serve-max-qubits", type=int, default=28)
     ap.add_argument("--serve-max-depth", type=int, default=200)
+    ap.add_argument("--serve-rates", default="2000", help="offered request rates (req/s), one stream each")
     ap.add_argument("--qft-qubits", type=int, default=33)
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--precisions", default="f64,f32")

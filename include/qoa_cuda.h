@@ -84,6 +84,11 @@ extern "C" {
  * tensor cores (3xTF32) instead of the default complex64 tile passes; needs
  * n >= 11 */
 #define QOA_FLAG_F32_TENSOR         0x10u
+/* Plan every op list with the pass scheduler's slot search, whatever the
+ * state size (states of 26 or more qubits always plan with it). Results do
+ * not depend on it beyond rounding; it exercises the deeper passes that
+ * large states run, on states small enough to check against the CPU. */
+#define QOA_FLAG_SLOT_SEARCH        0x20u
 
 /* ---- opcodes: the reference byte code numbers (src/instructions.rs) ---- */
 #define QOA_OP_APPLYGATE   0x02  /* q[0]=qubit, q[1]= 'H','X','Y','Z','T','S' (execute_arithmetic APPLYGATE) */
@@ -145,7 +150,8 @@ typedef struct qoa_status_t {
     uint32_t nan_seen;
     uint32_t inf_seen;
     uint32_t zero_norm_resets;  /* times normalize() found norm^2 <= 1e-12 and reset to |0..0> */
-    uint32_t reserved;
+    uint32_t copy_timeouts;     /* nonzero: a streamed pass gave up waiting (~2 s) for a tile's
+                                   copy into shared memory; the state is not valid */
 } qoa_status_t;
 
 /* ---- (i) handle API ----------------------------------------------------- */
@@ -428,11 +434,14 @@ int qoa_jit_translate(uint32_t n, int precision, uint32_t flags, const qoa_op* o
  * device buffer itself, or a latency-critical caller that cannot accept
  * cudaMalloc's implicit synchronisation. Its scratch is one fixed static
  * device array of 75,776 bytes that every device loading the library holds
- * until exit. The first call on each device resolves that array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race: order
- * them. More than QOA_NOALLOC_MAX_MASKS masks -> QOA_E_ARG (see
- * qoa_last_error(NULL)). */
+ * until exit. The first call in each CUDA context (a device's primary
+ * context, or one the caller made with cuCtxCreate) resolves that array's
+ * address in that context (cudaGetSymbolAddress); make that first call before
+ * any stream capture. All calls share the array, so calls that overlap on the
+ * GPU race: order them. More than QOA_NOALLOC_MAX_MASKS masks -> QOA_E_ARG
+ * (see qoa_last_error(NULL)); a failed launch of its own -> QOA_E_CUDA (an
+ * error left pending by earlier work of the caller is neither reported nor
+ * cleared). */
 #define QOA_NOALLOC_MAX_MASKS 8
 int qoa_expect_z_noalloc(const void* d_amps, size_t len, const uint64_t* masks, size_t k, double* d_out,
                          void* stream);

@@ -31,6 +31,8 @@ def _load():
         "orc_get_max_threads": (i32, []),
         "orc_new": (vp, [sz, u32]),
         "orc_free": (None, [vp]),
+        "orc_touch": (None, [vp]),
+        "orc_set_defer_norm": (None, [vp, i32]),
         "orc_num_qubits": (sz, [vp]),
         "orc_amps": (vp, [vp]),
         "orc_set_noise": (None, [vp, i32, dbl, u64, u64]),
@@ -94,6 +96,18 @@ class OracleState:
 
     def __init__(self, n: int, flags: int = 0):
         self.h = lib.orc_new(n, flags)
+
+    def defer_norm(self, on: bool = True):
+        """Skips the per-gate normalize (noiseless unitary circuits at large n;
+        call normalize() once at the end)."""
+        lib.orc_set_defer_norm(self.h, 1 if on else 0)
+
+    def normalize(self):
+        lib.orc_normalize(self.h)
+
+    def touch(self):
+        """Maps every page of the state (untimed set-up before a timing)."""
+        lib.orc_touch(self.h)
 
     def close(self):
         if self.h:

@@ -5,14 +5,18 @@ over the C ABI of ``include/qoa_cuda.h`` (``libqoa_cuda.so``, built in-tree by
 ``make -C qoa_b200``). Method names, argument meaning and error behaviour follow
 the reference: gate methods given an out-of-range qubit print an error and do
 nothing (quantum_state.rs:189-195); ``measure`` raises on a bad qubit
-(quantum_state.rs:400-402). There is no CPU fallback: importing this package
-without the CUDA library raises ``ImportError``.
+(quantum_state.rs:400-402). There is no CPU fallback. The CUDA library is
+loaded on the first call into it, not at import, so the seeded circuit
+generators (``qoa_b200.circuits``) can be used by code that never touches
+the GPU engine; that first call raises ``ImportError`` when the library is
+missing.
 """
 from __future__ import annotations
 
 import ctypes
 import os
 import sys
+import threading
 from typing import Iterable, Optional, Sequence
 
 import numpy as np
@@ -33,6 +37,8 @@ QOA_JIT_OFF, QOA_JIT_ASYNC, QOA_JIT_SYNC = 0, 1, 2
 QOA_FLAG_PER_GATE = 0x2
 QOA_FLAG_PROFILE = 0x4
 QOA_FLAG_NOISE_GATE_QUBITS = 0x8
+QOA_FLAG_SLOT_SEARCH = 0x20
+QOA_PLAN_SLOT_SEARCH = 0x100  # qoa_plan only
 
 
 class QoaError(RuntimeError):
@@ -43,7 +49,7 @@ class QoaError(RuntimeError):
 
 class QoaStatus(ctypes.Structure):
     _fields_ = [("nan_seen", ctypes.c_uint32), ("inf_seen", ctypes.c_uint32),
-                ("zero_norm_resets", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("zero_norm_resets", ctypes.c_uint32), ("copy_timeouts", ctypes.c_uint32)]
 
 
 class JitStats(ctypes.Structure):
@@ -80,6 +86,9 @@ class RequestResult(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "done", "queued", "admitted", "trajectories_running",
                                                "states_resident", "bytes_reserved", "peak_bytes_reserved")]
+
+
+_EXTRA_SIGS: dict = {}
 
 
 def _load() -> ctypes.CDLL:
@@ -164,6 +173,7 @@ def _load() -> ctypes.CDLL:
         "qoa_vec_apply_controlled_phase_rotation": (i32, [vp, sz, sz, sz, dbl]),
         "qoa_vec_apply_reset_all": (i32, [vp, sz]),
     }
+    sig.update(_EXTRA_SIGS)
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
         f.restype = res
@@ -171,7 +181,42 @@ def _load() -> ctypes.CDLL:
     return lib
 
 
-lib = _load()
+class _Library:
+    """libqoa_cuda.so, opened (and its signatures declared) on first use."""
+
+    def __init__(self):
+        self._cdll = None
+        self._lock = threading.Lock()
+
+    def _get(self) -> ctypes.CDLL:
+        if self._cdll is None:
+            with self._lock:
+                if self._cdll is None:
+                    self._cdll = _load()
+        return self._cdll
+
+    @property
+    def loaded(self) -> bool:
+        return self._cdll is not None
+
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        return getattr(self._get(), name)
+
+
+lib = _Library()
+
+
+def register_signatures(sigs: dict):
+    """Declares result and argument types of further entry points (used by
+    the submodules); applied at load, or at once if the library is open."""
+    _EXTRA_SIGS.update(sigs)
+    if lib.loaded:
+        for name, (res, args) in sigs.items():
+            f = getattr(lib._cdll, name)
+            f.restype = res
+            f.argtypes = args
 
 
 def _check(rc: int, h=None, allow_range: bool = False) -> int:
@@ -221,8 +266,9 @@ class QuantumState:
     def __init__(self, n_qubits: int, noise_config: Optional[NoiseConfig] = None, *,
                  compat_mask_quirk: bool = False, per_gate: bool = False, profile: bool = False,
                  noise_gate_qubits_only: bool = False, seed: int = 0, precision: str = "f64",
-                 f32_tensor: bool = False):
+                 f32_tensor: bool = False, slot_search: bool = False):
         flags = ((QOA_FLAG_F32_TENSOR if f32_tensor else 0)
+                 | (QOA_FLAG_SLOT_SEARCH if slot_search else 0)
                  | (QOA_FLAG_COMPAT_MASK_QUIRK if compat_mask_quirk else 0)
                  | (QOA_FLAG_PER_GATE if per_gate else 0)
                  | (QOA_FLAG_PROFILE if profile else 0)
@@ -436,7 +482,8 @@ class QuantumState:
     def get_status(self) -> dict:
         st = QoaStatus()
         _check(lib.qoa_status(self._h, ctypes.byref(st)), self._h)
-        return {"nan": bool(st.nan_seen), "overflow": bool(st.inf_seen), "zero_norm_resets": st.zero_norm_resets}
+        return {"nan": bool(st.nan_seen), "overflow": bool(st.inf_seen), "zero_norm_resets": st.zero_norm_resets,
+                "copy_timeouts": st.copy_timeouts}
 
     # ---- engine plumbing --------------------------------------------------------
     def sync(self):

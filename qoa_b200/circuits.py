@@ -138,6 +138,28 @@ def layered_h_workload(n: int = 30, depth: int = 20, seed: int = 1) -> List[Op]:
     return random_layered(n, depth, seed, initial_h=True)
 
 
+def inverse(ops: Sequence[Op]) -> List[Op]:
+    """The adjoint circuit: the gates in reverse order, each inverted (H, X,
+    Z, CNOT, CZ, SWAP are their own inverses; T and S become PHASESHIFT by
+    -pi/4 and -pi/2; rotations and phases take the negated angle). The
+    CZ / CPHASE condition mask is whatever the state's mode makes of the same
+    operands, so the inverse holds in both mask modes."""
+    out: List[Op] = []
+    for op in reversed(list(ops)):
+        c = op.opcode
+        if c in (H, X, Z, CNOT, CZ, SWAP):
+            out.append(Op(c, op.qubits))
+        elif c == T:
+            out.append(Op(P, op.qubits, -math.pi / 4))
+        elif c == S:
+            out.append(Op(P, op.qubits, -math.pi / 2))
+        elif c in (RX, RY, RZ, P, CPHASE):
+            out.append(Op(c, op.qubits, -op.angle))
+        else:
+            raise ValueError(f"no inverse for opcode {c:#x}")
+    return out
+
+
 def qft(n: int, with_swaps: bool = True) -> List[Op]:
     """Quantum Fourier transform: for q = n-1 .. 0: H(q), then CPHASE(c, q,
     pi/2^k) for the lower qubits c = q-1 .. 0 (k = 1, 2, ...); then the swap

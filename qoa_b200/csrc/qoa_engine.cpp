@@ -830,7 +830,8 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     P.map0 = m;
 
     int nops = 0, ncoef = 0, nx = 0;
-    uint32_t dirty = 0;  // pending factor depends on lane / warp bits
+    // T positions (lane bits 0..4, warp bits 5..6) the pending factor depends on
+    uint32_t dirty = 0;
     auto new_op = [&]() -> PassOp* {
         if (nops >= MAX_PASS_OPS) return nullptr;
         PassOp* o = &P.ops[nops++];
@@ -992,7 +993,17 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
     };
     auto exchange_to = [&](const TileMap& nm) -> bool {
         if (!flush_tab() || !flush_mx() || !flush_tm() || !flush_ang_reg(0xfu) || !flush_ang_thr()) return false;
-        if (dirty) {
+        // The pending factor stays with the thread across the exchange when
+        // every lane / warp position it depends on keeps its tile bit: each
+        // amplitude the thread receives then came from a thread with the
+        // same bits there, so it owes the same factor. Otherwise flush it
+        // into the registers first.
+        uint32_t moved = 0;
+        for (int i = 0; i < LANE_BITS; ++i)
+            if (nm.lane[i] != m.lane[i]) moved |= 1u << i;
+        for (int k = 0; k < WARP_BITS; ++k)
+            if (nm.warp[k] != m.warp[k]) moved |= 1u << (LANE_BITS + k);
+        if (dirty & moved) {
             PassOp* f = new_op();
             if (!f) return false;
             f->code = PC_FLUSH;
@@ -1040,7 +1051,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         // tile bit needed last (the complex64 pass pairs amplitudes along it)
         auto key = [&](uint8_t x) { return x == pin ? (1 << 30) + 1 : (x == must ? -1 : next_use(i, x)); };
         std::stable_sort(nm.reg, nm.reg + REG_BITS, [&](uint8_t x, uint8_t y) { return key(x) < key(y); });
-        order_lanes(nm);
+        if (!getenv("QOA_NO_ORDER_LANES")) order_lanes(nm);
         return exchange_to(nm);
     };
     auto cond = [&](uint64_t mask, PassOp& op) {
@@ -1087,7 +1098,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
                     ang_reg_bits |= 1u << k;
                 } else {
                     ang_thr[thr].push_back({outer, th});
-                    if (thr) dirty = 1;
+                    dirty |= (uint32_t)thr;
                 }
                 ++ang_pending;
                 return true;
@@ -1095,7 +1106,7 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         }
         if (o.cond_reg == 0) {  // thread-only: joins the pending factor
             o.code = PC_DIAG_T;
-            if (o.cond_lane || o.cond_warp) dirty = 1;
+            dirty |= (uint32_t)(o.tmask & ((1ull << (LANE_BITS + WARP_BITS)) - 1));
             tm.push_back({o, d});
             return true;
         }
@@ -1559,13 +1570,15 @@ int run_pass_built(qoa_state_t s, const PassParams& P, const JitKernel& jk) {
     const bool c64 = s->precision == QOA_PREC_F32;
     {
         Timer tm(s, 2.0 * std::ldexp(c64 ? 8.0 : 16.0, (int)s->n), c64 ? 3 : 0);
+        cudaError_t je = cudaErrorNotReady;
         if (jk.ready()) {
-            CK(jk.launch(s->amps, P, s->scal, s->partials, s->stream));
-            s->jit_launches++;
-        } else if (c64) {
-            CK(launch_pass_p32((float2*)s->amps, P, s->scal, s->partials, s->stream));
-        } else {
-            CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
+            je = jk.launch(s->amps, P, s->scal, s->partials, s->status + 3, s->stream);
+            if (je == cudaSuccess) s->jit_launches++;
+            else if (je != cudaErrorNotSupported) CK(je);
+        }
+        if (je != cudaSuccess) {  // not compiled yet, or its launch set-up unavailable: the interpreter
+            if (c64) CK(launch_pass_p32((float2*)s->amps, P, s->scal, s->partials, s->stream));
+            else CK(launch_pass(s->amps, P, s->scal, s->partials, s->stream));
         }
     }
     CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
@@ -1833,7 +1846,8 @@ int execute(qoa_state_t s, std::vector<Gate>& G) {
         if (fresh) {
             // the plan depends on the op list and the size only, so a list
             // executed again gives bit-identical results
-            pe->steps = schedule(seg, s->n, per_gate, false, state_pass_budget(s), slot_search_pays(s->n));
+            pe->steps = schedule(seg, s->n, per_gate, false, state_pass_budget(s),
+                                 slot_search_pays(s->n) || (s->flags & QOA_FLAG_SLOT_SEARCH));
             pe->built_of.assign(pe->steps.size(), -1);
             // tile passes of a large state: built ahead, and their generated
             // kernels requested from the compile cache
@@ -2887,7 +2901,7 @@ int qoa_status(qoa_state_t s, qoa_status_t* out) {
     out->nan_seen = h[0];
     out->inf_seen = h[1];
     out->zero_norm_resets = h[2] + s->host_resets;
-    out->reserved = 0;
+    out->copy_timeouts = h[3];
     return QOA_OK;
 }
 

@@ -48,6 +48,10 @@ const char kDev32Header[] =
 #include "qoa_pass32_dev.cuh.inc"
     ;
 
+// Marker of the streamed form in a kernel body (launch and compile options
+// depend on it).
+const char kStreamMark[] = "/*qoa:streamed*/";
+
 // NVRTC has no C library headers: the fixed-width types the headers use.
 const char kPrelude[] =
     "typedef unsigned char uint8_t;\n"
@@ -70,6 +74,14 @@ int occ_target(bool c64) {
     if (!v) return d;
     const int k = atoi(v);
     return (k >= 1 && k <= 16) ? k : d;
+}
+
+// Resident CTAs per SM of a streamed pass (two 32 KB tile buffers each):
+// QOA_JIT_OCC_STREAMED overrides.
+int occ_streamed() {
+    const char* v = getenv("QOA_JIT_OCC_STREAMED");
+    const int k = v ? atoi(v) : 3;
+    return (k >= 1 && k <= 3) ? k : 3;
 }
 
 uint32_t spos_host(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
@@ -343,37 +355,10 @@ void emit_head(Emit& E, const PassParams& P, bool c64, bool arena) {
     if (P.nang) E.line("pass_angles(P, blk, sang);");
 }
 
-std::string jit_pass_body(const PassParams& P, bool arena) {
-    Emit E;
-    // complex128 coefficients: the parameter's constant bank, or the staged copy
-    const char* cf = arena ? "scoef" : "P.coef";
-    emit_head(E, P, false, arena);
-    E.line("const bool valid = nrm > 1e-12;");
-    E.line("T pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;");
-    E.line("T a[REGS];");
-    auto stride = [&](int t) -> unsigned long long {
-        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
-    };
-    {
-        const TileMap& m = P.map0;
-        E.line("{");
-        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
-               stride(m.warp[0]), stride(m.warp[1]));
-        unsigned long long off[REGS];
-        for (int v = 0; v < REGS; ++v) {
-            off[v] = 0;
-            for (int k = 0; k < REG_BITS; ++k)
-                if ((v >> k) & 1) off[v] += stride(m.reg[k]);
-        }
-        E.line("if (valid) {");
-        for (int v = 0; v < REGS; ++v) E.line("a[%d] = __ldcs(amps + (tb + 0x%llxull));", v, off[v]);
-        E.line("} else {");
-        for (int v = 0; v < REGS; ++v) E.line("a[%d] = make_double2(tb + 0x%llxull == 0 ? 1.0 : 0.0, 0.0);", v, off[v]);
-        E.line("}");
-        E.line("}");
-    }
-    if (P.nang || arena) E.line("__syncthreads();");
-
+// The op stream of a complex128 pass (gates, diagonal factors, exchanges
+// through the shared-memory array `tile`), emitted as straight-line code;
+// returns the mapping in force at its end.
+const TileMap* emit_ops128(Emit& E, const PassParams& P, bool arena, const char* cf) {
     // one exchange layout for the whole pass where one exists
     Swizzle zp;
     bool shared_layout = false;
@@ -500,6 +485,174 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
             }
         }
     }
+
+    return cur;
+}
+
+// The single-state complex128 pass as a persistent kernel: CTA b runs tiles
+// b, b + gridDim.x, ... Each tile arrives by bulk copies into one of two
+// shared-memory buffers while the previous tile is computed (that buffer
+// then serves the tile's exchanges); the tile's rows are its 64 runs of 32
+// consecutive amplitudes (lanes = qubits 0..4), merged into longer runs
+// where the lowest high slots are qubits 5, 6, ... The results are stored
+// from registers as in k_pass, with the same arithmetic, so a streamed pass
+// is bit-identical to k_pass.
+std::string jit_pass_body_streamed(const PassParams& P) {
+    Emit E;
+    const int lt = (int)P.n - TILE_BITS;
+    E.line("(double2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
+    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials, uint32_t* __restrict__ status) {");
+    E.line("%s", kStreamMark);
+    E.line("using namespace qoa;");
+    E.line("typedef double2 T;");
+    E.line("extern __shared__ __align__(128) unsigned char qoa_dsm[];");
+    E.line("__shared__ __align__(8) uint64_t mbar[2];");
+    E.line("__shared__ double red[PASS_THREADS / 32];");
+    if (P.nang) E.line("__shared__ T sang[%u];", P.nang);
+    E.line("const int lane = threadIdx.x & 31;");
+    E.line("const int wid = threadIdx.x >> 5;");
+    E.line("const double nrm = *norm2_in;");
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("const uint64_t ntiles = 1ull << %d;", lt);
+    // tile origin of tile number b: its bits deposited into the outer qubits
+    {
+        std::string g = "0ull";
+        char b[128];
+        for (int k = 0; k < lt;) {
+            int len = 1;
+            while (k + len < lt && P.outer_qubits[k + len] == P.outer_qubits[k] + len) ++len;
+            snprintf(b, sizeof b, " | (((b >> %d) & 0x%llxull) << %d)", k,
+                     (unsigned long long)((len >= 64) ? ~0ull : ((1ull << len) - 1)), P.outer_qubits[k]);
+            g += b;
+            k += len;
+        }
+        E.line("auto origin = [](uint64_t b) -> uint64_t { return %s; };", g.c_str());
+    }
+    // rows of a tile: the lowest r high slots on qubits 5 .. 4 + r make runs
+    // of 32 << r consecutive amplitudes, 64 >> r runs per tile
+    int r = 0;
+    while (r < HIGH_SLOTS && P.slot_qubit[r] == LANE_BITS + r) ++r;
+    const int nrun = 64 >> r;
+    const unsigned run_bytes = (unsigned)(16u * (32u << r));
+    {
+        std::string off = "0ull";
+        char b[96];
+        for (int k = r; k < HIGH_SLOTS; ++k) {
+            snprintf(b, sizeof b, " + ((c & %uu) ? 0x%llxull : 0ull)", 1u << (k - r),
+                     (unsigned long long)(1ull << P.slot_qubit[k]));
+            off += b;
+        }
+        E.line("auto issue = [&](uint64_t b, int buf) {");
+        E.line("  uint64_t* mb = &mbar[buf];");
+        E.line("  T* dst = reinterpret_cast<T*>(qoa_dsm) + (buf << %d);", TILE_BITS);
+        E.line("  const uint64_t gq = origin(b);");
+        E.line("  if (lane == 0) mbar_expect_tx(mb, %uu);", 16u << TILE_BITS);
+        E.line("  __syncwarp();");
+        E.line("  for (uint32_t c = lane; c < %du; c += 32u)", nrun);
+        E.line("    bulk_load(dst + (c << %d), amps + (gq + %s), %uu, mb);", 5 + r, off.c_str(), run_bytes);
+        E.line("};");
+    }
+    E.line("if (threadIdx.x == 0) { mbar_init(&mbar[0], 1); mbar_init(&mbar[1], 1); mbar_init_fence(); }");
+    E.line("__syncthreads();");
+    E.line("if (valid && wid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);");
+    E.line("uint32_t it = 0;");
+    E.line("for (uint64_t blk = blockIdx.x; blk < ntiles; blk += gridDim.x, ++it) {");
+    E.line("T* const tile = reinterpret_cast<T*>(qoa_dsm) + ((it & 1u) << %d);", TILE_BITS);
+    E.line("const uint64_t g0 = origin(blk);");
+    E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
+           LANE_BITS + WARP_BITS);
+    if (P.nang) E.line("pass_angles(P, blk, sang);");
+    E.line("T pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;");
+    E.line("T a[REGS];");
+    {
+        const TileMap& m = P.map0;
+        unsigned joff[REGS];
+        for (int v = 0; v < REGS; ++v) {
+            joff[v] = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) joff[v] |= 1u << m.reg[k];
+        }
+        auto stride = [&](int t) -> unsigned long long {
+            return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+        };
+        E.line("if (valid) {");
+        E.line("mbar_wait(&mbar[it & 1u], (it >> 1) & 1u, status);");
+        E.line("const uint32_t jb = (uint32_t)lane | ((wid & 1) ? %uu : 0u) | ((wid & 2) ? %uu : 0u);",
+               1u << m.warp[0], 1u << m.warp[1]);
+        for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[jb | %uu];", v, joff[v]);
+        E.line("} else {");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        for (int v = 0; v < REGS; ++v) {
+            unsigned long long off = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) off += stride(m.reg[k]);
+            E.line("a[%d] = make_double2(tb + 0x%llxull == 0 ? 1.0 : 0.0, 0.0);", v, off);
+        }
+        E.line("}");
+    }
+    // every thread is done with both buffers' previous contents: the next
+    // tile may now arrive in the other one
+    E.line("proxy_fence_async();");
+    E.line("__syncthreads();");
+    E.line("if (valid && wid == 0 && blk + gridDim.x < ntiles) issue(blk + gridDim.x, (int)((it + 1u) & 1u));");
+
+    const TileMap* cur = emit_ops128(E, P, false, "P.coef");
+
+    {
+        const TileMap& m = *cur;
+        auto ostride = [&](int t) -> unsigned long long { return 1ull << P.out_qubit[t]; };
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               ostride(m.warp[0]), ostride(m.warp[1]));
+        E.line("double ss = 0.0;");
+        for (int v = 0; v < REGS; ++v) {
+            unsigned long long off = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) off += ostride(m.reg[k]);
+            E.line("{ const T x = c_mul(a[%d], pend); __stcs(amps + (tb + 0x%llxull), x); ss += c_abs2(x); }", v, off);
+        }
+        E.line("block_norm_partial(ss, red, partials + blk);");
+        E.line("}");
+    }
+    E.line("}");  // tile loop
+    E.line("}");
+    return E.s;
+}
+
+std::string jit_pass_body(const PassParams& P, bool arena) {
+    if (!arena && !getenv("QOA_JIT_UNSTREAMED")) return jit_pass_body_streamed(P);
+    Emit E;
+    // complex128 coefficients: the parameter's constant bank, or the staged copy
+    const char* cf = arena ? "scoef" : "P.coef";
+    emit_head(E, P, false, arena);
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("T pend = valid ? make_double2(P.phase.x / sqrt(nrm), P.phase.y / sqrt(nrm)) : P.phase;");
+    E.line("T a[REGS];");
+    auto stride = [&](int t) -> unsigned long long {
+        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+    };
+    {
+        const TileMap& m = P.map0;
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        unsigned long long off[REGS];
+        for (int v = 0; v < REGS; ++v) {
+            off[v] = 0;
+            for (int k = 0; k < REG_BITS; ++k)
+                if ((v >> k) & 1) off[v] += stride(m.reg[k]);
+        }
+        E.line("if (valid) {");
+        for (int v = 0; v < REGS; ++v) E.line("a[%d] = __ldcs(amps + (tb + 0x%llxull));", v, off[v]);
+        E.line("} else {");
+        for (int v = 0; v < REGS; ++v) E.line("a[%d] = make_double2(tb + 0x%llxull == 0 ? 1.0 : 0.0, 0.0);", v, off[v]);
+        E.line("}");
+        E.line("}");
+    }
+    if (P.nang || arena) E.line("__syncthreads();");
+
+    const TileMap* cur = emit_ops128(E, P, arena, cf);
 
     // store under the final mapping: tile bit t goes to qubit out_qubit[t]
     {
@@ -770,17 +923,60 @@ struct JitEntry {
     std::atomic<int> state{0};  // 0 compiling, 1 ready, 2 failed
     cudaKernel_t kernel = nullptr;
     std::string name;
+    bool streamed = false;  // persistent double-buffered form (jit_pass_body_streamed)
+    // streamed form, per device: dynamic shared memory allowed and the
+    // persistent grid (SMs x resident CTAs), set at the first launch there
+    std::mutex setup_mu;
+    uint64_t setup_devices = 0;
+    unsigned grid[64] = {};
 };
+
+namespace {
+constexpr unsigned kStreamSmem = 2u * (16u << TILE_BITS);  // two complex128 tiles
+
+// Grid of a streamed kernel on the current device (0: cannot launch).
+unsigned streamed_grid(JitEntry& e) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::lock_guard<std::mutex> lk(e.setup_mu);
+    if (!((e.setup_devices >> dev) & 1)) {
+        const void* f = reinterpret_cast<const void*>(e.kernel);
+        int occ = 0, nsm = 0;
+        if (cudaKernelSetAttributeForDevice(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem,
+                                            dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, PASS_THREADS, kStreamSmem) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || occ < 1) {
+            cudaGetLastError();
+            return 0;
+        }
+        e.grid[dev] = (unsigned)(occ * nsm);
+        e.setup_devices |= 1ull << dev;
+    }
+    return e.grid[dev];
+}
+}  // namespace
 
 bool JitKernel::ready() const { return e_ && e_->state.load(std::memory_order_acquire) == 1; }
 bool JitKernel::failed() const { return !e_ || e_->state.load(std::memory_order_acquire) == 2; }
 
 cudaError_t JitKernel::launch(void* amps, const PassParams& P, const double* norm2_in, double* partials,
-                              cudaStream_t st) const {
+                              uint32_t* status, cudaStream_t st) const {
     if (!ready()) return cudaErrorNotReady;
+    const unsigned tiles = 1u << (P.n - TILE_BITS);
+    if (e_->streamed) {
+        unsigned g = streamed_grid(*e_);
+        if (!g) return cudaErrorNotSupported;  // the caller runs the pass on k_pass instead
+        // QOA_JIT_STREAM_GRID caps the persistent grid (tests: many tiles per CTA)
+        if (const char* v = getenv("QOA_JIT_STREAM_GRID")) {
+            const int cap = atoi(v);
+            if (cap > 0 && (unsigned)cap < g) g = (unsigned)cap;
+        }
+        void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials, &status};
+        return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(std::min(g, tiles)),
+                                dim3(PASS_THREADS), args, kStreamSmem, st);
+    }
     void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials};
-    const unsigned blocks = 1u << (P.n - TILE_BITS);
-    return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(blocks), dim3(PASS_THREADS), args, 0, st);
+    return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(tiles), dim3(PASS_THREADS), args, 0, st);
 }
 
 cudaError_t JitKernel::launch_arena(const ArenaJob* jobs, uint32_t njobs, uint32_t lt, cudaStream_t st) const {
@@ -811,8 +1007,9 @@ std::string program_text(const std::vector<std::string>& names, const std::vecto
     char head[160];
     for (size_t i = 0; i < names.size(); ++i) {
         const bool c64 = body_is_c64(bodies[i]);
+        const bool streamed = bodies[i].find(kStreamMark) != std::string::npos;
         snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS,
-                 occ_target(c64), names[i].c_str());
+                 streamed ? occ_streamed() : occ_target(c64), names[i].c_str());
         src += head;
         src += bodies[i];
     }
@@ -972,6 +1169,7 @@ public:
                 ++misses_;
                 auto e = std::make_shared<JitEntry>();
                 e->name = kernel_name(b);
+                e->streamed = b.find(kStreamMark) != std::string::npos;
                 cache_.emplace(key, e);
                 queue_.push_back(JitJob{e, b});
                 ++pending_;

@@ -28,11 +28,13 @@ public:
     explicit JitKernel(std::shared_ptr<JitEntry> e) : e_(std::move(e)) {}
     bool ready() const;
     bool failed() const;
-    // Launches the pass over the state (grid 2^(n - TILE_BITS)); the same
-    // arguments as k_pass.
+    // Launches the pass over the state: the same arguments as k_pass, plus
+    // the handle's status words (a streamed pass sets bit 0 of status[0]
+    // when a tile copy did not arrive in time). Grid 2^(n - TILE_BITS), or
+    // for the streamed form one persistent CTA per resident slot.
     // amps: double2* (complex128 kernels) or float2* (complex64 kernels).
     cudaError_t launch(void* amps, const PassParams& P, const double* norm2_in, double* partials,
-                       cudaStream_t st) const;
+                       uint32_t* status, cudaStream_t st) const;
     // Arena form: njobs device ArenaJob records from `jobs`, 2^lt tiles each.
     cudaError_t launch_arena(const ArenaJob* jobs, uint32_t njobs, uint32_t lt, cudaStream_t st) const;
 

@@ -1,9 +1,9 @@
 // qoa_kernels.cu — sm_100a kernels of the state-vector engine.
 //
 // Hot path: k_pass, one HBM read + write of the whole state for a run of gates
-// whose non-diagonal targets fall inside a 12-qubit tile (5 lane qubits that
-// keep every warp access 512 contiguous bytes, 4 register qubits, 3 warp
-// qubits). It replaces the per-gate sweeps of src/vectorization.rs:915-1260
+// whose non-diagonal targets fall inside an 11-qubit tile (5 lane qubits that
+// keep every warp access 512 contiguous bytes, 4 register qubits, 2 warp
+// qubits; TILE_BITS, REG_BITS and WARP_BITS in qoa_kernels.cuh). It replaces the per-gate sweeps of src/vectorization.rs:915-1260
 // plus the two normalize() sweeps that follow every gate
 // (src/runtime/quantum_state.rs:839-907): the pass scales its input by the
 // pending 1/||psi|| and leaves per-CTA partial sums of |a|^2 for the next one.

@@ -14,6 +14,13 @@
 // call's contents. Each launch writes every partial it later reads, so nothing
 // in it has to start at zero. Calls whose kernels overlap on the GPU (two
 // streams, or two host threads) race on it; the caller must order them.
+//
+// A __device__ array has one address per CUDA context, not per device: a
+// caller may run in a context of its own (cuCtxCreate) beside the primary
+// one, and cudaDeviceReset replaces the primary context. The resolved
+// address is therefore cached by the current context's id (cuCtxGetId, unique
+// for the life of the process), not by device number.
+#include <cuda.h>  // CUcontext / CUresult types only; the two driver calls are resolved at run time
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -28,7 +35,7 @@ void note_global_error(const char* msg);
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 148 * 8;                    // partials per mask
 constexpr int kMaxMasks = QOA_NOALLOC_MAX_MASKS;       // masks per call
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;                       // cached (context id, address) pairs
 
 // The scratch: 8 masks x 1184 blocks x 8 bytes = 75,776 bytes on every device
 // that loads the library, held until the process exits.
@@ -40,28 +47,30 @@ struct Masks {
     uint64_t m[kMaxMasks];
 };
 
-__global__ void k_expz_partials_noalloc(const double2* __restrict__ a, uint64_t len, const Masks mk, uint32_t k,
+// K masks (1..8), so a call with fewer masks accumulates only those.
+template <int K>
+__global__ void k_expz_partials_noalloc(const double2* __restrict__ a, uint64_t len, const Masks mk,
                                         double* __restrict__ partials) {
-    __shared__ double sh[kMaxMasks][kThreads / 32];
-    double v[kMaxMasks];
+    __shared__ double sh[K][kThreads / 32];
+    double v[K];
 #pragma unroll
-    for (int j = 0; j < kMaxMasks; ++j) v[j] = 0.0;
+    for (int j = 0; j < K; ++j) v[j] = 0.0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
         const double2 x = a[i];
         const double p = fma(x.x, x.x, x.y * x.y);
 #pragma unroll
-        for (int j = 0; j < kMaxMasks; ++j) v[j] += (__popcll(i & mk.m[j]) & 1) ? -p : p;
+        for (int j = 0; j < K; ++j) v[j] += (__popcll(i & mk.m[j]) & 1) ? -p : p;
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < kMaxMasks; ++j) {
+    for (int j = 0; j < K; ++j) {
         double x = v[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
         if (lane == 0) sh[j][w] = x;
     }
     __syncthreads();
-    if (threadIdx.x < k) {
+    if (threadIdx.x < K) {
         double t = 0.0;
         for (int q = 0; q < kThreads / 32; ++q) t += sh[threadIdx.x][q];
         partials[(uint64_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
@@ -85,8 +94,67 @@ __global__ void k_expz_reduce_noalloc(const double* __restrict__ partials, uint3
     }
 }
 
+const void* const kPartials[kMaxMasks + 1] = {
+    nullptr,
+    (const void*)k_expz_partials_noalloc<1>, (const void*)k_expz_partials_noalloc<2>,
+    (const void*)k_expz_partials_noalloc<3>, (const void*)k_expz_partials_noalloc<4>,
+    (const void*)k_expz_partials_noalloc<5>, (const void*)k_expz_partials_noalloc<6>,
+    (const void*)k_expz_partials_noalloc<7>, (const void*)k_expz_partials_noalloc<8>,
+};
+
+// The current context's unique id, through driver entry points the runtime
+// hands out (no link against libcuda). False when unavailable or when no
+// context is current.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+bool current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? (CtxGetCurrentFn)f : nullptr;
+    }();
+    static CtxGetIdFn get_id = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess) ? (CtxGetIdFn)f : nullptr;
+    }();
+    CUcontext c = nullptr;
+    if (!get_current || !get_id || get_current(&c) != CUDA_SUCCESS || !c) return false;
+    return get_id(c, id) == CUDA_SUCCESS;
+}
+
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    double* ptr;
+};
 std::mutex g_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+ScratchSlot g_slots[kMaxContexts];
+int g_nslots = 0;
+
+// Device address of g_expz_scratch in the current context: cached per
+// context id; resolved with cudaGetSymbolAddress on a context's first call
+// (and on every call if the context id cannot be read).
+cudaError_t scratch_address(double** out) {
+    unsigned long long id = 0;
+    bool have = current_context_id(&id);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (have)
+        for (int i = 0; i < g_nslots; ++i)
+            if (g_slots[i].ctx_id == id) {
+                *out = g_slots[i].ptr;
+                return cudaSuccess;
+            }
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_expz_scratch);
+    if (e != cudaSuccess || !p) return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
+    if (!have) have = current_context_id(&id);  // the runtime may have just made its context current
+    if (have && g_nslots < kMaxContexts) g_slots[g_nslots++] = {id, p};
+    *out = p;
+    return cudaSuccess;
+}
 
 }  // namespace
 
@@ -103,35 +171,35 @@ extern "C" int qoa_expect_z_noalloc(const void* d_amps, size_t len, const uint64
     }
     if (k == 0 || len == 0) return QOA_OK;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         qoa::note_global_error("qoa_expect_z_noalloc: no usable current CUDA device");
         return QOA_E_NOGPU;
     }
-    // Set-up, once per device with that device current: the host-side name of
-    // g_expz_scratch is not a device address, so resolve the real one.
-    double* scratch;
-    {
-        std::lock_guard<std::mutex> lk(g_mu);
-        scratch = g_scratch_ptr[dev];
-        if (!scratch) {
-            const cudaError_t e = cudaGetSymbolAddress((void**)&scratch, g_expz_scratch);
-            if (e != cudaSuccess || !scratch) {
-                qoa::note_global_error("qoa_expect_z_noalloc: cudaGetSymbolAddress of the scratch array failed");
-                return QOA_E_CUDA;
-            }
-            g_scratch_ptr[dev] = scratch;
-        }
+    // Set-up on a context's first call: the host-side name of g_expz_scratch
+    // is not a device address, so resolve the real one (cached per context).
+    double* scratch = nullptr;
+    if (scratch_address(&scratch) != cudaSuccess) {
+        qoa::note_global_error("qoa_expect_z_noalloc: cudaGetSymbolAddress of the scratch array failed");
+        return QOA_E_CUDA;
     }
     cudaStream_t st = (cudaStream_t)stream;
     uint64_t nb = (len + kThreads - 1) / kThreads;
     if (nb > (uint64_t)kMaxBlocks) nb = kMaxBlocks;
     Masks mk{};
     for (size_t j = 0; j < k; ++j) mk.m[j] = masks[j];
-    k_expz_partials_noalloc<<<(unsigned)nb, kThreads, 0, st>>>((const double2*)d_amps, (uint64_t)len, mk, (uint32_t)k,
-                                                               scratch);
-    k_expz_reduce_noalloc<<<(unsigned)k, 1024, 0, st>>>(scratch, (uint32_t)nb, d_out);
-    const cudaError_t e = cudaGetLastError();
+    const double2* a = (const double2*)d_amps;
+    uint64_t len64 = (uint64_t)len;
+    uint32_t count = (uint32_t)nb;
+    // Each launch's own status (cudaLaunchKernel returns it), so an error
+    // left pending by the caller's earlier work is neither reported nor cleared.
+    void* pargs[] = {(void*)&a, (void*)&len64, (void*)&mk, (void*)&scratch};
+    cudaError_t e = cudaLaunchKernel(kPartials[k], dim3((unsigned)nb), dim3(kThreads), pargs, 0, st);
+    if (e == cudaSuccess) {
+        void* rargs[] = {(void*)&scratch, (void*)&count, (void*)&d_out};
+        e = cudaLaunchKernel((const void*)k_expz_reduce_noalloc, dim3((unsigned)k), dim3(1024), rargs, 0, st);
+    }
     if (e != cudaSuccess) {
+        cudaGetLastError();  // this call's own launch error
         qoa::note_global_error(cudaGetErrorString(e));
         return QOA_E_CUDA;
     }

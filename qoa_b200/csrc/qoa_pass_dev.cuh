@@ -150,6 +150,70 @@ __device__ __forceinline__ void pass_angles(const PassParams& P, const uint64_t 
     }
 }
 
+// ------------------------------------------ streamed tiles (generated passes)
+// A persistent pass CTA walks tiles blockIdx.x, +gridDim.x, ... and keeps two
+// shared-memory tile buffers: while it computes one tile (that buffer also
+// serves the tile's exchanges) the next tile arrives in the other by bulk
+// copies (cp.async.bulk, this GPU's own memory, no multicast) that complete
+// on the buffer's mbarrier.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* mb, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// the issuing thread's arrival, announcing `bytes` of copies to come
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)), "r"(bytes)
+                 : "memory");
+}
+// `bytes` (a multiple of 16, both addresses 16-byte aligned) from global
+// memory into shared memory, counted on mbarrier mb
+__device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, uint32_t bytes, uint64_t* mb) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst_smem)),
+        "l"(src), "r"(bytes), "r"(smem_u32(mb))
+        : "memory");
+}
+// orders this thread's generic shared-memory accesses before later bulk
+// copies into the same memory
+__device__ __forceinline__ void proxy_fence_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for phase `parity` of mb to complete, for at most ~2 s: past that it
+// sets bit 0 of *status (the pass's data is then not valid) and returns
+// false, so that a lost copy never hangs the GPU.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, uint32_t parity, uint32_t* status) {
+    const uint32_t a = smem_u32(mb);
+    uint64_t t0 = 0;
+    for (uint32_t i = 0;; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255u) == 0) {
+            const uint64_t t = global_ns();
+            if (i == 0) t0 = t;
+            else if (t - t0 > 2000000000ull) {
+                atomicOr(status, 1u);
+                return false;
+            }
+        }
+    }
+}
+
 // Sum of the block's per-thread squared norms into *out (thread 0 writes).
 __device__ __forceinline__ void block_norm_partial(double ss, double* red, double* out) {
     const int lane = threadIdx.x & 31;

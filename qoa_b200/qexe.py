@@ -13,7 +13,7 @@ from typing import Iterable, List, Optional, Tuple
 
 import numpy as np
 
-from . import OP_DTYPE, QoaError, _check, lib
+from . import OP_DTYPE, QoaError, _check, lib, register_signatures
 
 MAGIC = {"qexe": b"QEXE", "oexe": b"OEXE", "qox": b"QOX ", "xexe": b"XEXE", "qex": b"QEX ", "qx": b"QX\0\0"}
 EXE_LOOPS = 0x1
@@ -213,14 +213,13 @@ class ExeResult(ctypes.Structure):
 
 
 _vp, _sz, _u32, _u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64
-lib.qoa_exe_parse.restype = ctypes.c_int
-lib.qoa_exe_parse.argtypes = [ctypes.c_char_p, _sz, ctypes.POINTER(ExeInfo)]
-lib.qoa_exe_run.restype = ctypes.c_int
-lib.qoa_exe_run.argtypes = [_vp, ctypes.c_char_p, _sz, _u32, _u64, ctypes.POINTER(ExeResult), ctypes.c_char_p, _sz,
-                            ctypes.POINTER(_sz)]
-lib.qoa_exe_trace.restype = ctypes.c_int
-lib.qoa_exe_trace.argtypes = [ctypes.c_char_p, _sz, _u32, _u64, _vp, _sz, ctypes.POINTER(_sz),
-                              ctypes.POINTER(ExeResult), ctypes.c_char_p, _sz, ctypes.POINTER(_sz)]
+register_signatures({
+    "qoa_exe_parse": (ctypes.c_int, [ctypes.c_char_p, _sz, ctypes.POINTER(ExeInfo)]),
+    "qoa_exe_run": (ctypes.c_int, [_vp, ctypes.c_char_p, _sz, _u32, _u64, ctypes.POINTER(ExeResult),
+                                   ctypes.c_char_p, _sz, ctypes.POINTER(_sz)]),
+    "qoa_exe_trace": (ctypes.c_int, [ctypes.c_char_p, _sz, _u32, _u64, _vp, _sz, ctypes.POINTER(_sz),
+                                     ctypes.POINTER(ExeResult), ctypes.c_char_p, _sz, ctypes.POINTER(_sz)]),
+})
 
 
 def parse(file: bytes) -> dict:

@@ -159,3 +159,20 @@ def test_repeated_op_lists_reuse_their_plans():
         assert np.array_equal(o.view(np.float64), outs[0].view(np.float64))
     ref = oracle_run(n, C.random_layered(n, 3, 61, initial_h=True), 1)
     assert rel_l2(outs[0], ref) < TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grid", ["1", "3", "7"])
+def test_streamed_passes_with_many_tiles_per_cta(monkeypatch, grid):
+    # the generated complex128 pass is persistent: each CTA walks tiles
+    # b, b + grid, ... with two shared-memory buffers whose copies complete
+    # on alternating mbarrier phases; a capped grid makes every CTA take
+    # many tiles (both buffers, both phases), still bit-identical to k_pass
+    monkeypatch.setenv("QOA_JIT_STREAM_GRID", grid)
+    n = 17
+    ops = C.random_layered(n, 6, 61, initial_h=True)
+    got_jit, st_jit = run(n, ops, qb.QOA_JIT_SYNC, True)
+    got_int, _ = run(n, ops, qb.QOA_JIT_OFF, True)
+    assert st_jit["launches"] > 0 and st_jit["failures"] == 0
+    assert np.array_equal(got_jit.view(np.float64), got_int.view(np.float64))
+    assert rel_l2(got_jit, oracle_run(n, ops, 1)) < TOL
