@@ -76,12 +76,13 @@ int occ_target(bool c64) {
     return (k >= 1 && k <= 16) ? k : d;
 }
 
-// Resident CTAs per SM of a streamed pass (two 32 KB tile buffers each):
-// QOA_JIT_OCC_STREAMED overrides.
-int occ_streamed() {
+// Resident CTAs per SM of a streamed pass (two tile buffers each: 64 KB for
+// complex128, 32 KB for complex64); QOA_JIT_OCC_STREAMED overrides.
+int occ_streamed(bool c64) {
+    const int d = c64 ? 6 : 3;
     const char* v = getenv("QOA_JIT_OCC_STREAMED");
-    const int k = v ? atoi(v) : 3;
-    return (k >= 1 && k <= 3) ? k : 3;
+    const int k = v ? atoi(v) : d;
+    return (k >= 1 && k <= d) ? k : d;
 }
 
 uint32_t spos_host(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
@@ -680,65 +681,10 @@ std::string jit_pass_body(const PassParams& P, bool arena) {
 // (pass_tile_p32) for the same PassParams. Registers hold re[j] / im[j] =
 // packed (amplitude j, amplitude j + 8); coefficients are rounded to float
 // once per CTA into shared memory, as the interpreter stages them.
-std::string jit_pass32_body(const PassParams& P, bool arena) {
-    Emit E;
-    emit_head(E, P, true, arena);
-    // register tables (PC_DIAG_TAB): staged once per CTA already packed as
-    // (factor j, factor j + 8) pairs, real parts then imaginary parts
-    std::vector<uint32_t> tab_at(P.nops, 0);
-    {
-        uint32_t ntab = 0;
-        for (uint32_t oi = 0; oi < P.nops; ++oi) {
-            const int code = P.ops[oi].code;
-            if (code == PC_DIAG_TAB) tab_at[oi] = ntab++;
-            if (code == PC_DIAG_MX || code == PC_DIAG_TM) oi += P.ops[oi].k;
-        }
-        if (ntab) {
-            E.line("__shared__ u64p stab[%u];", 16 * ntab);
-            for (uint32_t oi = 0; oi < P.nops; ++oi) {
-                const PassOp& op = P.ops[oi];
-                if (op.code == PC_DIAG_TAB) {
-                    const uint32_t t = tab_at[oi], c = op.coef;
-                    E.line("if (threadIdx.x < 8) { const int j = threadIdx.x; const double2 x = P.coef[%u + j], y = P.coef[%u + j];", c, c + 8);
-                    E.line("  stab[%u + j] = pk((float)x.x, (float)y.x); stab[%u + j] = pk((float)x.y, (float)y.y); }", 16 * t, 16 * t + 8);
-                }
-                if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) oi += op.k;
-            }
-        }
-    }
-    E.line("const bool valid = nrm > 1e-12;");
-    E.line("float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))");
-    E.line("                    : make_float2((float)P.phase.x, (float)P.phase.y);");
-    E.line("u64p re[8], im[8];");
-    auto stride = [&](int t) -> unsigned long long {
-        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
-    };
-    {
-        const TileMap& m = P.map0;
-        E.line("{");
-        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
-               stride(m.warp[0]), stride(m.warp[1]));
-        const unsigned long long r3 = stride(m.reg[3]);
-        E.line("if (valid) {");
-        for (int j = 0; j < 8; ++j) {
-            unsigned long long off = 0;
-            for (int k = 0; k < 3; ++k)
-                if ((j >> k) & 1) off += stride(m.reg[k]);
-            E.line("{ const float2 a = __ldcs(amps + (tb + 0x%llxull)), b = __ldcs(amps + (tb + 0x%llxull)); re[%d] = pk(a.x, b.x); im[%d] = pk(a.y, b.y); }",
-                   off, off + r3, j, j);
-        }
-        E.line("} else {");
-        for (int j = 0; j < 8; ++j) {
-            unsigned long long off = 0;
-            for (int k = 0; k < 3; ++k)
-                if ((j >> k) & 1) off += stride(m.reg[k]);
-            E.line("re[%d] = pk(tb + 0x%llxull == 0 ? 1.f : 0.f, 0.f); im[%d] = 0ull;", j, off, j);
-        }
-        E.line("}");
-        E.line("}");
-    }
-    E.line("__syncthreads();");
-
+// The op stream of a complex64 pass (packed FP32 registers re[8] / im[8],
+// coefficients in scoef, register tables in stab at tab_at[op]); returns
+// the mapping in force at its end.
+const TileMap* emit_ops64(Emit& E, const PassParams& P, bool arena, const std::vector<uint32_t>& tab_at) {
     // one pair-exchange layout for the whole pass, when every exchange keeps
     // the same pairing bit and one layout serves all of them
     Swizzle zp;
@@ -895,6 +841,223 @@ std::string jit_pass32_body(const PassParams& P, bool arena) {
             }
         }
     }
+    return cur;
+}
+
+// The single-state complex64 pass as a persistent kernel (the streamed
+// form of jit_pass_body_streamed for packed FP32 registers): coefficients
+// and register tables are staged once per CTA, tiles stream through two
+// 16 KB shared-memory buffers by bulk copies, results are stored from
+// registers with the same arithmetic as k_pass_p32.
+std::string jit_pass32_body_streamed(const PassParams& P) {
+    Emit E;
+    const int lt = (int)P.n - TILE_BITS;
+    E.line("(float2* __restrict__ amps, const __grid_constant__ qoa::PassParams P,");
+    E.line(" const double* __restrict__ norm2_in, double* __restrict__ partials, uint32_t* __restrict__ status) {");
+    E.line("%s", kStreamMark);
+    E.line("using namespace qoa;");
+    E.line("using namespace qoa::p32;");
+    E.line("typedef float2 T;");
+    E.line("extern __shared__ __align__(128) unsigned char qoa_dsm[];");
+    E.line("__shared__ __align__(8) uint64_t mbar[2];");
+    E.line("__shared__ double red[PASS_THREADS / 32];");
+    E.line("__shared__ __align__(16) T scoef[%u];", P.ncoef ? P.ncoef : 1);
+    if (P.nang) E.line("__shared__ T sang[%u];", P.nang);
+    E.line("const int lane = threadIdx.x & 31;");
+    E.line("const int wid = threadIdx.x >> 5;");
+    E.line("const double nrm = *norm2_in;");
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("const uint64_t ntiles = 1ull << %d;", lt);
+    E.line("for (uint32_t i = threadIdx.x; i < %uu; i += PASS_THREADS) scoef[i] = make_float2((float)P.coef[i].x, (float)P.coef[i].y);",
+           P.ncoef);
+    std::vector<uint32_t> tab_at(P.nops, 0);
+    {
+        uint32_t ntab = 0;
+        for (uint32_t oi = 0; oi < P.nops; ++oi) {
+            const int code = P.ops[oi].code;
+            if (code == PC_DIAG_TAB) tab_at[oi] = ntab++;
+            if (code == PC_DIAG_MX || code == PC_DIAG_TM) oi += P.ops[oi].k;
+        }
+        if (ntab) {
+            E.line("__shared__ u64p stab[%u];", 16 * ntab);
+            for (uint32_t oi = 0; oi < P.nops; ++oi) {
+                const PassOp& op = P.ops[oi];
+                if (op.code == PC_DIAG_TAB) {
+                    const uint32_t t = tab_at[oi], c = op.coef;
+                    E.line("if (threadIdx.x < 8) { const int j = threadIdx.x; const double2 x = P.coef[%u + j], y = P.coef[%u + j];", c, c + 8);
+                    E.line("  stab[%u + j] = pk((float)x.x, (float)y.x); stab[%u + j] = pk((float)x.y, (float)y.y); }", 16 * t, 16 * t + 8);
+                }
+                if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) oi += op.k;
+            }
+        }
+    }
+    {
+        std::string g = "0ull";
+        char b[128];
+        for (int k = 0; k < lt;) {
+            int len = 1;
+            while (k + len < lt && P.outer_qubits[k + len] == P.outer_qubits[k] + len) ++len;
+            snprintf(b, sizeof b, " | (((b >> %d) & 0x%llxull) << %d)", k,
+                     (unsigned long long)((len >= 64) ? ~0ull : ((1ull << len) - 1)), P.outer_qubits[k]);
+            g += b;
+            k += len;
+        }
+        E.line("auto origin = [](uint64_t b) -> uint64_t { return %s; };", g.c_str());
+    }
+    int r = 0;
+    while (r < HIGH_SLOTS && P.slot_qubit[r] == LANE_BITS + r) ++r;
+    const int nrun = 64 >> r;
+    const unsigned run_bytes = (unsigned)(8u * (32u << r));
+    {
+        std::string off = "0ull";
+        char b[96];
+        for (int k = r; k < HIGH_SLOTS; ++k) {
+            snprintf(b, sizeof b, " + ((c & %uu) ? 0x%llxull : 0ull)", 1u << (k - r),
+                     (unsigned long long)(1ull << P.slot_qubit[k]));
+            off += b;
+        }
+        E.line("auto issue = [&](uint64_t b, int buf) {");
+        E.line("  uint64_t* mb = &mbar[buf];");
+        E.line("  T* dst = reinterpret_cast<T*>(qoa_dsm) + (buf << %d);", TILE_BITS);
+        E.line("  const uint64_t gq = origin(b);");
+        E.line("  if (lane == 0) mbar_expect_tx(mb, %uu);", 8u << TILE_BITS);
+        E.line("  __syncwarp();");
+        E.line("  for (uint32_t c = lane; c < %du; c += 32u)", nrun);
+        E.line("    bulk_load(dst + (c << %d), amps + (gq + %s), %uu, mb);", 5 + r, off.c_str(), run_bytes);
+        E.line("};");
+    }
+    E.line("if (threadIdx.x == 0) { mbar_init(&mbar[0], 1); mbar_init(&mbar[1], 1); mbar_init_fence(); }");
+    E.line("__syncthreads();");
+    E.line("if (valid && wid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);");
+    E.line("uint32_t it = 0;");
+    E.line("for (uint64_t blk = blockIdx.x; blk < ntiles; blk += gridDim.x, ++it) {");
+    E.line("T* const tile = reinterpret_cast<T*>(qoa_dsm) + ((it & 1u) << %d);", TILE_BITS);
+    E.line("const uint64_t g0 = origin(blk);");
+    E.line("const uint32_t tw = (uint32_t)lane | ((uint32_t)wid << %d) | ((uint32_t)blk << %d);", LANE_BITS,
+           LANE_BITS + WARP_BITS);
+    if (P.nang) E.line("pass_angles(P, blk, sang);");
+    E.line("float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))");
+    E.line("                    : make_float2((float)P.phase.x, (float)P.phase.y);");
+    E.line("u64p re[8], im[8];");
+    {
+        const TileMap& m = P.map0;
+        auto stride = [&](int t) -> unsigned long long {
+            return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+        };
+        E.line("if (valid) {");
+        E.line("mbar_wait(&mbar[it & 1u], (it >> 1) & 1u, status);");
+        E.line("const uint32_t jb = (uint32_t)lane | ((wid & 1) ? %uu : 0u) | ((wid & 2) ? %uu : 0u);",
+               1u << m.warp[0], 1u << m.warp[1]);
+        const unsigned j3 = 1u << m.reg[3];
+        for (int j = 0; j < 8; ++j) {
+            unsigned off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off |= 1u << m.reg[k];
+            E.line("{ const float2 a = tile[jb | %uu], b = tile[jb | %uu]; re[%d] = pk(a.x, b.x); im[%d] = pk(a.y, b.y); }",
+                   off, off | j3, j, j);
+        }
+        E.line("} else {");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += stride(m.reg[k]);
+            E.line("re[%d] = pk(tb + 0x%llxull == 0 ? 1.f : 0.f, 0.f); im[%d] = 0ull;", j, off, j);
+        }
+        E.line("}");
+    }
+    E.line("proxy_fence_async();");
+    E.line("__syncthreads();");
+    E.line("if (valid && wid == 0 && blk + gridDim.x < ntiles) issue(blk + gridDim.x, (int)((it + 1u) & 1u));");
+
+    const TileMap* cur = emit_ops64(E, P, false, tab_at);
+
+    {
+        const TileMap& m = *cur;
+        auto ostride = [&](int t) -> unsigned long long { return 1ull << P.out_qubit[t]; };
+        E.line("{");
+        E.line("const u64p cr = bc(pend.x), ci = bc(pend.y);");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               ostride(m.warp[0]), ostride(m.warp[1]));
+        const unsigned long long r3 = ostride(m.reg[3]);
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += ostride(m.reg[k]);
+            E.line("{ cmul2(re[%d], im[%d], cr, ci); const float2 a = make_float2(lo(re[%d]), lo(im[%d])), b = make_float2(hi(re[%d]), hi(im[%d]));",
+                   j, j, j, j, j, j);
+            E.line("  __stcs(amps + (tb + 0x%llxull), a); __stcs(amps + (tb + 0x%llxull), b); }", off, off + r3);
+        }
+        E.line("block_norm_partial(norm2_p(re, im), red, partials + blk);");
+        E.line("}");
+    }
+    E.line("}");  // tile loop
+    E.line("}");
+    return E.s;
+}
+
+std::string jit_pass32_body(const PassParams& P, bool arena) {
+    if (!arena && !getenv("QOA_JIT_UNSTREAMED")) return jit_pass32_body_streamed(P);
+    Emit E;
+    emit_head(E, P, true, arena);
+    // register tables (PC_DIAG_TAB): staged once per CTA already packed as
+    // (factor j, factor j + 8) pairs, real parts then imaginary parts
+    std::vector<uint32_t> tab_at(P.nops, 0);
+    {
+        uint32_t ntab = 0;
+        for (uint32_t oi = 0; oi < P.nops; ++oi) {
+            const int code = P.ops[oi].code;
+            if (code == PC_DIAG_TAB) tab_at[oi] = ntab++;
+            if (code == PC_DIAG_MX || code == PC_DIAG_TM) oi += P.ops[oi].k;
+        }
+        if (ntab) {
+            E.line("__shared__ u64p stab[%u];", 16 * ntab);
+            for (uint32_t oi = 0; oi < P.nops; ++oi) {
+                const PassOp& op = P.ops[oi];
+                if (op.code == PC_DIAG_TAB) {
+                    const uint32_t t = tab_at[oi], c = op.coef;
+                    E.line("if (threadIdx.x < 8) { const int j = threadIdx.x; const double2 x = P.coef[%u + j], y = P.coef[%u + j];", c, c + 8);
+                    E.line("  stab[%u + j] = pk((float)x.x, (float)y.x); stab[%u + j] = pk((float)x.y, (float)y.y); }", 16 * t, 16 * t + 8);
+                }
+                if (op.code == PC_DIAG_MX || op.code == PC_DIAG_TM) oi += op.k;
+            }
+        }
+    }
+    E.line("const bool valid = nrm > 1e-12;");
+    E.line("float2 pend = valid ? make_float2((float)(P.phase.x / sqrt(nrm)), (float)(P.phase.y / sqrt(nrm)))");
+    E.line("                    : make_float2((float)P.phase.x, (float)P.phase.y);");
+    E.line("u64p re[8], im[8];");
+    auto stride = [&](int t) -> unsigned long long {
+        return 1ull << (t < LANE_BITS ? t : P.slot_qubit[t - LANE_BITS]);
+    };
+    {
+        const TileMap& m = P.map0;
+        E.line("{");
+        E.line("const uint64_t tb = g0 + (uint64_t)lane + ((wid & 1) ? 0x%llxull : 0ull) + ((wid & 2) ? 0x%llxull : 0ull);",
+               stride(m.warp[0]), stride(m.warp[1]));
+        const unsigned long long r3 = stride(m.reg[3]);
+        E.line("if (valid) {");
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += stride(m.reg[k]);
+            E.line("{ const float2 a = __ldcs(amps + (tb + 0x%llxull)), b = __ldcs(amps + (tb + 0x%llxull)); re[%d] = pk(a.x, b.x); im[%d] = pk(a.y, b.y); }",
+                   off, off + r3, j, j);
+        }
+        E.line("} else {");
+        for (int j = 0; j < 8; ++j) {
+            unsigned long long off = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((j >> k) & 1) off += stride(m.reg[k]);
+            E.line("re[%d] = pk(tb + 0x%llxull == 0 ? 1.f : 0.f, 0.f); im[%d] = 0ull;", j, off, j);
+        }
+        E.line("}");
+        E.line("}");
+    }
+    E.line("__syncthreads();");
+
+    const TileMap* cur = emit_ops64(E, P, arena, tab_at);
     {
         const TileMap& m = *cur;
         auto ostride = [&](int t) -> unsigned long long { return 1ull << P.out_qubit[t]; };
@@ -923,7 +1086,8 @@ struct JitEntry {
     std::atomic<int> state{0};  // 0 compiling, 1 ready, 2 failed
     cudaKernel_t kernel = nullptr;
     std::string name;
-    bool streamed = false;  // persistent double-buffered form (jit_pass_body_streamed)
+    bool streamed = false;  // persistent double-buffered form (jit_pass*_body_streamed)
+    unsigned smem = 0;      // its dynamic shared memory (two tile buffers)
     // streamed form, per device: dynamic shared memory allowed and the
     // persistent grid (SMs x resident CTAs), set at the first launch there
     std::mutex setup_mu;
@@ -932,7 +1096,8 @@ struct JitEntry {
 };
 
 namespace {
-constexpr unsigned kStreamSmem = 2u * (16u << TILE_BITS);  // two complex128 tiles
+constexpr unsigned kStreamSmem = 2u * (16u << TILE_BITS);    // two complex128 tiles
+constexpr unsigned kStreamSmem32 = 2u * (8u << TILE_BITS);   // two complex64 tiles
 
 // Grid of a streamed kernel on the current device (0: cannot launch).
 unsigned streamed_grid(JitEntry& e) {
@@ -942,9 +1107,9 @@ unsigned streamed_grid(JitEntry& e) {
     if (!((e.setup_devices >> dev) & 1)) {
         const void* f = reinterpret_cast<const void*>(e.kernel);
         int occ = 0, nsm = 0;
-        if (cudaKernelSetAttributeForDevice(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStreamSmem,
+        if (cudaKernelSetAttributeForDevice(e.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem,
                                             dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, PASS_THREADS, kStreamSmem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, PASS_THREADS, e.smem) != cudaSuccess ||
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || occ < 1) {
             cudaGetLastError();
             return 0;
@@ -973,7 +1138,7 @@ cudaError_t JitKernel::launch(void* amps, const PassParams& P, const double* nor
         }
         void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials, &status};
         return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(std::min(g, tiles)),
-                                dim3(PASS_THREADS), args, kStreamSmem, st);
+                                dim3(PASS_THREADS), args, e_->smem, st);
     }
     void* args[] = {&amps, const_cast<PassParams*>(&P), &norm2_in, &partials};
     return cudaLaunchKernel(reinterpret_cast<const void*>(e_->kernel), dim3(tiles), dim3(PASS_THREADS), args, 0, st);
@@ -999,7 +1164,7 @@ uint64_t fnv64(const std::string& s) {
 }
 
 bool body_is_c64(const std::string& body) {
-    return body.find("using namespace qoa::p32;") < 200;
+    return body.find("using namespace qoa::p32;") != std::string::npos;
 }
 
 std::string program_text(const std::vector<std::string>& names, const std::vector<std::string>& bodies) {
@@ -1009,7 +1174,7 @@ std::string program_text(const std::vector<std::string>& names, const std::vecto
         const bool c64 = body_is_c64(bodies[i]);
         const bool streamed = bodies[i].find(kStreamMark) != std::string::npos;
         snprintf(head, sizeof head, "extern \"C\" __global__ void __launch_bounds__(%d, %d) %s", PASS_THREADS,
-                 streamed ? occ_streamed() : occ_target(c64), names[i].c_str());
+                 streamed ? occ_streamed(c64) : occ_target(c64), names[i].c_str());
         src += head;
         src += bodies[i];
     }
@@ -1170,6 +1335,7 @@ public:
                 auto e = std::make_shared<JitEntry>();
                 e->name = kernel_name(b);
                 e->streamed = b.find(kStreamMark) != std::string::npos;
+                e->smem = e->streamed ? (body_is_c64(b) ? kStreamSmem32 : kStreamSmem) : 0;
                 cache_.emplace(key, e);
                 queue_.push_back(JitJob{e, b});
                 ++pending_;
