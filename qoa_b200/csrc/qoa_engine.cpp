@@ -53,7 +53,7 @@ cudaError_t launch_sample(const void* a, bool f32, uint32_t n, const double* nor
                           const double* u, uint64_t shots, int mode, unsigned long long* out, cudaStream_t st);
 cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32PhaseOp* pops,
                             const F32Angle* angles, const F32Phase* phases, const float2* tables,
-                            const double* norm2_in, double* partials, cudaStream_t st);
+                            const double* norm2_in, double* partials, uint32_t* status, cudaStream_t st);
 cudaError_t launch_f32_reset(float2* a, uint64_t len, cudaStream_t st);
 cudaError_t launch_f32_norm(const float2* a, uint64_t len, double* partials, double* out, uint32_t* status,
                             cudaStream_t st);
@@ -73,7 +73,7 @@ cudaError_t launch_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32
                               int max_nops, int max_ncoef, cudaStream_t st);
 cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
                                   const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
-                                  const F32Phase* phases, const float2* tables, cudaStream_t st);
+                                  const F32Phase* phases, const float2* tables, uint32_t* status, cudaStream_t st);
 cudaError_t launch_arena_expz(bool f32, const ExpzJob* jobs, uint32_t njobs, uint32_t chunks, const uint64_t* masks,
                               double* partials, double* out, cudaStream_t st);
 cudaError_t launch_small_batch(bool f32, const SmallCircuit* circs, uint32_t count, const SmallOp* ops,
@@ -1392,7 +1392,10 @@ int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32Pa
             for (const Gate* g : blk) block_apply(*g, qs, v);
             for (int r = 0; r < 32; ++r) U[r][c] = v[r];
         }
-        // real embedding [[Ur, -Ui], [Ui, Ur]], split into TF32 hi / lo
+        // real embedding [[Ur, -Ui], [Ui, Ur]] (row r = output, column c =
+        // input), split into TF32 hi / lo, each stored as the tensor cores'
+        // K-major operand: 8-row x 4-element core matrices of 128 bytes, the
+        // 8 row groups of one 4-column chunk adjacent, chunks 1 KB apart
         const size_t base = mats.size();
         mats.resize(base + 8192);
         for (int r = 0; r < 64; ++r)
@@ -1403,8 +1406,9 @@ int build_f32_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, F32Pa
                 else x = (c < 32) ? u.imag() : u.real();
                 const float h = tf32_round((float)x);
                 const float l = tf32_round((float)(x - (double)h));
-                mats[base + r * 64 + c] = h;
-                mats[base + 4096 + r * 64 + c] = l;
+                const size_t off = (size_t)(c >> 2) * 256 + (size_t)(r >> 3) * 32 + (size_t)(r & 7) * 4 + (c & 3);
+                mats[base + off] = h;
+                mats[base + 4096 + off] = l;
             }
         F32Op& op = P.ops[nops++];
         op.kind = 0;
@@ -1719,7 +1723,7 @@ int f32_launch(qoa_state_t s) {
             Timer tm(s, 2.0 * std::ldexp(8.0, (int)s->n), 2);
             CK(launch_f32_pass((float2*)s->amps, P, (const float*)(dev + o[0]), (const F32PhaseOp*)(dev + o[1]),
                                (const F32Angle*)(dev + o[2]), (const F32Phase*)(dev + o[3]),
-                               (const float2*)(dev + o[4]), s->scal, s->partials, s->stream));
+                               (const float2*)(dev + o[4]), s->scal, s->partials, s->status + 3, s->stream));
         }
         CK(launch_reduce_partials(s->partials, 1u << (s->n - TILE_BITS), s->scal, s->status, s->stream));
         s->launches += 2;
@@ -2314,7 +2318,9 @@ int batch_prepare(qoa_batch_t b) {
     b->nsmall = (uint32_t)sc.size();
     b->small_max_n_used = maxn;
     BCK(cudaMalloc(&b->d_out, std::max<size_t>(1, b->nresults) * sizeof(double)));
-    BCK(cudaMalloc(&b->d_counter, sizeof(unsigned int)));
+    // [0] the small-circuit ticket counter, [1] the tensor passes' status word
+    BCK(cudaMalloc(&b->d_counter, 2 * sizeof(unsigned int)));
+    BCK(cudaMemset(b->d_counter, 0, 2 * sizeof(unsigned int)));
     int rc;
     if ((rc = upload(b, b->d_masks, masks))) return rc;
     if (!sc.empty()) {
@@ -2565,7 +2571,7 @@ int batch_enqueue(qoa_batch_t b) {
             BCK(launch_f32_pass_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                       (const float*)(fb + b->f32_off[0]), (const F32PhaseOp*)(fb + b->f32_off[1]),
                                       (const F32Angle*)(fb + b->f32_off[2]), (const F32Phase*)(fb + b->f32_off[3]),
-                                      (const float2*)(fb + b->f32_off[4]), s0));
+                                      (const float2*)(fb + b->f32_off[4]), b->d_counter + 1, s0));
         else if (f32)
             BCK(launch_pass_p32_arena(b->d_jobs + R.job_off, R.njobs, b->d_tstart + R.job_off, R.tiles,
                                       R.max_nops, R.max_ncoef, s0));

@@ -1,42 +1,46 @@
-// qoa_f32.cu — the FP32-fused precision form.
+// qoa_f32.cu — the FP32-fused precision form on the 5th-generation tensor
+// cores (tcgen05, accumulators in tensor memory).
 //
 // Complex64 amplitudes (float2), the same tile passes as the FP64 engine (the
 // 5 lowest qubits plus HIGH_SLOTS high qubits per CTA tile, one HBM read and
 // write per pass), but inside a pass the gates are fused on the host, in FP64,
 // into dense unitaries on at most 5 tile qubits. Each such block is applied to
-// the tile as a real GEMM on the tensor cores: with the block qubits as the
-// row index r (32 values) and the other 6 tile bits as the column index c
-// (64 values), Y = U X in complex form is
-//     [Yr; Yi] = [[Ur, -Ui], [Ui, Ur]] [Xr; Xi]      (64 x 64 by 64 x 64 real)
-// computed with mma.sync m16n8k8 TF32 and the 3xTF32 split a*b ~= ah*bh +
-// ah*bl + al*bh (h = round-to-TF32, l = the remainder), accumulated in FP32,
-// which keeps FP32-level accuracy. Diagonal gates that involve qubits outside
-// the tile become, per CTA, phases on single tile bits (their outer-qubit
-// condition is constant over a CTA) and are applied through two small tables.
-// Norm partial sums are FP64.
+// the tile as one real GEMM: with the block qubits as the inner index b (32
+// values) and the other 6 tile bits as the group index c (64 values), the
+// tile's 64 groups are the rows of X (64 x 64: Re x_b then Im x_b) and
+//     D = X U^T,   U = [[Ur, -Ui], [Ui, Ur]]     (64 x 64 real)
+// gives each group's 32 outputs (Re then Im). D is computed by
+// tcgen05.mma.cta_group::1.kind::tf32 (M = 64 groups, N = 64, K = 8 per
+// instruction) with both operands in shared memory in the K-major canonical
+// layout and the FP32 accumulator in tensor memory, with the 3xTF32 split
+// a*b ~= al*bh + ah*bl + ah*bh (h = round-to-TF32, l = the rounded
+// remainder), which keeps FP32-level accuracy. One thread issues the 24
+// instructions and commits them to an mbarrier; the warps read D back with
+// tcgen05.ld. Diagonal gates that involve qubits outside the tile become, per
+// CTA, phases on single tile bits (their outer-qubit condition is constant
+// over a CTA) and are applied through two small tables. Norm partial sums are
+// FP64.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "qoa_kernels.cuh"
+#include "qoa_pass_dev.cuh"
 
 namespace qoa {
 
 constexpr int F32_THREADS = 128;
-constexpr int F32_TILE = 1 << TILE_BITS;          // 2048 amplitudes, 16 KB per buffer
+constexpr int F32_TILE = 1 << TILE_BITS;          // 2048 amplitudes, 16 KB
 constexpr int F32_PER_THREAD = F32_TILE / F32_THREADS;
+// dynamic shared memory of a tensor pass CTA: the X operand (hi, lo), the
+// block's U operand (hi, lo), the tile, the MMA barrier and the
+// tensor-memory address
+constexpr unsigned F32_TC_SMEM = 4 * 16384 + F32_TILE * 8 + 16;
+constexpr uint32_t F32_TMEM_COLS = 64;            // one 64 x 64 FP32 accumulator
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
+__device__ __forceinline__ float tf32_hi(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-
-__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    return __uint_as_float(r);
 }
 
 __device__ __forceinline__ uint32_t pdep11(uint32_t x, uint32_t mask) {
@@ -49,68 +53,155 @@ __device__ __forceinline__ uint32_t pdep11(uint32_t x, uint32_t mask) {
     return r;
 }
 
-// One fused block: U applied to the tile bits in `bmask` (popcount 5; fewer
-// qubits are padded with tile bits the block acts on as identity).
-__device__ void f32_block(const float2* __restrict__ src, float2* __restrict__ dst, uint32_t bmask,
-                          const float* __restrict__ ahi, const float* __restrict__ alo, int* ro, int* co) {
+// Offset (in floats) of element (row, k) of a 64-row K-major operand of 64
+// TF32 columns: 8 x 4 core matrices of 128 B, row groups 128 B apart, 4-column
+// chunks 1 KB apart (the layout the host writes the block matrices in).
+__device__ __forceinline__ uint32_t kmaj(uint32_t row, uint32_t k) {
+    return (k >> 2) * 256u + (row >> 3) * 32u + (row & 7u) * 4u + (k & 3u);
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major, leading (K-chunk)
+// byte offset 1024, stride (row-group) byte offset 128, sm_100 version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(1024u >> 4) << 16) | ((uint64_t)(128u >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor of kind::tf32: FP32 accumulator, TF32 A and B, both
+// K-major, N = 64, M = 64.
+constexpr uint32_t F32_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %3, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %4, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(accumulate), "r"(F32_IDESC), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* mb) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mb))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive columns of this warp's 32 tensor-memory lanes
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,"
+        "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// The CTA's accumulator: F32_TMEM_COLS tensor-memory columns allocated by
+// warp 0 (address written to *slot) and freed by it at the end.
+__device__ __forceinline__ void tc_alloc(uint32_t* slot) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(F32_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_dealloc(uint32_t taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(F32_TMEM_COLS) : "memory");
+}
+
+struct F32Smem {
+    float* xh;        // X operand, TF32 hi (64 x 64, K-major)
+    float* xl;        // X operand, TF32 lo
+    float* uh;        // U operand of the current block, hi
+    float* ul;        // and lo (adjacent to uh, as in the host's upload)
+    float2* tile;     // 2048 amplitudes
+    uint64_t* mbar;   // MMA completion
+    uint32_t* tslot;  // tensor-memory address
+};
+
+__device__ __forceinline__ F32Smem f32_smem(unsigned char* base) {
+    F32Smem m;
+    m.xh = reinterpret_cast<float*>(base);
+    m.xl = m.xh + 4096;
+    m.uh = m.xl + 4096;
+    m.ul = m.uh + 4096;
+    m.tile = reinterpret_cast<float2*>(m.ul + 4096);
+    m.mbar = reinterpret_cast<uint64_t*>(m.tile + F32_TILE);
+    m.tslot = reinterpret_cast<uint32_t*>(m.mbar + 1);
+    return m;
+}
+
+// One fused block: U applied in place to the tile bits in `bmask` (popcount 5;
+// fewer qubits are padded with tile bits the block acts on as identity).
+// `nblk` counts the CTA's blocks so far (the mbarrier's phase).
+__device__ void f32_block(const F32Smem& S, uint32_t taddr, uint32_t bmask, const float* __restrict__ mat,
+                          uint32_t nblk, uint32_t* status) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, w = tid >> 5;
-    const int gq = lane >> 2, t4 = lane & 3;
     const uint32_t cmask = ((1u << TILE_BITS) - 1) & ~bmask;
-    if (tid < 32) ro[tid] = (int)pdep11((uint32_t)tid, bmask);
-    if (tid < 64) co[tid] = (int)pdep11((uint32_t)tid, cmask);
-    // A fragments for this warp's 16 real output rows, all 8 k-steps
-    uint32_t ah[8][4], al[8][4];
-    const int r0 = 16 * w + gq, r1 = r0 + 8;
-#pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-        const int c0 = 8 * kk + t4, c1 = c0 + 4;
-        ah[kk][0] = __float_as_uint(ahi[r0 * 64 + c0]);
-        ah[kk][1] = __float_as_uint(ahi[r1 * 64 + c0]);
-        ah[kk][2] = __float_as_uint(ahi[r0 * 64 + c1]);
-        ah[kk][3] = __float_as_uint(ahi[r1 * 64 + c1]);
-        al[kk][0] = __float_as_uint(alo[r0 * 64 + c0]);
-        al[kk][1] = __float_as_uint(alo[r1 * 64 + c0]);
-        al[kk][2] = __float_as_uint(alo[r0 * 64 + c1]);
-        al[kk][3] = __float_as_uint(alo[r1 * 64 + c1]);
+    // tile index of each block state
+    __shared__ uint32_t ro[32];
+    if (tid < 32) ro[tid] = pdep11((uint32_t)tid, bmask);
+    // the block's U (hi then lo), already in the operand layout
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(mat);
+        uint4* dst = reinterpret_cast<uint4*>(S.uh);
+#pragma unroll 4
+        for (int i = tid; i < 2048; i += F32_THREADS) dst[i] = __ldg(src + i);
     }
+    __syncthreads();  // ro
+    // X rows: thread t gathers half (16 block states) of group t >> 1
+    {
+        const uint32_t c = (uint32_t)tid >> 1, h = (uint32_t)tid & 1u;
+        const uint32_t cb = pdep11(c, cmask);
+#pragma unroll 4
+        for (uint32_t i = 0; i < 16; ++i) {
+            const uint32_t b = 16u * h + i;
+            const float2 x = S.tile[ro[b] | cb];
+            const float rh = tf32_hi(x.x), ih = tf32_hi(x.y);
+            S.xh[kmaj(c, b)] = rh;
+            S.xl[kmaj(c, b)] = tf32_hi(x.x - rh);
+            S.xh[kmaj(c, 32u + b)] = ih;
+            S.xl[kmaj(c, 32u + b)] = tf32_hi(x.y - ih);
+        }
+    }
+    proxy_fence_async();  // the operands written above are read by the tensor cores
+    tc_fence_before();
     __syncthreads();
-#pragma unroll 1
-    for (int nt = 0; nt < 8; ++nt) {
-        const int col = 8 * nt + gq;
-        const int cb = co[col];
-        // B rows 0..31 are Re X, rows 32..63 Im X of the same elements
-        float2 x0[4], x1[4];
+    if (tid == 0) {
+        tc_fence_after();
+        const uint32_t xh = smem_u32(S.xh), xl = smem_u32(S.xl), uh = smem_u32(S.uh), ul = smem_u32(S.ul);
+        // D = Xl Uh^T + Xh Ul^T + Xh Uh^T, K = 64 in steps of 8 (2 KB of operand per step)
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            x0[kk] = src[ro[8 * kk + t4] | cb];
-            x1[kk] = src[ro[8 * kk + t4 + 4] | cb];
-        }
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (uint32_t s = 0; s < 8; ++s) tc_mma(taddr, smem_desc(xl + 2048u * s), smem_desc(uh + 2048u * s), s);
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-            const float f0 = kk < 4 ? x0[kk].x : x0[kk - 4].y;
-            const float f1 = kk < 4 ? x1[kk].x : x1[kk - 4].y;
-            const uint32_t bh0 = to_tf32(f0), bh1 = to_tf32(f1);
-            const uint32_t bl0 = to_tf32(f0 - __uint_as_float(bh0)), bl1 = to_tf32(f1 - __uint_as_float(bh1));
-            mma_tf32(acc, al[kk], bh0, bh1);
-            mma_tf32(acc, ah[kk], bl0, bl1);
-            mma_tf32(acc, ah[kk], bh0, bh1);
-        }
-        // C fragment: rows r0 (acc 0,1) and r1 (acc 2,3), cols 8nt + 2 t4 (+1)
-        const int ca = co[8 * nt + 2 * t4], cbb = co[8 * nt + 2 * t4 + 1];
-        if (w < 2) {  // rows 0..31: real parts
-            dst[ro[r0] | ca].x = acc[0];
-            dst[ro[r0] | cbb].x = acc[1];
-            dst[ro[r1] | ca].x = acc[2];
-            dst[ro[r1] | cbb].x = acc[3];
-        } else {      // rows 32..63: imaginary parts
-            dst[ro[r0 - 32] | ca].y = acc[0];
-            dst[ro[r0 - 32] | cbb].y = acc[1];
-            dst[ro[r1 - 32] | ca].y = acc[2];
-            dst[ro[r1 - 32] | cbb].y = acc[3];
+        for (uint32_t s = 0; s < 8; ++s) tc_mma(taddr, smem_desc(xh + 2048u * s), smem_desc(ul + 2048u * s), 1u);
+#pragma unroll
+        for (uint32_t s = 0; s < 8; ++s) tc_mma(taddr, smem_desc(xh + 2048u * s), smem_desc(uh + 2048u * s), 1u);
+        tc_commit(S.mbar);
+    }
+    mbar_wait(S.mbar, nblk & 1u, status);
+    tc_fence_after();
+    // D row c (M = 64: rows 16w..16w+15 sit in lanes 0..15 of warp w's
+    // quarter of tensor memory) -> group c's 32 amplitudes
+    {
+        const uint32_t base = taddr + ((uint32_t)(32 * w) << 16);
+        float re[32], im[32];
+        tc_ld32(base, re);
+        tc_ld32(base + 32u, im);
+        if (lane < 16) {
+            const uint32_t c = 16u * (uint32_t)w + (uint32_t)lane;
+            const uint32_t cb = pdep11(c, cmask);
+#pragma unroll
+            for (uint32_t b = 0; b < 32; ++b) S.tile[ro[b] | cb] = make_float2(re[b], im[b]);
         }
     }
+    tc_fence_before();
     __syncthreads();
 }
 
@@ -121,9 +212,11 @@ __device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F
                                               const float* __restrict__ mats, const F32PhaseOp* __restrict__ pops,
                                               const F32Angle* __restrict__ angles,
                                               const F32Phase* __restrict__ phases, const float2* __restrict__ tables,
-                                              const double nrm, const uint64_t blk, double* __restrict__ partial_out) {
-    __shared__ float2 buf[2][F32_TILE];
-    __shared__ int ro[32], co[64];
+                                              const double nrm, const uint64_t blk, double* __restrict__ partial_out,
+                                              uint32_t* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char f32_dsm[];
+    const F32Smem S = f32_smem(f32_dsm);
+    float2* const buf = S.tile;
     __shared__ float2 tlo[32], thi[64];
     __shared__ double alpha[TILE_BITS + 1];
     __shared__ double red[F32_THREADS / 32];
@@ -150,17 +243,24 @@ __device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F
         const uint64_t g = gidx(j);
         float2 x = valid ? __ldcs(amps + g) : make_float2(g == 0 ? 1.f : 0.f, 0.f);
         if (valid) x = make_float2(x.x * scale, x.y * scale);
-        buf[0][j] = x;
+        buf[j] = x;
     }
+    // the tensor-memory accumulator (warp 0 allocates) and the MMA barrier
+    if (tid < 32) tc_alloc(S.tslot);
+    if (tid == 0) {
+        mbar_init(S.mbar, 1);
+        mbar_init_fence();
+    }
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = *S.tslot;
 
-    int cur = 0;
+    uint32_t nblk = 0;
     for (uint32_t oi = 0; oi < P.nops; ++oi) {
         const F32Op op = P.ops[oi];
         if (op.kind == 0) {  // dense block
-            const float* a = mats + (size_t)op.index * 8192;
-            f32_block(buf[cur], buf[cur ^ 1], op.bmask, a, a + 4096, ro, co);
-            cur ^= 1;
+            f32_block(S, taddr, op.bmask, mats + (size_t)op.index * 8192, nblk++, status);
         } else {
             const F32PhaseOp po = pops[op.index];
             // per-CTA angle of each tile bit (and of the scalar part)
@@ -191,7 +291,7 @@ __device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F
             }
             __syncthreads();
             const float2* tab = po.table >= 0 ? tables + (size_t)po.table * F32_TILE : nullptr;
-            float2* s = buf[cur];
+            float2* s = buf;
             for (int i = 0; i < F32_PER_THREAD; ++i) {
                 const uint32_t j = (uint32_t)(tid + F32_THREADS * i);
                 const float2 l = tlo[j & 31u], h = thi[j >> LANE_BITS];
@@ -214,10 +314,12 @@ __device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F
         }
     }
 
+    // every tensor-memory read is done (behind the last block's barrier)
+    if (tid < 32) tc_dealloc(taddr);
     double ss = 0.0;
     for (int i = 0; i < F32_PER_THREAD; ++i) {
         const uint32_t j = (uint32_t)(tid + F32_THREADS * i);
-        const float2 x = buf[cur][j];
+        const float2 x = buf[j];
         __stcs(amps + gidx(j), x);
         ss += (double)x.x * x.x + (double)x.y * x.y;
     }
@@ -233,22 +335,22 @@ __device__ __forceinline__ void f32_pass_tile(float2* __restrict__ amps, const F
     }
 }
 
-__global__ void __launch_bounds__(F32_THREADS, 4)
+__global__ void __launch_bounds__(F32_THREADS, 2)
 k_f32_pass(float2* __restrict__ amps, const __grid_constant__ F32PassParams P, const float* __restrict__ mats,
            const F32PhaseOp* __restrict__ pops, const F32Angle* __restrict__ angles,
            const F32Phase* __restrict__ phases, const float2* __restrict__ tables, const double* __restrict__ norm2_in,
-           double* __restrict__ partials) {
-    f32_pass_tile(amps, P, mats, pops, angles, phases, tables, *norm2_in, blockIdx.x, partials + blockIdx.x);
+           double* __restrict__ partials, uint32_t* __restrict__ status) {
+    f32_pass_tile(amps, P, mats, pops, angles, phases, tables, *norm2_in, blockIdx.x, partials + blockIdx.x, status);
 }
 
 // Arena form: one launch runs one pass of each of many circuits (see
 // k_pass_arena); every circuit's block matrices, phase groups, angle lists
 // and tables lie in one shared upload, so the base pointers are common.
-__global__ void __launch_bounds__(F32_THREADS, 4)
+__global__ void __launch_bounds__(F32_THREADS, 2)
 k_f32_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32_t* __restrict__ tile_start,
                  const float* __restrict__ mats, const F32PhaseOp* __restrict__ pops,
                  const F32Angle* __restrict__ angles, const F32Phase* __restrict__ phases,
-                 const float2* __restrict__ tables) {
+                 const float2* __restrict__ tables, uint32_t* __restrict__ status) {
     const uint32_t b = blockIdx.x;
     uint32_t lo = 0, hi = njobs - 1;
     while (lo < hi) {
@@ -258,22 +360,44 @@ k_f32_pass_arena(const ArenaJob* __restrict__ jobs, uint32_t njobs, const uint32
     }
     const ArenaJob J = jobs[lo];
     f32_pass_tile(reinterpret_cast<float2*>(J.amps), *reinterpret_cast<const F32PassParams*>(J.params), mats, pops,
-                  angles, phases, tables, J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr);
+                  angles, phases, tables, J.fresh ? 0.0 : 1.0, b - tile_start[lo], nullptr, status);
+}
+
+// The tensor pass kernels need more than the default 48 KB of dynamic shared
+// memory: allowed once per device.
+static cudaError_t f32_tc_setup() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    static uint64_t done = 0;  // devices set up (the set-up is idempotent, so racing threads are harmless)
+    if ((__atomic_load_n(&done, __ATOMIC_ACQUIRE) >> dev) & 1) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_f32_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_TC_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_f32_pass_arena, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_TC_SMEM);
+    if (e == cudaSuccess) __atomic_fetch_or(&done, 1ull << dev, __ATOMIC_RELEASE);
+    return e;
 }
 
 cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const uint32_t* tile_start, uint32_t tiles,
                                   const float* mats, const F32PhaseOp* pops, const F32Angle* angles,
-                                  const F32Phase* phases, const float2* tables, cudaStream_t st) {
+                                  const F32Phase* phases, const float2* tables, uint32_t* status, cudaStream_t st) {
     if (!njobs || !tiles) return cudaSuccess;
-    k_f32_pass_arena<<<tiles, F32_THREADS, 0, st>>>(jobs, njobs, tile_start, mats, pops, angles, phases, tables);
+    const cudaError_t e = f32_tc_setup();
+    if (e != cudaSuccess) return e;
+    k_f32_pass_arena<<<tiles, F32_THREADS, F32_TC_SMEM, st>>>(jobs, njobs, tile_start, mats, pops, angles, phases,
+                                                              tables, status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_f32_pass(float2* amps, const F32PassParams& P, const float* mats, const F32PhaseOp* pops,
                             const F32Angle* angles, const F32Phase* phases, const float2* tables,
-                            const double* norm2_in, double* partials, cudaStream_t st) {
+                            const double* norm2_in, double* partials, uint32_t* status, cudaStream_t st) {
+    const cudaError_t e = f32_tc_setup();
+    if (e != cudaSuccess) return e;
     const unsigned blocks = 1u << (P.n - TILE_BITS);
-    k_f32_pass<<<blocks, F32_THREADS, 0, st>>>(amps, P, mats, pops, angles, phases, tables, norm2_in, partials);
+    k_f32_pass<<<blocks, F32_THREADS, F32_TC_SMEM, st>>>(amps, P, mats, pops, angles, phases, tables, norm2_in,
+                                                        partials, status);
     return cudaGetLastError();
 }
 
