@@ -119,18 +119,18 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def pass_traffic_bytes(n: int, generated: bool = True):
-    """DRAM bytes per tile-pass launch at n qubits, scaled from the committed
-    ncu capture of the 26-qubit instance (traffic grows with the amplitudes):
-    the generated pass kernel's capture, or the interpreter's."""
-    p = os.path.join(ROOT, "profiles", "qoa_jit_pass_layered26.md" if generated else "k_pass_layered26.md")
+def pass_traffic_bytes(n: int, kernel: str):
+    """DRAM bytes per tile-pass launch at n qubits: the ncu-measured bytes per
+    amplitude of a smaller capture of the same kernel (profiles/
+    ncu_counters.json, written from the capture's dram__bytes_read.sum +
+    dram__bytes_write.sum), scaled by the amplitudes (traffic grows with
+    them). None when no capture of that kernel is recorded."""
+    p = os.path.join(ROOT, "profiles", "ncu_counters.json")
     try:
-        for line in open(p):
-            if line.startswith("dram_bytes_per_amplitude:"):
-                return float(line.split(":")[1]) * (1 << n)
-    except OSError:
-        pass
-    return None
+        rec = json.load(open(p))[kernel]
+        return float(rec["dram_bytes"]) / float(1 << int(rec["n_qubits"])) * (1 << n), rec["source"]
+    except (OSError, KeyError, ValueError):
+        return None, None
 
 
 def measured_peaks():
@@ -309,6 +309,8 @@ def run_ours(args):
     ms, by, kind = prof.launch_times()
     prof_jit = prof.jit_stats()["launches"]
     prof.close()
+    traffic, traffic_src = pass_traffic_bytes(n, "qoa_jit_pass (streamed, complex128)" if prof_jit > 0
+                                              else "k_pass (complex128)")
     pass_ms = ms[kind == 0]
     pass_bytes = by[kind == 0]
     peak, peak_src = measured_peaks()
@@ -316,8 +318,7 @@ def run_ours(args):
     achieved = float(pass_bytes.mean() / (avg_ms / 1e3) / 1e9) if pass_ms.size else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": pass_traffic_bytes(n, generated=prof_jit > 0),
-                "traffic_source": "ncu dram bytes of the 26-qubit instance, scaled per amplitude",
+                "traffic": traffic, "traffic_source": traffic_src,
                 "kernel": "qoa_jit_pass_* (generated tile pass)" if prof_jit > 0 else "k_pass (interpreter)",
                 "launches_per_step": int(pass_ms.size), "avg_launch_ms": avg_ms,
                 "algorithmic_bytes_per_launch": float(pass_bytes.mean()) if pass_ms.size else None,

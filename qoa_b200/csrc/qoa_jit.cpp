@@ -85,6 +85,22 @@ int occ_streamed(bool c64) {
     return (k >= 1 && k <= d) ? k : d;
 }
 
+// Which generated single-state passes take the streamed (persistent,
+// double-buffered) form. complex128: off by default — at 128 registers a
+// thread its two 32 KB tile buffers allow 3 CTAs per SM instead of 4, and
+// the deep complex128 passes lose more to the lower occupancy than the
+// overlapped loads win (30-qubit layered circuit: 13.6 against 10.6 ms a
+// pass). QOA_JIT_STREAM=0/1/2/3: neither / complex128 / complex64 / both.
+int stream_mode() {
+    static const int m = [] {
+        const char* v = getenv("QOA_JIT_STREAM");
+        return v ? atoi(v) : 2;
+    }();
+    return m;
+}
+bool stream_f64() { return (stream_mode() & 1) != 0; }
+bool stream_f32() { return (stream_mode() & 2) != 0; }
+
 uint32_t spos_host(uint32_t j) { return j ^ (((j >> 3) ^ (j >> 6) ^ (j >> 9)) & 7u); }
 
 struct Emit {
@@ -137,6 +153,14 @@ std::string tcond(uint32_t tm) {
     char b[64];
     snprintf(b, sizeof b, "((tw & 0x%xu) == 0x%xu)", tm, tm);
     return b;
+}
+
+// Both mappings put the same tile bits on the warp bits: an exchange between
+// them moves data only among the threads of each warp.
+bool same_warps(const TileMap& a, const TileMap& b) {
+    for (int k = 0; k < WARP_BITS; ++k)
+        if (a.warp[k] != b.warp[k]) return false;
+    return true;
 }
 
 // Tile index (shared-memory bits) of this thread's register 0 under map m:
@@ -475,7 +499,10 @@ const TileMap* emit_ops128(Emit& E, const PassParams& P, bool arena, const char*
                     E.line("{ const uint32_t pb = %s;", swz_base(z, mo, pos).c_str());
                     for (int v = 0; v < REGS; ++v) E.line("tile[pb ^ %uu] = a[%d];", off(mo, v), v);
                     E.line("}");
-                    E.line("__syncthreads();");
+                    // an exchange that keeps the warp bits moves data only within
+                    // each warp: with the pass's one layout a warp stores to and
+                    // loads from its own part of the tile, so a warp barrier does
+                    E.line(shared_layout && same_warps(mo, mn) ? "__syncwarp();" : "__syncthreads();");
                     E.line("{ const uint32_t pb = %s;", swz_base(z, mn, pos).c_str());
                     for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[pb ^ %uu];", v, off(mn, v));
                     E.line("}");
@@ -622,7 +649,7 @@ std::string jit_pass_body_streamed(const PassParams& P) {
 }
 
 std::string jit_pass_body(const PassParams& P, bool arena) {
-    if (!arena && !getenv("QOA_JIT_UNSTREAMED")) return jit_pass_body_streamed(P);
+    if (!arena && stream_f64()) return jit_pass_body_streamed(P);
     Emit E;
     // complex128 coefficients: the parameter's constant bank, or the staged copy
     const char* cf = arena ? "scoef" : "P.coef";
@@ -813,7 +840,7 @@ const TileMap* emit_ops64(Emit& E, const PassParams& P, bool arena, const std::v
                         for (int j = 0; j < 8; ++j)
                             E.line("pt[pb ^ %uu] = make_ulonglong2(re[%d], im[%d]);", off(mo, j), j, j);
                         E.line("}");
-                        E.line("__syncthreads();");
+                        E.line(shared_layout && same_warps(mo, mn) ? "__syncwarp();" : "__syncthreads();");
                         E.line("{ const ulonglong2* pt = reinterpret_cast<const ulonglong2*>(tile); const uint32_t pb = %s;",
                                swz_base(z, mn, pos).c_str());
                         for (int j = 0; j < 8; ++j)
@@ -998,7 +1025,7 @@ std::string jit_pass32_body_streamed(const PassParams& P) {
 }
 
 std::string jit_pass32_body(const PassParams& P, bool arena) {
-    if (!arena && !getenv("QOA_JIT_UNSTREAMED")) return jit_pass32_body_streamed(P);
+    if (!arena && stream_f32()) return jit_pass32_body_streamed(P);
     Emit E;
     emit_head(E, P, true, arena);
     // register tables (PC_DIAG_TAB): staged once per CTA already packed as

@@ -16,13 +16,13 @@ TERM = re.compile(r"\(\(0u - \(\(\(uint32_t\)(lane|wid) >> (\d)\) & 1u\)\) & 0x(
 
 
 def exchanges(kernel, precision):
-    """[(barrier_before_store, store_units[thread][k], load_units[thread][k])]"""
+    """[(barrier_before_store, store_units[thread][k], load_units[thread][k], warp_local)]"""
     if precision == "f64":
         pat = re.compile(r"(__syncthreads\(\);\n)?\{ const uint32_t pb = (0u[^;]*);\n((?:tile\[pb \^ \d+u\] = a\[\d+\];\n){16})\}\n"
-                         r"__syncthreads\(\);\n\{ const uint32_t pb = (0u[^;]*);\n((?:a\[\d+\] = tile\[pb \^ \d+u\];\n){16})")
+                         r"(__syncthreads\(\);|__syncwarp\(\);)\n\{ const uint32_t pb = (0u[^;]*);\n((?:a\[\d+\] = tile\[pb \^ \d+u\];\n){16})")
     else:
         pat = re.compile(r"(__syncthreads\(\);\n)?\{ ulonglong2\* pt = reinterpret_cast<ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
-                         r"((?:pt\[pb \^ \d+u\] = .*\n){8})\}\n__syncthreads\(\);\n"
+                         r"((?:pt\[pb \^ \d+u\] = .*\n){8})\}\n(__syncthreads\(\);|__syncwarp\(\);)\n"
                          r"\{ const ulonglong2\* pt = reinterpret_cast<const ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
                          r"((?:\{ const ulonglong2 u = pt\[pb \^ \d+u\].*\n){8})")
     out = []
@@ -40,7 +40,8 @@ def exchanges(kernel, precision):
                         base ^= c
                 res.append([base ^ o for o in offs])
             return res
-        out.append((m.group(1) is not None, units(m.group(2), m.group(3)), units(m.group(4), m.group(5))))
+        out.append((m.group(1) is not None, units(m.group(2), m.group(3)), units(m.group(5), m.group(6)),
+                    m.group(4) == "__syncwarp();"))
     return out
 
 
@@ -67,7 +68,12 @@ def test_generated_exchanges(name, n, make, flags, precision):
         # every exchange of the kernel was recognised
         assert len(xs) == (k.count("tile[pb ^") // 32 if precision == "f64" else k.count("make_ulonglong2") // 8)
         prev_load = None
-        for i, (barrier, st, ld) in enumerate(xs):
+        for i, (barrier, st, ld, warp_local) in enumerate(xs):
+            if warp_local:
+                for w in range(4):
+                    warp = range(32 * w, 32 * w + 32)
+                    assert sorted(u for t in warp for u in st[t]) == sorted(u for t in warp for u in ld[t]), \
+                        "a warp-local exchange loads units another warp stored"
             for side in (st, ld):
                 flat = [u for t in side for u in t]
                 assert sorted(flat) == list(range(nunits)), "layout is not a bijection"
