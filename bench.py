@@ -309,8 +309,9 @@ def run_ours(args):
     ms, by, kind = prof.launch_times()
     prof_jit = prof.jit_stats()["launches"]
     prof.close()
-    traffic, traffic_src = pass_traffic_bytes(n, "qoa_jit_pass (streamed, complex128)" if prof_jit > 0
-                                              else "k_pass (complex128)")
+    streamed = os.environ.get("QOA_JIT_STREAM", "0") in ("1", "3")
+    traffic, traffic_src = pass_traffic_bytes(n, ("qoa_jit_pass (streamed, complex128)" if streamed else
+                                                  "qoa_jit_pass (complex128)") if prof_jit > 0 else "k_pass (complex128)")
     pass_ms = ms[kind == 0]
     pass_bytes = by[kind == 0]
     peak, peak_src = measured_peaks()

@@ -86,17 +86,16 @@ int occ_streamed(bool c64) {
 }
 
 // Which generated single-state passes take the streamed (persistent,
-// double-buffered) form. complex128: off by default — at 128 registers a
-// thread its two 32 KB tile buffers allow 3 CTAs per SM instead of 4, and
-// the deep complex128 passes lose more to the lower occupancy than the
-// overlapped loads win (30-qubit layered circuit: 13.6 against 10.6 ms a
-// pass). QOA_JIT_STREAM=0/1/2/3: neither / complex128 / complex64 / both.
+// double-buffered) form: QOA_JIT_STREAM=0/1/2/3 = neither (the default) /
+// complex128 / complex64 / both. Measured on B200, the streamed form loses
+// for both precisions: the passes are bound by FP64 (complex128) or
+// instruction issue (complex64), not by their loads, and the second tile
+// buffer lowers residency (complex128: 3 CTAs per SM instead of 4; 30-qubit
+// layered circuit 13.6 against 10.6 ms a pass; complex64 QFT at 32 qubits
+// 156 against 151 ms).
 int stream_mode() {
-    static const int m = [] {
-        const char* v = getenv("QOA_JIT_STREAM");
-        return v ? atoi(v) : 2;
-    }();
-    return m;
+    const char* v = getenv("QOA_JIT_STREAM");  // read at each pass's generation (cheap, and tests switch it)
+    return v ? atoi(v) : 0;
 }
 bool stream_f64() { return (stream_mode() & 1) != 0; }
 bool stream_f32() { return (stream_mode() & 2) != 0; }

@@ -163,16 +163,21 @@ def test_repeated_op_lists_reuse_their_plans():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("grid", ["1", "3", "7"])
-def test_streamed_passes_with_many_tiles_per_cta(monkeypatch, grid):
-    # the generated complex128 pass is persistent: each CTA walks tiles
-    # b, b + grid, ... with two shared-memory buffers whose copies complete
-    # on alternating mbarrier phases; a capped grid makes every CTA take
-    # many tiles (both buffers, both phases), still bit-identical to k_pass
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_streamed_passes_with_many_tiles_per_cta(monkeypatch, grid, precision):
+    # the streamed form of a generated pass (QOA_JIT_STREAM) is persistent:
+    # each CTA walks tiles b, b + grid, ... with two shared-memory buffers
+    # whose copies complete on alternating mbarrier phases; a capped grid
+    # makes every CTA take many tiles (both buffers, both phases), still
+    # bit-identical to the interpreter
     monkeypatch.setenv("QOA_JIT_STREAM_GRID", grid)
+    monkeypatch.setenv("QOA_JIT_STREAM", "3")
     n = 17
     ops = C.random_layered(n, 6, 61, initial_h=True)
-    got_jit, st_jit = run(n, ops, qb.QOA_JIT_SYNC, True)
-    got_int, _ = run(n, ops, qb.QOA_JIT_OFF, True)
+    got_jit, st_jit = run(n, ops, qb.QOA_JIT_SYNC, True, precision=precision)
+    got_int, _ = run(n, ops, qb.QOA_JIT_OFF, True, precision=precision)
     assert st_jit["launches"] > 0 and st_jit["failures"] == 0
-    assert np.array_equal(got_jit.view(np.float64), got_int.view(np.float64))
-    assert rel_l2(got_jit, oracle_run(n, ops, 1)) < TOL
+    assert np.array_equal(got_jit.view(np.float32 if precision == "f32" else np.float64),
+                          got_int.view(np.float32 if precision == "f32" else np.float64))
+    tol = 1e-5 if precision == "f32" else TOL
+    assert rel_l2(got_jit.astype(np.complex128), oracle_run(n, ops, 1)) < tol
