@@ -1222,6 +1222,8 @@ struct NvrtcApi {
     std::string why;  // set when unavailable
 };
 
+void jit_stop_at_exit();
+
 const NvrtcApi& nvrtc() {
     static const NvrtcApi api = [] {
         NvrtcApi a;
@@ -1257,6 +1259,10 @@ const NvrtcApi& nvrtc() {
         if (!ok) {
             a = NvrtcApi();
             a.why = "libnvrtc lacks an entry point the engine needs: passes run on the interpreter kernels";
+        } else {
+            // registered after NVRTC was loaded, so it runs at exit before
+            // NVRTC's own teardown: no compile thread may still be inside it
+            std::atexit(jit_stop_at_exit);
         }
         return a;
     }();
@@ -1315,13 +1321,28 @@ struct JitJob {
 
 class JitCompiler {
 public:
-    ~JitCompiler() {
+    ~JitCompiler() { shutdown(); }
+
+    // Stops compiling: queued compiles are dropped (their kernels stay on
+    // the interpreter), compiles in flight finish without loading, and the
+    // compile threads are joined. Runs at process exit before NVRTC's own
+    // teardown (see nvrtc()), so that no thread is inside NVRTC then.
+    void shutdown() {
+        std::vector<std::thread> ws;
         {
             std::lock_guard<std::mutex> lk(mu_);
             stop_ = true;
+            for (auto& j : queue_) {
+                j.entry->state.store(2, std::memory_order_release);
+                --pending_;
+                ++failures_;
+            }
+            queue_.clear();
+            ws.swap(workers_);
         }
         cv_.notify_all();
-        for (auto& t : workers_)
+        done_cv_.notify_all();
+        for (auto& t : ws)
             if (t.joinable()) t.join();
     }
 
@@ -1333,6 +1354,10 @@ public:
         bool queued = false;
         {
             std::lock_guard<std::mutex> lk(mu_);
+            if (stop_) {  // exiting: everything stays on the interpreter
+                out.resize(bodies.size());
+                return out;
+            }
             for (const std::string& b : bodies) {
                 const Key key{fnv64(b), std::hash<std::string>()(b)};
                 auto it = cache_.find(key);
@@ -1497,6 +1522,8 @@ JitCompiler& compiler() {
     static JitCompiler c;
     return c;
 }
+
+void jit_stop_at_exit() { compiler().shutdown(); }
 
 }  // namespace
 
