@@ -1259,10 +1259,6 @@ const NvrtcApi& nvrtc() {
         if (!ok) {
             a = NvrtcApi();
             a.why = "libnvrtc lacks an entry point the engine needs: passes run on the interpreter kernels";
-        } else {
-            // registered after NVRTC was loaded, so it runs at exit before
-            // NVRTC's own teardown: no compile thread may still be inside it
-            std::atexit(jit_stop_at_exit);
         }
         return a;
     }();
@@ -1287,6 +1283,12 @@ bool build_cubin(const std::vector<std::string>& names, const std::vector<std::s
     }
     const char* opts[] = {"-arch=sm_100a", "-std=c++17", "--fmad=true"};
     const nvrtcResult rc = nv.compile(prog, 3, opts);
+    // NVRTC registers its own exit-time teardown lazily, inside compiles;
+    // exit handlers run last-registered first, so registering the compile
+    // threads' shutdown after every compile makes it run before NVRTC's:
+    // no compile thread can then still be inside NVRTC when it is torn
+    // down (an in-flight compile at exit crashed in nvrtcCompileProgram)
+    std::atexit(jit_stop_at_exit);
     if (rc != NVRTC_SUCCESS) {
         size_t n = 0;
         nv.log_size(prog, &n);
