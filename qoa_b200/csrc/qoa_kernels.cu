@@ -13,6 +13,8 @@
 // quantum_state.rs:399-458, the marginal tree behind measure_all-order
 // sampling (quantum_state.rs:909-918), and expectation values.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 #include <string.h>
 
@@ -409,46 +411,71 @@ __global__ void k_reset_all(T* __restrict__ a, uint64_t len) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid_constant__ PermParams P) {
     extern __shared__ __align__(16) unsigned char sw_smem[];
-    T* s0 = reinterpret_cast<T*>(sw_smem);
     const uint32_t tn = 1u << P.na;
+    T* s0 = reinterpret_cast<T*>(sw_smem);
     T* s1 = s0 + tn;
+    // tile index j = lo | hi << hl: its global offset and its source's tile
+    // index, from two small tables each (built once per CTA)
+    const uint32_t hl = P.na / 2, hh = P.na - hl;
+    __shared__ uint64_t glo[64], ghi[64];
+    __shared__ uint32_t slo[64], shi[64];
+    for (uint32_t x = threadIdx.x; x < (1u << hh); x += blockDim.x) {
+        uint64_t gl = 0, gh = 0;
+        uint32_t sl = 0, sh = 0;
+        for (uint32_t k = 0; k < hh; ++k) {
+            if (k < hl && ((x >> k) & 1)) {
+                gl |= 1ull << P.tq[k];
+                sl |= 1u << P.src_bit[k];
+            }
+            if ((x >> k) & 1) {
+                gh |= 1ull << P.tq[hl + k];
+                sh |= 1u << P.src_bit[hl + k];
+            }
+        }
+        if (x < (1u << hl)) {
+            glo[x] = gl;
+            slo[x] = sl;
+        }
+        ghi[x] = gh;
+        shi[x] = sh;
+    }
+    __syncthreads();
     const uint32_t nout = P.n - P.na;
-    const uint64_t b = blockIdx.x;
-    uint64_t o = 0, po = 0, pb = 0;
-    for (uint32_t k = 0; k < nout; ++k)
-        if ((b >> k) & 1) o |= 1ull << P.oq[k];
-    for (uint32_t k = 0; k < nout; ++k)
-        if ((o >> P.oq[k]) & 1) po |= 1ull << P.pi[P.oq[k]];
-    for (uint32_t k = 0; k < nout; ++k)
-        if ((po >> P.oq[k]) & 1) pb |= 1ull << k;
-    if (pb < b) return;  // the partner tile's CTA moves both
-    auto dep = [&](uint32_t j) {
-        uint64_t g = 0;
-        for (uint32_t k = 0; k < P.na; ++k)
-            if ((j >> k) & 1) g |= 1ull << P.tq[k];
-        return g;
-    };
+    const uint64_t ntiles = 1ull << nout;
     // shared-memory slot of tile index j: its low five bits XORed with the
     // next five, so the permuted reads of a warp spread over the banks
     auto sp = [](uint32_t j) { return j ^ ((j >> 5) & 31u); };
-    for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
-        const uint64_t g = dep(j);
-        s0[sp(j)] = a[o | g];
-        if (pb != b) s1[sp(j)] = a[po | g];
-    }
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
-        uint32_t src = 0;
-        for (uint32_t k = 0; k < P.na; ++k)
-            if ((j >> k) & 1) src |= 1u << P.src_bit[k];
-        const uint64_t g = dep(j);
-        a[po | g] = s0[sp(src)];
-        if (pb != b) a[o | g] = s1[sp(src)];
+    // persistent: CTA walks tiles b, b + gridDim.x, ...; a tile whose partner
+    // (its outer bits permuted) comes first is moved by the partner's turn
+    for (uint64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        uint64_t o = 0, po = 0, pb = 0;
+        for (uint32_t k = 0; k < nout; ++k)
+            if ((b >> k) & 1) o |= 1ull << P.oq[k];
+        for (uint32_t k = 0; k < nout; ++k)
+            if ((o >> P.oq[k]) & 1) po |= 1ull << P.pi[P.oq[k]];
+        for (uint32_t k = 0; k < nout; ++k)
+            if ((po >> P.oq[k]) & 1) pb |= 1ull << k;
+        if (pb < b) continue;  // uniform over the CTA
+        const bool two = pb != b;
+        for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
+            const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
+            s0[sp(j)] = __ldcs(a + (o | g));
+            if (two) s1[sp(j)] = __ldcs(a + (po | g));
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
+            const uint32_t src = slo[j & ((1u << hl) - 1)] | shi[j >> hl];
+            const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
+            __stcs(a + (po | g), s0[sp(src)]);
+            if (two) __stcs(a + (o | g), s1[sp(src)]);
+        }
+        __syncthreads();  // the buffers are reused by the next tile
     }
 }
 
 cudaError_t launch_swapnet(void* a, bool c64, const PermParams& P, cudaStream_t st) {
-    const unsigned blocks = 1u << (P.n - P.na);
+    const uint64_t tiles = 1ull << (P.n - P.na);
+    const unsigned blocks = (unsigned)std::min<uint64_t>(tiles, 148ull * 8);
     const size_t smem = (size_t)2 << P.na;
     if (c64) k_swapnet<float2><<<blocks, 256, smem * sizeof(float2), st>>>((float2*)a, P);
     else k_swapnet<double2><<<blocks, 256, smem * sizeof(double2), st>>>((double2*)a, P);
