@@ -439,9 +439,35 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
         ghi[x] = gh;
         shi[x] = sh;
     }
-    __syncthreads();
+    // a tile number b's outer offset o, its partner's po and the partner's
+    // tile number pb, each a sum over b's bytes of 256-entry tables (built
+    // once per CTA; a tile's loops over its outer bits cost more than its
+    // data movement)
     const uint32_t nout = P.n - P.na;
     const uint64_t ntiles = 1ull << nout;
+    const uint32_t nchunk = (nout + 7) / 8;  // <= 4: the launcher checks nout <= 32
+    __shared__ uint64_t t_o[4][256], t_po[4][256];
+    __shared__ uint32_t t_pb[4][256];
+    __shared__ uint8_t oidx[64];  // qubit -> its position in oq
+    for (uint32_t k = threadIdx.x; k < nout; k += blockDim.x) oidx[P.oq[k]] = (uint8_t)k;
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < nchunk * 256; e += blockDim.x) {
+        const uint32_t c = e >> 8, x = e & 255;
+        uint64_t o = 0, po = 0;
+        uint32_t pb = 0;
+        for (uint32_t i = 0; i < 8; ++i) {
+            const uint32_t k = 8 * c + i;
+            if (k >= nout || !((x >> i) & 1)) continue;
+            o |= 1ull << P.oq[k];
+            const uint32_t q = P.pi[P.oq[k]];
+            po |= 1ull << q;
+            pb |= 1u << oidx[q];
+        }
+        t_o[c][x] = o;
+        t_po[c][x] = po;
+        t_pb[c][x] = pb;
+    }
+    __syncthreads();
     // shared-memory slot of tile index j: its low five bits XORed with the
     // next five, so the permuted reads of a warp spread over the banks
     auto sp = [](uint32_t j) { return j ^ ((j >> 5) & 31u); };
@@ -449,12 +475,12 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
     // (its outer bits permuted) comes first is moved by the partner's turn
     for (uint64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
         uint64_t o = 0, po = 0, pb = 0;
-        for (uint32_t k = 0; k < nout; ++k)
-            if ((b >> k) & 1) o |= 1ull << P.oq[k];
-        for (uint32_t k = 0; k < nout; ++k)
-            if ((o >> P.oq[k]) & 1) po |= 1ull << P.pi[P.oq[k]];
-        for (uint32_t k = 0; k < nout; ++k)
-            if ((po >> P.oq[k]) & 1) pb |= 1ull << k;
+        for (uint32_t c = 0; c < nchunk; ++c) {
+            const uint32_t x = (uint32_t)(b >> (8 * c)) & 255u;
+            o |= t_o[c][x];
+            po |= t_po[c][x];
+            pb |= (uint64_t)t_pb[c][x];
+        }
         if (pb < b) continue;  // uniform over the CTA
         const bool two = pb != b;
         for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
@@ -474,6 +500,7 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
 }
 
 cudaError_t launch_swapnet(void* a, bool c64, const PermParams& P, cudaStream_t st) {
+    if (P.n - P.na > 32) return cudaErrorInvalidValue;  // the outer-bit tables cover 32 bits
     const uint64_t tiles = 1ull << (P.n - P.na);
     const unsigned blocks = (unsigned)std::min<uint64_t>(tiles, 148ull * 8);
     const size_t smem = (size_t)2 << P.na;
