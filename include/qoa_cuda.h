@@ -196,7 +196,9 @@ int qoa_set_random_state(qoa_state_t s, uint64_t seed);
 int qoa_compare(qoa_state_t a, qoa_state_t b, double* rel_l2, double* infidelity);
 /* seed_rng (quantum_state.rs:956): seeds the handle's Philox4x32-10 stream. */
 int qoa_seed(qoa_state_t s, uint64_t seed);
-/* NoiseConfig (quantum_state.rs:15-24): mode 0 Ideal, 1 Fixed(p), 2 Random. */
+/* NoiseConfig (quantum_state.rs:15-24): mode 0 Ideal, 1 Fixed(p), 2 Random;
+ * mode 3 = no config at all (the Option's None, a fresh handle's state: no
+ * noise, like Ideal, but saved as null in the JSON checkpoint). */
 int qoa_set_noise(qoa_state_t s, int mode, double p);
 /* Selects the Philox stream of the noise and MEASURE draws (one per Pauli
  * trajectory) and restarts its event counter. No reference counterpart: the
@@ -352,8 +354,12 @@ int qoa_exe_trace(const uint8_t* file, size_t len, uint32_t flags, uint64_t max_
                   size_t* nops, qoa_exe_result* res, char* out_text, size_t out_cap, size_t* out_len);
 
 /* ---- checkpoint I/O ------------------------------------------------------- */
-/* Binary: the stored amplitudes and norm2 exactly ("QOAS" v1, checksummed),
- * any size or precision; a save/load round trip is bit-exact. */
+/* Binary: the stored amplitudes and norm2 exactly ("QOAS" version 2,
+ * checksummed), any size or precision, with the handle's generator state
+ * (seed, noise trajectory and draw counters, measurement draws), noise
+ * configuration and status words, so that a loaded handle continues the same
+ * trajectory; a save/load round trip is bit-exact. Version-1 files (amplitudes
+ * and norm2 only) still load, with a fresh handle's generator state. */
 int qoa_state_save(qoa_state_t s, const char* path);
 int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out);
 /* JSON in the reference's --save-state / --load-state layout: serde_json of

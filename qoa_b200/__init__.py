@@ -308,7 +308,11 @@ class QuantumState:
         _check(lib.qoa_state_load(os.fsencode(path), flags, ctypes.byref(h)))
         p = ctypes.c_int()
         _check(lib.qoa_get_precision(h, ctypes.byref(p)), h)
-        return cls._adopt(h, "f32" if p.value == QOA_PREC_F32 else "f64", flags)
+        st = cls._adopt(h, "f32" if p.value == QOA_PREC_F32 else "f64", flags)
+        m, q = ctypes.c_int(), ctypes.c_double()
+        _check(lib.qoa_get_noise(h, ctypes.byref(m), ctypes.byref(q)), h)
+        st.noise_config = [None, NoiseConfig.Fixed(q.value), NoiseConfig.Random()][m.value]
+        return st
 
     def save_json(self, path: str, registers: Sequence[float] = ()):
         """The reference's serde JSON checkpoint of (QuantumState, registers)."""
@@ -473,7 +477,7 @@ class QuantumState:
 
     def set_noise_config(self, cfg: Optional[NoiseConfig]):
         self.noise_config = cfg
-        mode, p = (0, 0.0) if cfg is None else (cfg.mode, cfg.p)
+        mode, p = (3, 0.0) if cfg is None else (cfg.mode, cfg.p)  # 3: no config (the Option's None)
         _check(lib.qoa_set_noise(self._h, mode, p), self._h)
 
     def get_noise_config(self):

@@ -29,6 +29,16 @@ namespace qoa {
 void note_global_error(const char* msg);
 }
 
+namespace qoa {
+struct JsonExtras {
+    bool noise_none;
+    bool div_by_zero;
+    std::vector<double> regs;
+};
+JsonExtras json_extras(qoa_state_t s);
+int set_json_extras(qoa_state_t s, const JsonExtras& x, bool nan, bool overflow);
+}  // namespace qoa
+
 namespace {
 
 constexpr uint32_t kJsonMaxQubits = 26;
@@ -206,12 +216,26 @@ int qoa_state_save_json(qoa_state_t s, const double* regs, size_t nregs, const c
         put_f64(o, a[2 * i + 1]);
         o += ']';
     }
+    // the state's own registers as loaded (a fresh state: max(n, 10) zeros)
+    const qoa::JsonExtras ex = qoa::json_extras(s);
     o += "],\n    \"regs\": [";
-    const uint32_t nr = n > 10 ? n : 10;
-    for (uint32_t i = 0; i < nr; ++i) o += i ? ",[0.0,0.0]" : "[0.0,0.0]";
+    if (!ex.regs.empty()) {
+        for (size_t i = 0; i + 1 < ex.regs.size(); i += 2) {
+            o += i ? ",[" : "[";
+            put_f64(o, ex.regs[i]);
+            o += ',';
+            put_f64(o, ex.regs[i + 1]);
+            o += ']';
+        }
+    } else {
+        const uint32_t nr = n > 10 ? n : 10;
+        for (uint32_t i = 0; i < nr; ++i) o += i ? ",[0.0,0.0]" : "[0.0,0.0]";
+    }
     o += "],\n    \"status\": {\"nan\": ";
     o += st.nan_seen ? "true" : "false";
-    o += ", \"div_by_zero\": false, \"overflow\": ";
+    o += ", \"div_by_zero\": ";
+    o += ex.div_by_zero ? "true" : "false";
+    o += ", \"overflow\": ";
     o += st.inf_seen ? "true" : "false";
     o += "},\n    \"noise_config\": ";
     if (mode == 2) o += "\"Random\"";
@@ -220,7 +244,7 @@ int qoa_state_save_json(qoa_state_t s, const double* regs, size_t nregs, const c
         put_f64(o, p);
         o += "}";
     } else {
-        o += "null";
+        o += ex.noise_none ? "null" : "\"Ideal\"";  // Option::None against Some(Ideal)
     }
     o += "\n  },\n  [";
     for (size_t i = 0; i < nregs; ++i) {
@@ -248,9 +272,17 @@ int qoa_state_load_json(const char* path, uint32_t flags, qoa_state_t* out, doub
     std::fclose(f);
     J j{text.data(), text.data() + text.size(), ""};
     double nd = -1;
-    std::vector<double> amps, rl;
+    std::vector<double> amps, rl, sregs;
     int mode = 0;
     double p = 0;
+    bool none = true, nan = false, dbz = false, ovf = false;
+    // a JSON boolean
+    auto flag = [&](bool& v) {
+        if (j.word("true")) v = true;
+        else if (j.word("false")) v = false;
+        else return false;
+        return true;
+    };
     bool ok = j.expect('[') && j.expect('{');
     if (ok && !j.lit('}')) {
         do {
@@ -260,8 +292,11 @@ int qoa_state_load_json(const char* path, uint32_t flags, qoa_state_t* out, doub
             else if (key == "amps") ok = j.complex_list(amps);
             else if (key == "noise_config") {
                 std::string t;
-                if (j.word("null")) mode = 0;
-                else if (j.lit('{')) {
+                none = false;
+                if (j.word("null")) {
+                    mode = 0;
+                    none = true;
+                } else if (j.lit('{')) {
                     ok = j.str(t) && j.expect(':') && j.num(p) && j.expect('}');
                     if (ok && t != "Fixed") { ok = false; j.err = "unknown noise_config"; }
                     mode = 1;
@@ -271,8 +306,24 @@ int qoa_state_load_json(const char* path, uint32_t flags, qoa_state_t* out, doub
                     else if (t == "Ideal") mode = 0;
                     else if (ok) { ok = false; j.err = "unknown noise_config"; }
                 }
+            } else if (key == "regs") {
+                ok = j.complex_list(sregs);
+            } else if (key == "status") {
+                // {"nan": b, "div_by_zero": b, "overflow": b}
+                ok = j.expect('{');
+                if (ok && !j.lit('}')) {
+                    do {
+                        std::string k2;
+                        if (!(ok = j.str(k2) && j.expect(':'))) break;
+                        if (k2 == "nan") ok = flag(nan);
+                        else if (k2 == "div_by_zero") ok = flag(dbz);
+                        else if (k2 == "overflow") ok = flag(ovf);
+                        else ok = j.skip_value();
+                    } while (ok && j.lit(','));
+                    ok = ok && j.expect('}');
+                }
             } else {
-                ok = j.skip_value();  // regs, status: not engine state
+                ok = j.skip_value();
             }
         } while (ok && j.lit(','));
         ok = ok && j.expect('}');
@@ -286,7 +337,8 @@ int qoa_state_load_json(const char* path, uint32_t flags, qoa_state_t* out, doub
     qoa_state_t s = nullptr;
     int rc = qoa_create(n, QOA_PREC_F64, flags, &s);
     if (rc) return rc;
-    if ((rc = qoa_set_noise(s, mode, p)) || (rc = qoa_set_state(s, amps.data(), amps.size() * sizeof(double)))) {
+    if ((rc = qoa_set_noise(s, mode, p)) || (rc = qoa_set_state(s, amps.data(), amps.size() * sizeof(double))) ||
+        (rc = qoa::set_json_extras(s, qoa::JsonExtras{none, dbz, sregs}, nan, ovf))) {
         qoa_destroy(s);
         return rc;
     }

@@ -198,6 +198,13 @@ struct qoa_state_s {
     double noise_p = 0.0;
     uint64_t launches = 0;
     uint32_t host_resets = 0;     // normalize() resets decided on the host
+    // The reference's serde JSON view that the engine does not otherwise
+    // keep: noise_config None (never set) as opposed to Some(Ideal), the
+    // Status.div_by_zero flag, and the QuantumState's own registers
+    // (complex pairs), restored by a JSON load and written back on save.
+    bool noise_none = true;
+    bool div_by_zero = false;
+    std::vector<double> json_regs;
     std::shared_ptr<void> plans;    // PlanCache: plans of repeated op lists
     int jit_mode = QOA_JIT_ASYNC;   // generated complex128 pass kernels (qoa_jit.cpp)
     uint32_t jit_min_qubits = 20;   // smaller states interpret their passes
@@ -2610,6 +2617,25 @@ int batch_refresh_graph(qoa_batch_t b) {
 }  // namespace
 
 // ==================================================================== C ABI
+namespace qoa {
+// The serde-only fields above, for qoa_checkpoint.cpp.
+struct JsonExtras {
+    bool noise_none;
+    bool div_by_zero;
+    std::vector<double> regs;
+};
+JsonExtras json_extras(qoa_state_t s) { return JsonExtras{s->noise_none, s->div_by_zero, s->json_regs}; }
+int set_json_extras(qoa_state_t s, const JsonExtras& x, bool nan, bool overflow) {
+    s->noise_none = x.noise_none;
+    s->div_by_zero = x.div_by_zero;
+    s->json_regs = x.regs;
+    const uint32_t w[2] = {nan ? 1u : 0u, overflow ? 1u : 0u};
+    CK(cudaMemcpyAsync(s->status, w, sizeof w, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return QOA_OK;
+}
+}  // namespace qoa
+
 extern "C" {
 
 const char* qoa_strerror(int code) {
@@ -2884,9 +2910,10 @@ int qoa_seed(qoa_state_t s, uint64_t seed) {
 
 int qoa_set_noise(qoa_state_t s, int mode, double p) {
     if (!s) return set_err(nullptr, QOA_E_ARG, "null handle");
-    if (mode < 0 || mode > 2 || (mode == 1 && !(p >= 0.0 && p <= 1.0))) return set_err(s, QOA_E_ARG, "bad noise config");
-    s->noise_mode = mode;
-    s->noise_p = p;
+    if (mode < 0 || mode > 3 || (mode == 1 && !(p >= 0.0 && p <= 1.0))) return set_err(s, QOA_E_ARG, "bad noise config");
+    s->noise_none = mode == 3;  // Option::None: no noise, like Ideal
+    s->noise_mode = mode == 3 ? 0 : mode;
+    s->noise_p = mode == 1 ? p : 0.0;
     return QOA_OK;
 }
 
@@ -3206,6 +3233,18 @@ uint64_t ckpt_mix(uint64_t w, uint64_t i) {
     x *= 0xBF58476D1CE4E5B9ull;
     return x ^ (x >> 29);
 }
+
+// The version-2 header fields, mixed into the checksum ahead of the amplitudes.
+uint64_t ckpt_header_sum(const uint64_t (&rng)[4], const int32_t (&mode)[2], double noise_p,
+                         const uint32_t (&words)[6], uint64_t& word) {
+    uint64_t sum = 0, bits = 0;
+    for (uint64_t x : rng) sum += ckpt_mix(x, word++);
+    sum += ckpt_mix((uint64_t)(uint32_t)mode[0] | ((uint64_t)(uint32_t)mode[1] << 32), word++);
+    std::memcpy(&bits, &noise_p, 8);
+    sum += ckpt_mix(bits, word++);
+    for (int k = 0; k < 6; k += 2) sum += ckpt_mix((uint64_t)words[k] | ((uint64_t)words[k + 1] << 32), word++);
+    return sum;
+}
 }  // namespace
 
 int qoa_state_save(qoa_state_t s, const char* path) {
@@ -3219,15 +3258,27 @@ int qoa_state_save(qoa_state_t s, const char* path) {
     CK(cudaMemcpyAsync(s->host_scal, s->scal, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     const double norm2 = s->host_scal[0];
-    const uint32_t hdr[4] = {0x53414f51u /* "QOAS" */, 1u, (uint32_t)s->precision, s->n};
+    // version 2: after the amplitudes' header, the handle's noise and
+    // measurement generator state and its status words, so that a loaded
+    // handle continues the same trajectory and reports the same status
+    uint32_t status[4];
+    CK(cudaMemcpyAsync(status, s->status, sizeof status, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const uint32_t hdr[4] = {0x53414f51u /* "QOAS" */, 2u, (uint32_t)s->precision, s->n};
+    const uint64_t rng[4] = {s->seed, s->noise_stream, s->noise_event, s->meas_draws};
+    const int32_t mode[2] = {s->noise_mode, s->noise_none ? 1 : 0};
+    const uint32_t words[6] = {status[0], status[1], status[2], status[3], s->host_resets, 0u};
     bool ok = std::fwrite(hdr, sizeof hdr, 1, f) == 1 && std::fwrite(&norm2, 8, 1, f) == 1 &&
-              std::fwrite(&bytes, 8, 1, f) == 1;
+              std::fwrite(&bytes, 8, 1, f) == 1 && std::fwrite(rng, sizeof rng, 1, f) == 1 &&
+              std::fwrite(mode, sizeof mode, 1, f) == 1 && std::fwrite(&s->noise_p, 8, 1, f) == 1 &&
+              std::fwrite(words, sizeof words, 1, f) == 1;
     void* stage = nullptr;
     if (ok && cudaMallocHost(&stage, kCkptChunk) != cudaSuccess) {
         std::fclose(f);
         return set_err(s, QOA_E_OOM, "pinned staging buffer");
     }
     uint64_t sum = 0, word = 0;
+    sum += ckpt_header_sum(rng, mode, s->noise_p, words, word);
     for (uint64_t off = 0; ok && off < bytes; off += kCkptChunk) {
         const size_t k = (size_t)std::min<uint64_t>(kCkptChunk, bytes - off);
         if (cudaMemcpyAsync(stage, (const unsigned char*)s->amps + off, k, cudaMemcpyDeviceToHost, s->stream) !=
@@ -3255,10 +3306,22 @@ int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out) {
     uint32_t hdr[4];
     double norm2 = 0;
     uint64_t bytes = 0;
-    if (std::fread(hdr, sizeof hdr, 1, f) != 1 || hdr[0] != 0x53414f51u || hdr[1] != 1u ||
+    if (std::fread(hdr, sizeof hdr, 1, f) != 1 || hdr[0] != 0x53414f51u || (hdr[1] != 1u && hdr[1] != 2u) ||
         std::fread(&norm2, 8, 1, f) != 1 || std::fread(&bytes, 8, 1, f) != 1) {
         std::fclose(f);
-        return set_err(nullptr, QOA_E_ARG, "%s is not a version-1 state checkpoint", path);
+        return set_err(nullptr, QOA_E_ARG, "%s is not a state checkpoint (version 1 or 2)", path);
+    }
+    // version 2 carries the generator state and status words (version 1:
+    // a fresh handle's, i.e. seed 0, noise off, clear status)
+    uint64_t rng[4] = {0, 0, 0, 0};
+    int32_t mode[2] = {0, 0};
+    double noise_p = 0.0;
+    uint32_t words[6] = {0, 0, 0, 0, 0, 0};
+    if (hdr[1] == 2u && (std::fread(rng, sizeof rng, 1, f) != 1 || std::fread(mode, sizeof mode, 1, f) != 1 ||
+                         std::fread(&noise_p, 8, 1, f) != 1 || std::fread(words, sizeof words, 1, f) != 1 ||
+                         mode[0] < 0 || mode[0] > 2)) {
+        std::fclose(f);
+        return set_err(nullptr, QOA_E_ARG, "%s: truncated checkpoint header", path);
     }
     const int prec = (int)hdr[2];
     const uint32_t n = hdr[3];
@@ -3280,6 +3343,7 @@ int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out) {
         return set_err(nullptr, QOA_E_OOM, "pinned staging buffer");
     }
     uint64_t sum = 0, word = 0, want = 0;
+    if (hdr[1] == 2u) sum += ckpt_header_sum(rng, mode, noise_p, words, word);
     bool ok = true;
     for (uint64_t off = 0; ok && off < bytes; off += kCkptChunk) {
         const size_t k = (size_t)std::min<uint64_t>(kCkptChunk, bytes - off);
@@ -3300,13 +3364,23 @@ int qoa_state_load(const char* path, uint32_t flags, qoa_state_t* out) {
     }
     s->host_scal[0] = norm2;
     if (cudaMemcpyAsync(s->scal, s->host_scal, sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+        cudaMemcpyAsync(s->status, words, 4 * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess) {
         qoa_destroy(s);
-        return set_err(nullptr, QOA_E_CUDA, "restoring norm2 failed");
+        return set_err(nullptr, QOA_E_CUDA, "restoring norm2 and status failed");
     }
+    s->seed = rng[0];
+    s->noise_stream = rng[1];
+    s->noise_event = rng[2];
+    s->meas_draws = rng[3];
+    s->noise_mode = mode[0];
+    s->noise_p = noise_p;
+    s->noise_none = mode[1] != 0;
+    s->host_resets = words[4];
     *out = s;
     return QOA_OK;
 }
+
 
 int qoa_get_noise(qoa_state_t s, int* mode, double* p) {
     if (!s || !mode || !p) return set_err(s, QOA_E_ARG, "null argument");

@@ -446,25 +446,25 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
     const uint32_t nout = P.n - P.na;
     const uint64_t ntiles = 1ull << nout;
     const uint32_t nchunk = (nout + 7) / 8;  // <= 4: the launcher checks nout <= 32
-    __shared__ uint64_t t_o[4][256], t_po[4][256];
+    // (the partner's offset po is the deposit of pb, so one offset table
+    // serves both; 12 KB of tables keep the kernel under 48 KB of shared
+    // memory with two complex128 tiles)
+    __shared__ uint64_t t_o[4][256];
     __shared__ uint32_t t_pb[4][256];
     __shared__ uint8_t oidx[64];  // qubit -> its position in oq
     for (uint32_t k = threadIdx.x; k < nout; k += blockDim.x) oidx[P.oq[k]] = (uint8_t)k;
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < nchunk * 256; e += blockDim.x) {
         const uint32_t c = e >> 8, x = e & 255;
-        uint64_t o = 0, po = 0;
+        uint64_t o = 0;
         uint32_t pb = 0;
         for (uint32_t i = 0; i < 8; ++i) {
             const uint32_t k = 8 * c + i;
             if (k >= nout || !((x >> i) & 1)) continue;
             o |= 1ull << P.oq[k];
-            const uint32_t q = P.pi[P.oq[k]];
-            po |= 1ull << q;
-            pb |= 1u << oidx[q];
+            pb |= 1u << oidx[P.pi[P.oq[k]]];
         }
         t_o[c][x] = o;
-        t_po[c][x] = po;
         t_pb[c][x] = pb;
     }
     __syncthreads();
@@ -478,9 +478,9 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
         for (uint32_t c = 0; c < nchunk; ++c) {
             const uint32_t x = (uint32_t)(b >> (8 * c)) & 255u;
             o |= t_o[c][x];
-            po |= t_po[c][x];
             pb |= (uint64_t)t_pb[c][x];
         }
+        for (uint32_t c = 0; c < nchunk; ++c) po |= t_o[c][(uint32_t)(pb >> (8 * c)) & 255u];
         if (pb < b) continue;  // uniform over the CTA
         const bool two = pb != b;
         for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {

@@ -32,6 +32,32 @@ def test_binary_checkpoint_round_trip_exact(tmp_path, precision, n):
 
 
 @pytest.mark.gpu
+def test_binary_checkpoint_continues_a_noisy_trajectory(tmp_path):
+    # the checkpoint carries the generator state: a loaded handle draws the
+    # same noise and measurement outcomes as the original would have
+    n = 10
+    first = C.ops_to_array(C.random_layered(n, 3, 5, initial_h=True))
+    rest = C.ops_to_array(C.random_layered(n, 4, 6))
+    path = str(tmp_path / "noisy.qoas")
+
+    def finish(st):
+        st.execute(rest)
+        outs = [st.measure(q) for q in range(n)]
+        return outs, st.get_state_vector(), st.get_status()
+
+    with qb.QuantumState(n, qb.NoiseConfig.Fixed(0.02), seed=99) as st:
+        st.execute(first)
+        st.save(path)
+        want = finish(st)
+    with qb.QuantumState.load(path) as back:
+        assert back.get_noise_config().kind == "fixed"
+        got = finish(back)
+    assert got[0] == want[0]
+    assert np.array_equal(got[1], want[1])
+    assert got[2] == want[2]
+
+
+@pytest.mark.gpu
 def test_binary_checkpoint_detects_corruption(tmp_path):
     path = str(tmp_path / "s.qoas")
     with qb.QuantumState(6) as st:
@@ -66,6 +92,30 @@ def test_json_checkpoint_round_trip(tmp_path):
         assert back.noise_config.kind == "fixed" and back.noise_config.p == 0.125
     assert list(regs) == [1.5, -2.0, 0.0]
     assert np.max(np.abs(got - want)) < 1e-15
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,text", [(None, None), ("ideal", "Ideal")])
+def test_json_checkpoint_keeps_none_ideal_status_and_state_registers(tmp_path, cfg, text):
+    # what a save / load / save cycle through the reference's serde layout
+    # keeps: null against "Ideal", the status flags and the state's own
+    # registers as they were loaded
+    path, path2 = str(tmp_path / "a.json"), str(tmp_path / "b.json")
+    with qb.QuantumState(3, None if cfg is None else qb.NoiseConfig.Ideal()) as st:
+        st.apply_h(0)
+        st.save_json(path)
+    d = json.load(open(path))
+    assert d[0]["noise_config"] == text
+    d[0]["status"] = {"nan": False, "div_by_zero": True, "overflow": True}
+    d[0]["regs"] = [[0.5, -1.0], [2.0, 0.0], [0.0, 3.0]]
+    json.dump(d, open(path, "w"))
+    back, _ = qb.QuantumState.load_json(path)
+    with back:
+        back.save_json(path2)
+    e = json.load(open(path2))
+    assert e[0]["noise_config"] == text
+    assert e[0]["status"] == {"nan": False, "div_by_zero": True, "overflow": True}
+    assert e[0]["regs"] == [[0.5, -1.0], [2.0, 0.0], [0.0, 3.0]]
 
 
 @pytest.mark.gpu
