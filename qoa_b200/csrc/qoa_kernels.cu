@@ -483,29 +483,58 @@ __global__ void __launch_bounds__(256) k_swapnet(T* __restrict__ a, const __grid
         for (uint32_t c = 0; c < nchunk; ++c) po |= t_o[c][(uint32_t)(pb >> (8 * c)) & 255u];
         if (pb < b) continue;  // uniform over the CTA
         const bool two = pb != b;
-        for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
-            const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
-            s0[sp(j)] = __ldcs(a + (o | g));
-            if (two) s1[sp(j)] = __ldcs(a + (po | g));
+        // all of the thread's loads first (tn <= 1024: at most 4 per tile),
+        // so that they are in flight together
+        constexpr int kMax = 1024 / 256;
+        T x0[kMax], x1[kMax];
+#pragma unroll
+        for (int r = 0; r < kMax; ++r) {
+            const uint32_t j = threadIdx.x + 256u * (uint32_t)r;
+            if (j < tn) {
+                const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
+                x0[r] = __ldcs(a + (o | g));
+                if (two) x1[r] = __ldcs(a + (po | g));
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kMax; ++r) {
+            const uint32_t j = threadIdx.x + 256u * (uint32_t)r;
+            if (j < tn) {
+                s0[sp(j)] = x0[r];
+                if (two) s1[sp(j)] = x1[r];
+            }
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < tn; j += blockDim.x) {
-            const uint32_t src = slo[j & ((1u << hl) - 1)] | shi[j >> hl];
-            const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
-            __stcs(a + (po | g), s0[sp(src)]);
-            if (two) __stcs(a + (o | g), s1[sp(src)]);
+#pragma unroll
+        for (int r = 0; r < kMax; ++r) {
+            const uint32_t j = threadIdx.x + 256u * (uint32_t)r;
+            if (j < tn) {
+                const uint32_t src = slo[j & ((1u << hl) - 1)] | shi[j >> hl];
+                const uint64_t g = glo[j & ((1u << hl) - 1)] | ghi[j >> hl];
+                __stcs(a + (po | g), s0[sp(src)]);
+                if (two) __stcs(a + (o | g), s1[sp(src)]);
+            }
         }
         __syncthreads();  // the buffers are reused by the next tile
     }
 }
 
 cudaError_t launch_swapnet(void* a, bool c64, const PermParams& P, cudaStream_t st) {
-    if (P.n - P.na > 32) return cudaErrorInvalidValue;  // the outer-bit tables cover 32 bits
+    // the outer-bit tables cover 32 bits; a tile holds at most 1024 amplitudes
+    if (P.n - P.na > 32 || P.na > 10) return cudaErrorInvalidValue;
     const uint64_t tiles = 1ull << (P.n - P.na);
-    const unsigned blocks = (unsigned)std::min<uint64_t>(tiles, 148ull * 8);
-    const size_t smem = (size_t)2 << P.na;
-    if (c64) k_swapnet<float2><<<blocks, 256, smem * sizeof(float2), st>>>((float2*)a, P);
-    else k_swapnet<double2><<<blocks, 256, smem * sizeof(double2), st>>>((double2*)a, P);
+    const size_t smem = ((size_t)2 << P.na) * (c64 ? sizeof(float2) : sizeof(double2));
+    // persistent: as many CTAs as are resident at once, so none waits for a
+    // slot behind CTAs that walk their whole share of the tiles
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = c64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_swapnet<float2>, 256, smem)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_swapnet<double2>, 256, smem);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * (uint64_t)std::max(per_sm, 1));
+    if (c64) k_swapnet<float2><<<blocks, 256, smem, st>>>((float2*)a, P);
+    else k_swapnet<double2><<<blocks, 256, smem, st>>>((double2*)a, P);
     return cudaGetLastError();
 }
 
