@@ -705,7 +705,9 @@ def serve_stream(reqs, prec: str, workers: int) -> dict:
     return {"value": len(res) / (last - first), "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": last - first,
             "failed": sum(1 for x in res if x["status"] != 0), "by_qubits": buckets,
-            "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": workers}
+            "peak_hbm_reserved_gb": st["peak_bytes_reserved"] / (1 << 30), "workers": workers,
+            "trajectories_batched": int(st["trajectories_batched"]),
+            "trajectories": int(sum(r["trajectories"] for r in reqs))}
 
 
 def serve_cpu_baseline(reqs, seconds: float) -> dict:

@@ -255,6 +255,26 @@ int qoa_batch_jit_info(qoa_batch_t b, uint32_t* structures, uint32_t* ready, uin
 /* Algorithmic bytes of one run's arena tile passes (each pass reads and
  * writes its circuit's state once) and the number of pass rounds. */
 int qoa_batch_traffic(qoa_batch_t b, double* arena_pass_bytes, uint32_t* rounds);
+/* Trajectory `trajectory` of a noisy circuit as a batch circuit, sampled
+ * after the run: the ops expanded with the depolarising draws that qoa_apply
+ * makes on a state given qoa_seed(seed), qoa_set_noise(1, noise_p) and
+ * qoa_set_trajectory(trajectory) (noise_p = 0: none), then `shots` outcomes
+ * of the final state by the inverse-CDF rule of qoa_sample mode 1, one
+ * uniform each from u. Unitary ops only (QOA_E_OPCODE otherwise). Returns
+ * QOA_E_RANGE, with the circuit added, where qoa_apply would skip an op. The
+ * serving form runs a request's trajectories this way. */
+int qoa_batch_add_trajectory(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, uint64_t seed,
+                             double noise_p, uint64_t trajectory, const double* u, uint32_t shots, uint32_t* id);
+/* The outcomes of circuit id (count = its shots) after qoa_batch_run. */
+int qoa_batch_shots(qoa_batch_t b, uint32_t id, uint64_t* out, size_t count);
+/* Empties a batch for reuse: its circuits and device buffers go, its streams
+ * and tuning stay. */
+int qoa_batch_reset(qoa_batch_t b);
+/* Host threads that plan the batch's circuits (0, the default: all cores). */
+int qoa_batch_set_host_threads(qoa_batch_t b, uint32_t threads);
+/* *unitary = 1 when every op expands to unitary gates (no measurement,
+ * reset or QINIT), i.e. the ops can run as batch circuits. */
+int qoa_ops_unitary(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int* unitary);
 const char* qoa_batch_last_error(qoa_batch_t b);
 int qoa_batch_destroy(qoa_batch_t b);
 
@@ -298,6 +318,7 @@ typedef struct qoa_request_result {
 typedef struct qoa_server_stats {
     uint64_t submitted, done, queued, admitted, trajectories_running, states_resident;
     uint64_t bytes_reserved, peak_bytes_reserved;
+    uint64_t trajectories_batched;  /* trajectories that ran in batch chunks */
 } qoa_server_stats;
 int qoa_server_create(const qoa_server_config* cfg, qoa_server_t* out);
 int qoa_server_submit(qoa_server_t s, const qoa_request* req, uint64_t* id);

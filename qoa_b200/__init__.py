@@ -85,7 +85,8 @@ class RequestResult(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "done", "queued", "admitted", "trajectories_running",
-                                               "states_resident", "bytes_reserved", "peak_bytes_reserved")]
+                                               "states_resident", "bytes_reserved", "peak_bytes_reserved",
+                                               "trajectories_batched")]
 
 
 _EXTRA_SIGS: dict = {}
@@ -134,6 +135,11 @@ def _load() -> ctypes.CDLL:
         "qoa_batch_info": (i32, [vp, P(u32), P(u32), P(u32), P(u32)]),
         "qoa_batch_traffic": (i32, [vp, P(dbl), P(u32)]),
         "qoa_batch_jit_info": (i32, [vp, P(u32), P(u32), P(u32)]),
+        "qoa_batch_add_trajectory": (i32, [vp, u32, vp, sz, u64, dbl, u64, vp, u32, P(u32)]),
+        "qoa_batch_shots": (i32, [vp, u32, vp, sz]),
+        "qoa_batch_reset": (i32, [vp]),
+        "qoa_batch_set_host_threads": (i32, [vp, u32]),
+        "qoa_ops_unitary": (i32, [u32, u32, vp, sz, P(i32)]),
         "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
         "qoa_batch_destroy": (i32, [vp]),
         "qoa_server_create": (i32, [P(ServerConfig), P(vp)]),
@@ -615,6 +621,35 @@ class Batch:
                                       _ptr(m) if len(m) else None, len(m), ctypes.byref(cid)))
         self._nresults += len(m)
         return cid.value
+
+    def add_trajectory(self, n: int, ops, seed: int, noise_p: float, trajectory: int, u) -> int:
+        """Trajectory `trajectory` of the noisy circuit (the draws a state
+        seeded `seed` with noise level noise_p makes on that trajectory),
+        sampled after the run with one inverse-CDF uniform per shot from u.
+        Out-of-range ops are skipped as in qoa_apply."""
+        arr = np.ascontiguousarray(ops if isinstance(ops, np.ndarray) else ops_to_array(ops))
+        uu = np.ascontiguousarray(np.asarray(u, dtype=np.float64).reshape(-1))
+        cid = ctypes.c_uint32()
+        rc = lib.qoa_batch_add_trajectory(self._h, n, _ptr(arr) if len(arr) else None, len(arr), seed, float(noise_p),
+                                          trajectory, _ptr(uu) if len(uu) else None, len(uu), ctypes.byref(cid))
+        if rc != QOA_E_RANGE:
+            self._check(rc)
+        self._keep.append(uu)
+        self._shots = getattr(self, "_shots", {})
+        self._shots[cid.value] = len(uu)
+        return cid.value
+
+    def shots(self, cid: int) -> np.ndarray:
+        out = np.zeros(self._shots[cid], dtype=np.uint64)
+        self._check(lib.qoa_batch_shots(self._h, cid, _ptr(out) if len(out) else None, len(out)))
+        return out
+
+    def reset(self):
+        """Empties the batch for reuse (circuits and device buffers go)."""
+        self._check(lib.qoa_batch_reset(self._h))
+        self._nresults = 0
+        self._keep = []
+        self._shots = {}
 
     def tuning(self) -> dict:
         t = BatchTuning()

@@ -3,7 +3,9 @@
 // Each CTA repeatedly takes the next circuit index from a global atomic
 // counter (no waiting on other CTAs), builds |0..0> of that circuit in shared
 // memory, applies its gate list there, and reduces its Z-string expectation
-// values straight from shared memory, so a small state never travels to HBM.
+// values straight from shared memory, so a small state never travels to HBM
+// (unless the circuit is sampled afterwards: then its final state is written
+// out for the sampler).
 // Circuits of up to SMALL_MAX_F64 (complex128) or SMALL_MAX_F32 (complex64)
 // qubits fit; larger ones go through the tile passes of the engine.
 #include <cuda_runtime.h>
@@ -86,6 +88,8 @@ __global__ void k_small_batch(const SmallCircuit* __restrict__ circs, uint32_t c
         for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) s[i] = Cx<T>::make(i == 0 ? 1.0 : 0.0, 0.0);
         __syncthreads();
         for (uint32_t k = 0; k < ci.op_count; ++k) small_apply<T>(s, ci.n, ops[ci.op_start + k]);
+        if (ci.state_out)  // sampled after the run: the state goes to HBM
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) reinterpret_cast<T*>(ci.state_out)[i] = s[i];
         // <Z_mask> of the normalised state, 8 masks per sweep
         for (uint32_t m0 = 0; m0 < ci.mask_count; m0 += 8) {
             double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -226,6 +230,70 @@ cudaError_t launch_arena_expz(bool f32, const ExpzJob* jobs, uint32_t njobs, uin
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_arena_expz_final<<<njobs, 256, 0, st>>>(jobs, partials, out);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------------------
+// Shots of sampled batch circuits: one CTA per circuit builds the marginal
+// tree of its final state in global scratch (level k, 1 <= k < n, holds the
+// 2^k sums over qubits k..n-1 at tree + 2^k - 2, as k_tree_leaf / k_tree_up
+// lay it out), then each thread takes shots and walks the tree from qubit 0:
+// the inverse-CDF rule of k_sample mode 1 (bit q = 0 while the remaining mass
+// is below the marginal of that prefix). The tree is not divided by the norm:
+// the states of a batch are unit vectors up to rounding, and t = u x total
+// scales with it.
+__device__ __forceinline__ double samp_abs2(const double2* a, uint64_t i) {
+    const double2 x = a[i];
+    return fma(x.x, x.x, x.y * x.y);
+}
+__device__ __forceinline__ double samp_abs2(const float2* a, uint64_t i) {
+    const float2 x = a[i];
+    return (double)x.x * x.x + (double)x.y * x.y;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_sample_jobs(const SampleJob* __restrict__ jobs, const double* __restrict__ u,
+                                                      unsigned long long* __restrict__ out) {
+    const SampleJob J = jobs[blockIdx.x];
+    const T* a = reinterpret_cast<const T*>(J.amps);
+    const uint32_t n = J.n;
+    double* tree = J.tree;
+    if (n >= 2) {
+        const uint64_t half = 1ull << (n - 1);
+        double* leaf = tree + (half - 2);
+        for (uint64_t p = threadIdx.x; p < half; p += blockDim.x) leaf[p] = samp_abs2(a, p) + samp_abs2(a, p + half);
+        __syncthreads();
+        for (int k = (int)n - 2; k >= 1; --k) {
+            const uint64_t cnt = 1ull << k;
+            const double* hi = tree + ((2ull << k) - 2);
+            double* lo = tree + (cnt - 2);
+            for (uint64_t p = threadIdx.x; p < cnt; p += blockDim.x) lo[p] = hi[p] + hi[p + cnt];
+            __syncthreads();
+        }
+    }
+    auto h = [&](uint32_t k, uint64_t p) -> double {
+        if (k == n) return samp_abs2(a, p);
+        if (k == 0) return n == 1 ? samp_abs2(a, 0) + samp_abs2(a, 1) : tree[0] + tree[1];
+        return tree[((1ull << k) - 2) + p];
+    };
+    for (uint32_t s = threadIdx.x; s < J.shots; s += blockDim.x) {
+        double t = u[J.u_start + s] * h(0, 0);
+        uint64_t pre = 0;
+        for (uint32_t q = 0; q < n; ++q) {
+            const double left = h(q + 1, pre);
+            if (t < left) continue;
+            t -= left;
+            pre |= 1ull << q;
+        }
+        out[J.out_start + s] = pre;
+    }
+}
+
+cudaError_t launch_sample_jobs(bool f32, const SampleJob* jobs, uint32_t njobs, const double* u,
+                               unsigned long long* out, cudaStream_t st) {
+    if (!njobs) return cudaSuccess;
+    if (f32) k_sample_jobs<float2><<<njobs, 1024, 0, st>>>(jobs, u, out);
+    else k_sample_jobs<double2><<<njobs, 1024, 0, st>>>(jobs, u, out);
     return cudaGetLastError();
 }
 

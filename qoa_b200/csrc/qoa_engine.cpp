@@ -76,6 +76,8 @@ cudaError_t launch_f32_pass_arena(const ArenaJob* jobs, uint32_t njobs, const ui
                                   const F32Phase* phases, const float2* tables, uint32_t* status, cudaStream_t st);
 cudaError_t launch_arena_expz(bool f32, const ExpzJob* jobs, uint32_t njobs, uint32_t chunks, const uint64_t* masks,
                               double* partials, double* out, cudaStream_t st);
+cudaError_t launch_sample_jobs(bool f32, const SampleJob* jobs, uint32_t njobs, const double* u,
+                               unsigned long long* out, cudaStream_t st);
 cudaError_t launch_small_batch(bool f32, const SmallCircuit* circs, uint32_t count, const SmallOp* ops,
                                const uint64_t* masks, double* out, unsigned int* counter, int max_n, int threads,
                                int ctas_per_sm, cudaStream_t st);
@@ -2023,10 +2025,14 @@ struct qoa_batch_s {
         std::vector<uint64_t> masks;
         uint32_t out_start;
         int route;
-        size_t state_off;  // arena / view: offset of the state in the arena
+        size_t state_off;  // arena / view (and sampled small circuits): offset of the state in the arena
+        uint32_t shots = 0;        // inverse-CDF shots of the final state
+        uint64_t shot_start = 0;   // its uniforms in shot_u and its outcomes in the shot output
     };
     std::vector<Circ> circs;
     uint32_t nresults = 0;
+    std::vector<double> shot_u;    // every sampled circuit's uniforms, in order of addition
+    unsigned host_threads = 0;     // planning threads (0: all host cores)
     bool prepared = false;
     uint64_t runs = 0;
     // device
@@ -2063,6 +2069,12 @@ struct qoa_batch_s {
     ExpzJob* d_ejobs = nullptr;
     uint32_t n_ejobs = 0, e_chunks = 0;
     double* d_epart = nullptr;
+    // sampled circuits (qoa_batch_add_trajectory)
+    double* d_shot_u = nullptr;
+    unsigned long long* d_shot_out = nullptr;
+    SampleJob* d_sjobs = nullptr;
+    double* d_trees = nullptr;
+    uint32_t n_sjobs = 0;
     // view route
     std::vector<qoa_state_t> views;
     std::vector<int> view_circ;
@@ -2118,9 +2130,21 @@ SmallOp to_small(const Gate& g) {
 }
 
 template <typename T>
-void dfree(T*& p) {
-    if (p) cudaFree((void*)p);
+void dfree(T*& p, cudaStream_t st) {
+    if (p) cudaFreeAsync((void*)p, st);  // stream-ordered: no device-wide synchronisation
     p = nullptr;
+}
+
+// Device buffers of a batch come from the stream-ordered allocator on the
+// batch's first stream (a freed batch returns its memory to the pool without
+// synchronising the device, which matters when many batches come and go, as
+// in the server's trajectory chunks).
+template <typename T>
+cudaError_t dalloc(qoa_batch_t b, T*& dst, size_t bytes) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocAsync(&p, bytes, b->streams[0]);
+    dst = static_cast<T*>(p);
+    return e;
 }
 
 void batch_free_device(qoa_batch_t b) {
@@ -2131,8 +2155,14 @@ void batch_free_device(qoa_batch_t b) {
     for (qoa_state_t v : b->views) qoa_destroy(v);
     b->views.clear();
     b->view_circ.clear();
-    dfree(b->arena); dfree(b->d_small); dfree(b->d_ops); dfree(b->d_masks); dfree(b->d_out); dfree(b->d_counter);
-    dfree(b->d_params); dfree(b->d_f32); dfree(b->d_jobs); dfree(b->d_tstart); dfree(b->d_ejobs); dfree(b->d_epart);
+    // every stream of a run is joined into stream 0, so frees ordered there
+    // follow all of the batch's work
+    cudaStream_t st = b->streams.empty() ? nullptr : b->streams[0];
+    dfree(b->arena, st); dfree(b->d_small, st); dfree(b->d_ops, st); dfree(b->d_masks, st); dfree(b->d_out, st);
+    dfree(b->d_counter, st); dfree(b->d_params, st); dfree(b->d_f32, st); dfree(b->d_jobs, st); dfree(b->d_tstart, st);
+    dfree(b->d_ejobs, st); dfree(b->d_epart, st);
+    dfree(b->d_shot_u, st); dfree(b->d_shot_out, st); dfree(b->d_sjobs, st); dfree(b->d_trees, st);
+    b->n_sjobs = 0;
     b->rounds.clear();
     b->jit_kernels.clear();
     b->graph_jit = false;
@@ -2144,14 +2174,21 @@ void batch_free_device(qoa_batch_t b) {
 
 template <typename T>
 int upload(qoa_batch_t b, T*& dst, const std::vector<T>& src) {
-    BCK(cudaMalloc((void**)&dst, std::max<size_t>(1, src.size()) * sizeof(T)));
-    if (!src.empty()) BCK(cudaMemcpy((void*)dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    BCK(dalloc(b, dst, std::max<size_t>(1, src.size()) * sizeof(T)));
+    if (!src.empty())
+        BCK(cudaMemcpyAsync((void*)dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, b->streams[0]));
     return QOA_OK;
 }
 
-// fn(0) .. fn(count - 1) on all host cores
-void parallel_for(size_t count, const std::function<void(size_t)>& fn) {
-    const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+// fn(0) .. fn(count - 1) on `threads` host threads (0: all host cores, at
+// most 64; 1: this thread)
+void parallel_for(size_t count, const std::function<void(size_t)>& fn, unsigned threads = 0) {
+    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+    if (threads) nt = std::min(nt, threads);
+    if (nt == 1 || count <= 1) {
+        for (size_t k = 0; k < count; ++k) fn(k);
+        return;
+    }
     std::atomic<size_t> next{0};
     std::vector<std::thread> pool;
     for (unsigned t = 0; t < nt; ++t)
@@ -2204,6 +2241,16 @@ struct PassShape {
 };
 
 int batch_prepare(qoa_batch_t b) {
+    // streams first: the device buffers are allocated in stream 0's order
+    const uint32_t nstreams = std::max<uint32_t>(1, b->tune.streams);
+    while (b->streams.size() < nstreams) {
+        cudaStream_t st;
+        BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        b->streams.push_back(st);
+        cudaEvent_t ev;
+        BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->events.push_back(ev);
+    }
     const bool f32 = b->precision == QOA_PREC_F32;
     const uint32_t cap = f32 ? SMALL_MAX_F32 : SMALL_MAX_F64;
     const uint32_t smax = std::min<uint32_t>(b->tune.small_max_n, cap);
@@ -2248,7 +2295,7 @@ int batch_prepare(qoa_batch_t b) {
             bool ok = true;
             for (const Step& st : steps_of[i]) ok = ok && st.pass;
             all_pass[i] = ok;
-        });
+        }, b->host_threads);
         size_t np = 0;
         std::vector<std::pair<size_t, size_t>> jobs;  // (circuit, step)
         for (size_t i = 0; i < NC; ++i)
@@ -2263,7 +2310,7 @@ int batch_prepare(qoa_batch_t b) {
             const size_t i = jobs[x].first, k = jobs[x].second;
             step_ok[x] = build_pass(b->circs[i].gates, steps_of[i][k], b->circs[i].n, p64[pbase[i] + k],
                                     b->precision == QOA_PREC_F32) == 0;
-        });
+        }, b->host_threads);
         for (size_t i = 0; i < NC; ++i) built_ok[i] = all_pass[i];
         for (size_t x = 0; x < jobs.size(); ++x)
             if (!step_ok[x]) built_ok[jobs[x].first] = 0;
@@ -2282,8 +2329,13 @@ int batch_prepare(qoa_batch_t b) {
             d.mask_start = mask_start[i];
             d.mask_count = (uint32_t)c.masks.size();
             d.out_start = c.out_start;
+            d.state_out = nullptr;  // set once the arena exists
             sc.push_back(d);
             maxn = std::max(maxn, c.n);
+            if (c.shots) {  // its final state is sampled from the arena
+                c.state_off = total;
+                total = al(total + (esz << c.n));
+            }
             continue;
         }
         if (tensor && c.n < (uint32_t)TILE_BITS)
@@ -2322,32 +2374,70 @@ int batch_prepare(qoa_batch_t b) {
         total = al(total + 16 * sizeof(double));
         total = al(total + 4 * sizeof(uint32_t));
     }
+    // sampled circuits: marginal-tree scratch (2^n - 2 doubles each)
+    std::vector<size_t> tree_off(NC, 0);
+    size_t tree_total = 0;
+    uint64_t shot_total = 0;
+    for (size_t i = 0; i < NC; ++i) {
+        const auto& c = b->circs[i];
+        if (!c.shots) continue;
+        tree_off[i] = tree_total;
+        tree_total += c.n >= 2 ? (1ull << c.n) - 2 : 1;
+        shot_total = std::max<uint64_t>(shot_total, c.shot_start + c.shots);
+    }
     b->nsmall = (uint32_t)sc.size();
     b->small_max_n_used = maxn;
-    BCK(cudaMalloc(&b->d_out, std::max<size_t>(1, b->nresults) * sizeof(double)));
+    BCK(dalloc(b, b->d_out, std::max<size_t>(1, b->nresults) * sizeof(double)));
     // [0] the small-circuit ticket counter, [1] the tensor passes' status word
-    BCK(cudaMalloc(&b->d_counter, 2 * sizeof(unsigned int)));
-    BCK(cudaMemset(b->d_counter, 0, 2 * sizeof(unsigned int)));
+    BCK(dalloc(b, b->d_counter, 2 * sizeof(unsigned int)));
+    BCK(cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(unsigned int), b->streams[0]));
     int rc;
     if ((rc = upload(b, b->d_masks, masks))) return rc;
+    if (total) BCK(dalloc(b, b->arena, total));
+    unsigned char* arena = (unsigned char*)b->arena;
     if (!sc.empty()) {
+        size_t k = 0;
+        for (size_t i = 0; i < NC; ++i) {
+            if (b->circs[i].route != R_SMALL) continue;
+            if (b->circs[i].shots) sc[k].state_out = arena + b->circs[i].state_off;
+            ++k;
+        }
         if ((rc = upload(b, b->d_small, sc))) return rc;
         if ((rc = upload(b, b->d_ops, sops))) return rc;
     }
-    if (total) BCK(cudaMalloc(&b->arena, total));
-    unsigned char* arena = (unsigned char*)b->arena;
+    if (shot_total) {
+        std::vector<SampleJob> sj;
+        BCK(dalloc(b, b->d_trees, std::max<size_t>(1, tree_total) * sizeof(double)));
+        for (size_t i = 0; i < NC; ++i) {
+            const auto& c = b->circs[i];
+            if (!c.shots) continue;
+            SampleJob J;
+            memset(&J, 0, sizeof J);
+            J.amps = arena + c.state_off;
+            J.tree = b->d_trees + tree_off[i];
+            J.n = c.n;
+            J.shots = c.shots;
+            J.u_start = c.shot_start;
+            J.out_start = c.shot_start;
+            sj.push_back(J);
+        }
+        if ((rc = upload(b, b->d_sjobs, sj))) return rc;
+        if ((rc = upload(b, b->d_shot_u, b->shot_u))) return rc;
+        BCK(dalloc(b, b->d_shot_out, shot_total * sizeof(unsigned long long)));
+        b->n_sjobs = (uint32_t)sj.size();
+    }
 
     // arena rounds
     const size_t psz = tensor ? sizeof(F32PassParams) : sizeof(PassParams);
     if (tensor ? !p32.empty() : !p64.empty()) {
-        BCK(cudaMalloc(&b->d_params, (tensor ? p32.size() : p64.size()) * psz));
-        BCK(cudaMemcpy(b->d_params, tensor ? (const void*)p32.data() : (const void*)p64.data(),
-                       (tensor ? p32.size() : p64.size()) * psz, cudaMemcpyHostToDevice));
+        BCK(dalloc(b, b->d_params, (tensor ? p32.size() : p64.size()) * psz));
+        BCK(cudaMemcpyAsync(b->d_params, tensor ? (const void*)p32.data() : (const void*)p64.data(),
+                            (tensor ? p32.size() : p64.size()) * psz, cudaMemcpyHostToDevice, b->streams[0]));
     }
     if (tensor && !p32.empty()) {
         std::vector<unsigned char> img = f32_pack(up, b->f32_off);
-        BCK(cudaMalloc(&b->d_f32, img.size()));
-        BCK(cudaMemcpy(b->d_f32, img.data(), img.size(), cudaMemcpyHostToDevice));
+        BCK(dalloc(b, b->d_f32, img.size()));
+        BCK(cudaMemcpyAsync(b->d_f32, img.data(), img.size(), cudaMemcpyHostToDevice, b->streams[0]));
     }
     std::vector<ArenaJob> jobs;
     std::vector<uint32_t> tstart;
@@ -2361,7 +2451,7 @@ int batch_prepare(qoa_batch_t b) {
     std::vector<uint32_t> reps;  // representative pass of each structure
     if (jit) {
         std::vector<uint64_t> hs(p64.size());
-        parallel_for(p64.size(), [&](size_t k) { hs[k] = PassShape{&p64[k]}.hash(); });
+        parallel_for(p64.size(), [&](size_t k) { hs[k] = PassShape{&p64[k]}.hash(); }, b->host_threads);
         std::unordered_map<uint64_t, std::vector<int>> by_hash;
         for (auto& v : pass_idx)
             for (uint32_t pi : v) {
@@ -2386,7 +2476,7 @@ int batch_prepare(qoa_batch_t b) {
         std::vector<std::string> bodies(reps.size());
         parallel_for(reps.size(), [&](size_t k) {
             bodies[k] = f32 ? jit_pass32_body(p64[reps[k]], true) : jit_pass_body(p64[reps[k]], true);
-        });
+        }, b->host_threads);
         b->jit_kernels = jit_request(bodies, b->tune.jit == QOA_JIT_SYNC ? JitWhen::WAIT : JitWhen::NOW);
     }
     for (size_t r = 0; r < maxp; ++r) {
@@ -2470,7 +2560,7 @@ int batch_prepare(qoa_batch_t b) {
     b->e_chunks = chunks;
     if (!ej.empty()) {
         if ((rc = upload(b, b->d_ejobs, ej))) return rc;
-        BCK(cudaMalloc(&b->d_epart, parts * sizeof(double)));
+        BCK(dalloc(b, b->d_epart, parts * sizeof(double)));
     }
 
     if (jit && b->rstreams.empty()) {
@@ -2486,16 +2576,7 @@ int batch_prepare(qoa_batch_t b) {
         }
     }
 
-    // streams
-    const uint32_t ns = std::max<uint32_t>(1, b->tune.streams);
-    while (b->streams.size() < ns) {
-        cudaStream_t st;
-        BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        b->streams.push_back(st);
-        cudaEvent_t ev;
-        BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        b->events.push_back(ev);
-    }
+    const uint32_t ns = (uint32_t)b->streams.size();
 
     // view handles
     size_t k = 0;
@@ -2519,7 +2600,7 @@ int batch_prepare(qoa_batch_t b) {
         v->scal = (double*)(base + o);
         o = al(o + 16 * sizeof(double));
         v->status = (uint32_t*)(base + o);
-        BCK(cudaMemset(v->status, 0, 4 * sizeof(uint32_t)));
+        BCK(cudaMemsetAsync(v->status, 0, 4 * sizeof(uint32_t), b->streams[0]));
         if (tensor) {
             rc = f32_prepare(v, c.gates);
             if (rc) { std::string m = v->err; qoa_destroy(v); return bset_err(b, rc, m.c_str()); }
@@ -2591,6 +2672,7 @@ int batch_enqueue(qoa_batch_t b) {
         BCK(cudaStreamWaitEvent(s0, b->events[i], 0));
     }
     BCK(launch_arena_expz(f32, b->d_ejobs, b->n_ejobs, b->e_chunks, b->d_masks, b->d_epart, b->d_out, s0));
+    BCK(launch_sample_jobs(f32, b->d_sjobs, b->n_sjobs, b->d_shot_u, b->d_shot_out, s0));
     b->graph_jit = all_ready;
     return QOA_OK;
 }
@@ -3092,6 +3174,101 @@ int qoa_batch_add(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, con
     b->nresults += (uint32_t)nmasks;
     if (id) *id = (uint32_t)b->circs.size();
     b->circs.push_back(std::move(c));
+    return QOA_OK;
+}
+
+int qoa_batch_add_trajectory(qoa_batch_t b, uint32_t n, const qoa_op* ops, size_t nops, uint64_t seed,
+                             double noise_p, uint64_t trajectory, const double* u, uint32_t shots, uint32_t* id) {
+    if (!b || (!ops && nops) || (!u && shots)) return bset_err(b, QOA_E_ARG, "null argument");
+    if (b->prepared) return bset_err(b, QOA_E_ARG, "batch already ran; reset it to add circuits");
+    if (n < 1 || n > 40) return bset_err(b, QOA_E_ARG, "bad qubit count");
+    if (!(noise_p >= 0.0 && noise_p <= 1.0)) return bset_err(b, QOA_E_ARG, "bad noise level");
+    // the noise draws of a state seeded `seed` on trajectory `trajectory` with
+    // qoa_set_noise(mode 1, noise_p): the same Expander over a host-only
+    // noise context, so the gates are those qoa_apply would insert
+    qoa_state_s ctx;
+    ctx.n = n;
+    ctx.flags = b->flags;
+    ctx.seed = seed;
+    ctx.noise_mode = noise_p > 0.0 ? 1 : 0;
+    ctx.noise_p = noise_p;
+    ctx.noise_stream = trajectory;
+    ctx.noise_event = 0;
+    Expander ex;
+    ex.n = n;
+    ex.flags = b->flags;
+    ex.s = &ctx;
+    ex.out.reserve(nops * 2 + 8);
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    if (ex.first_err != QOA_OK && ex.first_err != QOA_E_RANGE) return bset_err(b, ex.first_err, ex.err.c_str());
+    for (const Gate& g : ex.out)
+        if (g.kind > K_U2) return bset_err(b, QOA_E_OPCODE, "batched circuits take unitary ops only");
+    qoa_batch_s::Circ c;
+    c.n = n;
+    c.gates = std::move(ex.out);
+    c.out_start = b->nresults;
+    c.route = R_VIEW;
+    c.state_off = 0;
+    c.shots = shots;
+    c.shot_start = b->shot_u.size();
+    b->shot_u.insert(b->shot_u.end(), u, u + shots);
+    if (id) *id = (uint32_t)b->circs.size();
+    b->circs.push_back(std::move(c));
+    if (ex.first_err == QOA_E_RANGE) {  // the op was skipped, the circuit added (qoa_apply's rule)
+        bset_err(b, QOA_E_RANGE, ex.err.c_str());
+        return QOA_E_RANGE;
+    }
+    return QOA_OK;
+}
+
+int qoa_batch_shots(qoa_batch_t b, uint32_t id, uint64_t* out, size_t count) {
+    if (!b || (!out && count)) return bset_err(b, QOA_E_ARG, "null argument");
+    if (id >= b->circs.size()) return bset_err(b, QOA_E_ARG, "no such circuit");
+    if (count != b->circs[id].shots) return bset_err(b, QOA_E_ARG, "count must equal the circuit's shots");
+    if (!b->prepared || !b->runs) return bset_err(b, QOA_E_ARG, "run the batch first");
+    cudaSetDevice(b->device);
+    BCK(cudaStreamSynchronize(b->streams[0]));
+    if (count)
+        BCK(cudaMemcpy(out, b->d_shot_out + b->circs[id].shot_start, count * sizeof(uint64_t),
+                       cudaMemcpyDeviceToHost));
+    return QOA_OK;
+}
+
+int qoa_batch_reset(qoa_batch_t b) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    cudaSetDevice(b->device);
+    for (cudaStream_t st : b->streams) BCK(cudaStreamSynchronize(st));
+    for (cudaStream_t st : b->rstreams) BCK(cudaStreamSynchronize(st));
+    batch_free_device(b);
+    b->circs.clear();
+    b->nresults = 0;
+    b->shot_u.clear();
+    return QOA_OK;
+}
+
+int qoa_batch_set_host_threads(qoa_batch_t b, uint32_t threads) {
+    if (!b) return bset_err(nullptr, QOA_E_ARG, "null batch");
+    b->host_threads = threads;
+    return QOA_OK;
+}
+
+int qoa_ops_unitary(uint32_t n, uint32_t flags, const qoa_op* ops, size_t nops, int* unitary) {
+    if ((!ops && nops) || !unitary) return set_err(nullptr, QOA_E_ARG, "null argument");
+    if (n < 1 || n > 40) return set_err(nullptr, QOA_E_ARG, "bad qubit count");
+    Expander ex;
+    ex.n = n;
+    ex.flags = flags;
+    ex.s = nullptr;  // noise adds Paulis only: unitary either way
+    for (size_t i = 0; i < nops; ++i) {
+        ex.cur = (int)i;
+        ex.op(ops[i]);
+    }
+    bool ok = ex.first_err == QOA_OK || ex.first_err == QOA_E_RANGE;
+    for (const Gate& g : ex.out) ok = ok && g.kind <= K_U2;
+    *unitary = ok ? 1 : 0;
     return QOA_OK;
 }
 

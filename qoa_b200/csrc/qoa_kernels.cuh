@@ -233,6 +233,19 @@ struct SmallCircuit {
     uint32_t op_start, op_count;
     uint32_t mask_start, mask_count;
     uint32_t out_start;
+    void* state_out;  // where the final state is written (circuits that are sampled), else null
+};
+
+// A batch circuit sampled after the run (qoa_batch.cu, k_sample_jobs): its
+// final state, scratch for its marginal tree (2^n - 2 doubles), and its shots'
+// uniforms and outcomes (inverse CDF, one uniform per shot).
+struct SampleJob {
+    const void* amps;
+    double* tree;
+    uint32_t n;
+    uint32_t shots;
+    uint64_t u_start;
+    uint64_t out_start;
 };
 
 // ---------------------------------------------------------------------------

@@ -10,12 +10,19 @@
 //
 // Scheduling (continuous batching):
 //  - requests queue in arrival order;
-//  - each worker thread runs one trajectory at a time on a state handle of its
-//    own stream; workers take the next trajectory of the oldest admitted
-//    request, so the trajectories of several requests overlap on the device;
-//  - a request is admitted when a worker is free and a state of its size fits
-//    in the HBM budget (idle states of other sizes are freed to make room);
-//    states stay resident and are reused by later trajectories of that size.
+//  - a worker takes the next unit of work of the oldest admitted request, so
+//    the work of several requests overlaps on the device. A unit is
+//      * a chunk of trajectories run as one batch (qoa_batch_add_trajectory:
+//        every trajectory a batch circuit, its shots sampled on the device),
+//        for requests of unitary ops on up to kBatchMaxQubits qubits — a
+//        chunk is one launch per pass round for all of its trajectories
+//        instead of one launch per pass and trajectory; a noiseless request's
+//        trajectories are one circuit, sampled with all of their uniforms;
+//      * otherwise one trajectory on a pooled state handle of the worker's
+//        size (its own stream), reused by later trajectories of that size;
+//  - a unit starts when its memory (a state, or a chunk's states) fits in the
+//    HBM budget beside the running ones (idle pooled states of other sizes are
+//    freed to make room).
 // Every finished request holds its outcomes until qoa_server_take_shots.
 #include <cuda_runtime.h>
 
@@ -41,6 +48,10 @@ void note_global_error(const char* msg);
 namespace {
 
 constexpr uint32_t kShotStream = 0x73686f74u;  // "shot"
+// Trajectory chunks: requests of up to this many qubits, chunks of up to
+// kChunkBytes of states (and the budget) each.
+constexpr uint32_t kBatchMaxQubits = 22;
+constexpr size_t kChunkBytes = size_t(2) << 30;
 
 struct Request {
     uint64_t id = 0;
@@ -53,6 +64,8 @@ struct Request {
     uint32_t trajectories = 1, shots = 1;
     uint64_t seed = 0;
     uint32_t next_traj = 0, started = 0, done_traj = 0;
+    bool batched = false;   // trajectories run in chunks of `chunk` as batches
+    uint32_t chunk = 1;
     int status = QOA_OK;
     std::string err;
     double t_submit = 0, t_admit = -1, t_start = -1, t_done = -1;
@@ -89,6 +102,8 @@ struct qoa_server_s {
     std::deque<uint64_t> completed;                    // not yet polled
     std::list<Slot> slots;
     size_t bytes_reserved = 0, peak_bytes = 0;
+    size_t chunk_bytes = 0;                            // reserved by running chunks
+    uint64_t traj_batched = 0;
     uint64_t next_id = 1, use_clock = 0;
     uint64_t n_submitted = 0, n_done = 0, traj_running = 0;
     std::vector<std::thread> workers;
@@ -106,10 +121,37 @@ struct qoa_server_s {
     }
 
     size_t busy_bytes() const {
-        size_t b = 0;
+        size_t b = chunk_bytes;
         for (const Slot& s : slots)
             if (s.busy) b += s.bytes;
         return b;
+    }
+
+    // Memory a request's next unit needs.
+    size_t unit_bytes(const Request* q) const {
+        const size_t fp = footprint(q->n, q->precision);
+        if (!q->batched) return fp;
+        const uint32_t k = std::min(q->chunk, q->trajectories - q->next_traj);
+        return q->noise_p > 0.0 ? fp * k : fp;  // a noiseless chunk is one circuit
+    }
+
+    // Under the lock: reserves `need` bytes for a chunk, freeing idle pooled
+    // states (least recently used first); false when the budget does not
+    // allow it now.
+    bool acquire_bytes(size_t need, std::vector<qoa_state_t>& to_free) {
+        while (bytes_reserved + need > cfg.hbm_budget_bytes) {
+            auto victim = slots.end();
+            for (auto it = slots.begin(); it != slots.end(); ++it)
+                if (!it->busy && (victim == slots.end() || it->last_use < victim->last_use)) victim = it;
+            if (victim == slots.end()) return false;
+            if (victim->h) to_free.push_back(victim->h);
+            bytes_reserved -= victim->bytes;
+            slots.erase(victim);
+        }
+        bytes_reserved += need;
+        chunk_bytes += need;
+        peak_bytes = std::max(peak_bytes, bytes_reserved);
+        return true;
     }
 
     // Under the lock: an idle state of (n, precision), or room for a new one
@@ -137,24 +179,47 @@ struct qoa_server_s {
         return &slots.back();
     }
 
-    // Under the lock: the next trajectory to run (request, index, slot).
-    bool next_work(Request*& r, uint32_t& t, Slot*& slot, std::vector<qoa_state_t>& to_free) {
+    // A unit of work: trajectories [t, t + count) of request r, on a pooled
+    // state (slot) or, for a chunk, as a batch holding `bytes`.
+    struct Unit {
+        Request* r = nullptr;
+        uint32_t t = 0, count = 1;
+        Slot* slot = nullptr;
+        size_t bytes = 0;
+    };
+
+    // Under the lock: the next unit to run.
+    bool next_work(Unit& u, std::vector<qoa_state_t>& to_free) {
         for (;;) {
             for (Request* q : admitted) {
                 if (q->next_traj >= q->trajectories) continue;
-                Slot* s = acquire(q->n, q->precision, to_free);
-                if (!s) continue;
-                r = q;
-                t = q->next_traj++;
-                q->started++;
-                slot = s;
+                if (q->batched) {
+                    const size_t need = unit_bytes(q);
+                    if (!acquire_bytes(need, to_free)) continue;
+                    u.r = q;
+                    u.t = q->next_traj;
+                    u.count = std::min(q->chunk, q->trajectories - q->next_traj);
+                    u.slot = nullptr;
+                    u.bytes = need;
+                    q->next_traj += u.count;
+                    q->started += u.count;
+                } else {
+                    Slot* s = acquire(q->n, q->precision, to_free);
+                    if (!s) continue;
+                    u.r = q;
+                    u.t = q->next_traj++;
+                    u.count = 1;
+                    u.slot = s;
+                    u.bytes = 0;
+                    q->started++;
+                }
                 if (q->t_start < 0) q->t_start = now();
                 return true;
             }
             // nothing runnable among the admitted: admit the next arrival
             if (queue.empty()) return false;
             Request* q = queue.front();
-            const size_t need = footprint(q->n, q->precision);
+            const size_t need = unit_bytes(q);
             if (need > cfg.hbm_budget_bytes) {
                 queue.pop_front();
                 q->status = QOA_E_OOM;
@@ -172,16 +237,23 @@ struct qoa_server_s {
         }
     }
 
-    void finish_traj(Request* r, Slot* slot, int rc, const std::string& msg) {
-        slot->busy = false;
-        slot->last_use = ++use_clock;
-        traj_running--;
+    void finish_unit(const Unit& u, int rc, const std::string& msg) {
+        Request* r = u.r;
+        if (u.slot) {
+            u.slot->busy = false;
+            u.slot->last_use = ++use_clock;
+        } else {
+            bytes_reserved -= u.bytes;
+            chunk_bytes -= u.bytes;
+            traj_batched += u.count;
+        }
+        traj_running -= u.count;
         if (rc != QOA_OK && r->status == QOA_OK) {
             r->status = rc;
             r->err = msg;
             r->next_traj = r->trajectories;  // start none of its other trajectories
         }
-        r->done_traj++;
+        r->done_traj += u.count;
         if (r->next_traj >= r->trajectories && r->done_traj == r->started) {
             r->t_done = now();
             admitted.remove(r);
@@ -214,33 +286,92 @@ struct qoa_server_s {
         return qoa_sample(h, u.data(), r->shots, 1, r->out.data() + (size_t)t * r->shots);
     }
 
+    // Trajectories [t0, t0 + count) of r as one batch of worker-owned
+    // handle b (reset after the run); their shots go to r->out.
+    int run_chunk(Request* r, uint32_t t0, uint32_t count, qoa_batch_t b, std::string& msg) {
+        int rc = QOA_OK;
+        std::vector<double> u;
+        auto fail = [&](int code) {
+            const char* m = qoa_batch_last_error(b);
+            msg = m ? m : "";
+            qoa_batch_reset(b);
+            return code;
+        };
+        // a noiseless request's trajectories share one final state: one
+        // circuit, sampled with every trajectory's uniforms in order
+        const bool one = !(r->noise_p > 0.0);
+        const uint32_t ncirc = one ? 1 : count;
+        const uint32_t per = one ? count * r->shots : r->shots;
+        std::vector<uint32_t> ids(ncirc);
+        for (uint32_t c = 0; c < ncirc; ++c) {
+            u.resize(per);
+            for (uint32_t k = 0; k < per; ++k) {
+                const uint32_t t = one ? t0 + k / r->shots : t0 + c;
+                const uint32_t shot = one ? k % r->shots : k;
+                u[k] = qoa_philox_uniform(r->seed, t ^ kShotStream, shot, 0);
+            }
+            rc = qoa_batch_add_trajectory(b, r->n, r->ops.data(), r->ops.size(), r->seed, r->noise_p, t0 + c,
+                                          u.data(), per, &ids[c]);
+            if (rc && rc != QOA_E_RANGE) return fail(rc);  // out-of-range ops are skipped, as in the reference
+        }
+        if ((rc = qoa_batch_run(b))) return fail(rc);
+        for (uint32_t c = 0; c < ncirc; ++c)
+            if ((rc = qoa_batch_shots(b, ids[c], r->out.data() + (size_t)(t0 + c) * r->shots, per))) return fail(rc);
+        qoa_batch_reset(b);
+        return QOA_OK;
+    }
+
     void worker() {
         cudaSetDevice(device);
+        qoa_batch_t batches[2] = {nullptr, nullptr};  // this worker's chunk batches, by precision
         std::unique_lock<std::mutex> lk(mu);
         for (;;) {
-            Request* r = nullptr;
-            uint32_t t = 0;
-            Slot* slot = nullptr;
+            Unit u;
             std::vector<qoa_state_t> to_free;
-            while (!stop && !next_work(r, t, slot, to_free)) {
+            while (!stop && !next_work(u, to_free)) {
                 for (qoa_state_t h : to_free) qoa_destroy(h);
                 to_free.clear();
                 cv_work.wait(lk);
             }
-            if (!r) return;  // stopping
-            traj_running++;
+            if (!u.r) break;  // stopping
+            traj_running += u.count;
             lk.unlock();
             for (qoa_state_t h : to_free) qoa_destroy(h);
-            const int rc = run_traj(r, t, slot);
+            int rc;
             std::string msg;
-            if (rc) {
-                const char* m = qoa_last_error(slot->h);
-                msg = m ? m : "";
+            if (u.slot) {
+                rc = run_traj(u.r, u.t, u.slot);
+                if (rc) {
+                    const char* m = qoa_last_error(u.slot->h);
+                    msg = m ? m : "";
+                }
+            } else {
+                const int pi = u.r->precision == QOA_PREC_F32 ? 1 : 0;
+                rc = QOA_OK;
+                if (!batches[pi]) {
+                    rc = qoa_batch_create(u.r->precision, cfg.flags & ~QOA_FLAG_F32_TENSOR, &batches[pi]);
+                    if (!rc) {
+                        qoa_batch_tuning tu;
+                        qoa_batch_get_tuning(batches[pi], &tu);
+                        tu.streams = 1;           // a chunk's circuits are one size: arena or small route
+                        tu.jit = QOA_JIT_OFF;     // noisy trajectories rarely share a pass structure
+                        qoa_batch_set_tuning(batches[pi], &tu);
+                        qoa_batch_set_host_threads(batches[pi], 1);  // the workers are the parallelism
+                    } else {
+                        batches[pi] = nullptr;
+                        const char* m = qoa_last_error(nullptr);
+                        msg = m ? m : "";
+                    }
+                }
+                if (!rc) rc = run_chunk(u.r, u.t, u.count, batches[pi], msg);
             }
             lk.lock();
-            finish_traj(r, slot, rc, msg);
+            finish_unit(u, rc, msg);
             cv_work.notify_all();
         }
+        lk.unlock();
+        for (qoa_batch_t b : batches)
+            if (b) qoa_batch_destroy(b);
     }
 };
 
@@ -313,6 +444,19 @@ int qoa_server_submit(qoa_server_t s, const qoa_request* req, uint64_t* id) {
         }
     }
     r->out.assign((size_t)r->trajectories * r->shots, 0);
+    // trajectory chunks for unitary requests of up to kBatchMaxQubits qubits
+    // (the tensor-core block form keeps its per-state path); the chunk size
+    // depends on the request and the configuration only, so a result does not
+    // depend on the other requests
+    int unitary = 0;
+    const bool tensor = r->precision == QOA_PREC_F32 && (s->cfg.flags & QOA_FLAG_F32_TENSOR);
+    if (r->n <= kBatchMaxQubits && !tensor &&
+        qoa_ops_unitary(r->n, s->cfg.flags, r->ops.data(), r->ops.size(), &unitary) == QOA_OK && unitary) {
+        const size_t fp = footprint(r->n, r->precision);
+        const size_t cap = std::min(kChunkBytes, (size_t)s->cfg.hbm_budget_bytes);
+        r->batched = true;
+        r->chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(r->trajectories, cap / fp));
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     r->id = s->next_id++;
     r->t_submit = s->now();
@@ -392,6 +536,7 @@ int qoa_server_get_stats(qoa_server_t s, qoa_server_stats* out) {
     out->states_resident = s->slots.size();
     out->bytes_reserved = s->bytes_reserved;
     out->peak_bytes_reserved = s->peak_bytes;
+    out->trajectories_batched = s->traj_batched;
     return QOA_OK;
 }
 

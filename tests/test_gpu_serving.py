@@ -109,3 +109,61 @@ def test_request_over_budget_is_rejected():
         assert res and res[0]["id"] == rid and res[0]["status"] == qb.QOA_E_OOM
         with pytest.raises(qb.QoaError):
             srv.take_shots(rid, 1)
+
+
+def state_path_shots(n, ops, p, seed, t, u, precision):
+    """One trajectory the way the server runs it on a pooled state handle."""
+    with qb.QuantumState(n, precision=precision) as st:
+        st.seed_rng(seed)
+        st.set_noise_config(qb.NoiseConfig.Fixed(p) if p > 0 else None)
+        st.set_trajectory(t)
+        st.apply_reset_all()
+        st.execute(ops)
+        return st.sample(len(u), u=u, mode=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("n", [6, 12, 14, 16])
+def test_batch_trajectories_match_state_path(precision, n):
+    # trajectories as batch circuits (shared-memory route for small n, arena
+    # tile passes above) give the shots of the per-state path: the same noise
+    # draws, the same inverse-CDF rule
+    p, seed, S = 0.03, 777 + n, 24
+    ops = C.ops_to_array(C.random_layered(n, 5, 300 + n))
+    b = qb.Batch(precision)
+    ids, us = [], []
+    for t in range(4):
+        u = np.array([qb.philox_uniform(seed, t ^ qb.SHOT_STREAM, k, 0) for k in range(S)])
+        us.append(u)
+        ids.append(b.add_trajectory(n, ops, seed, p, t, u))
+    b.run()
+    for t in range(4):
+        got = b.shots(ids[t])
+        ref = state_path_shots(n, ops, p, seed, t, us[t], precision)
+        assert np.array_equal(got, ref), (t, got, ref)
+    # reuse after reset: a noiseless circuit sampled with many uniforms
+    b.reset()
+    u = np.array([qb.philox_uniform(seed, 5 ^ qb.SHOT_STREAM, k, 0) for k in range(3 * S)])
+    cid = b.add_trajectory(n, ops, seed, 0.0, 0, u)
+    b.run()
+    assert np.array_equal(b.shots(cid), state_path_shots(n, ops, 0.0, seed, 0, u, precision))
+
+
+@pytest.mark.gpu
+def test_server_runs_trajectory_chunks_and_per_state_fallback():
+    reqs = requests(seed=3, count=4, nmin=8, nmax=16)
+    meas = dict(n=6, ops=C.ops_to_array([C.Op(C.H, [0]), C.Op(C.CNOT, [0, 1]), C.Op(C.MEASURE, [0]),
+                                         C.Op(C.H, [2])]),
+                noise_p=0.01, trajectories=3, shots=5, seed=99)
+    with qb.Server("f64", hbm_budget_gb=4, workers=4) as srv:
+        shots, res = run(srv, reqs + [meas])
+        st = srv.stats()
+    # the unitary requests ran as batch chunks, the measuring one per state
+    assert st["trajectories_batched"] == sum(r["trajectories"] for r in reqs)
+    for r, got in zip(reqs, shots):
+        for t in (0, r["trajectories"] - 1):
+            u = np.array([qb.philox_uniform(r["seed"], t ^ qb.SHOT_STREAM, k, 0) for k in range(r["shots"])])
+            ref = state_path_shots(r["n"], r["ops"], r["noise_p"], r["seed"], t, u, "f64")
+            assert np.array_equal(got[t * r["shots"]:(t + 1) * r["shots"]], ref)
+    assert res[-1]["status"] == 0 and len(shots[-1]) == 15
