@@ -335,6 +335,11 @@ int qoa_server_destroy(qoa_server_t s);
  * counter (event lo, event hi, slot, stream); noise draws of trajectory t use
  * stream t, slots 2q+1 (hit test) and 2q+2 (Pauli type) of gate event e. */
 double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32_t slot);
+/* The hit tests of gate event `event` on trajectory `stream`: bit q (q < n <=
+ * 64) set where qoa_philox_uniform(seed, stream, event, 2q + 1) < p, i.e.
+ * the qubits that receive a Pauli (its type: slot 2q + 2, < 1/3 X, < 2/3 Y,
+ * else Z). */
+uint64_t qoa_noise_hits(uint64_t seed, uint32_t stream, uint64_t event, uint32_t n, double p);
 
 /* ---- bytecode front-end: .qexe / .qx programs -------------------------- */
 /* File = 4-byte magic ("QEXE","OEXE","QOX ","XEXE","QEX ","QX\0\0"), version

@@ -139,6 +139,7 @@ def _load() -> ctypes.CDLL:
         "qoa_batch_shots": (i32, [vp, u32, vp, sz]),
         "qoa_batch_reset": (i32, [vp]),
         "qoa_batch_set_host_threads": (i32, [vp, u32]),
+        "qoa_noise_hits": (u64, [u64, u32, u64, u32, dbl]),
         "qoa_ops_unitary": (i32, [u32, u32, vp, sz, P(i32)]),
         "qoa_batch_last_error": (ctypes.c_char_p, [vp]),
         "qoa_batch_destroy": (i32, [vp]),

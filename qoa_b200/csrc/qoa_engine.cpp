@@ -126,6 +126,77 @@ double uniform01(uint64_t seed, uint64_t stream, uint64_t event, uint32_t slot) 
 }
 const uint64_t kMeasStreamXor = 0x6d656173ull;
 
+// The hit tests of one gate event: bit q of the result is set when
+// uniform01(seed, stream, event, 2q + 1) < p, for q < n (n <= 64). The same
+// draws as one uniform01 call per qubit, computed W counters at a time
+// in structure-of-arrays form so that the rounds vectorise (AVX-512 or AVX2
+// where the host has it: a noisy circuit draws one uniform per qubit per
+// gate).
+template <int W>
+inline uint64_t hits8(uint32_t k0, uint32_t k1, uint32_t e0, uint32_t e1, uint32_t st, uint32_t q0, uint32_t n,
+                      double p) {
+    uint32_t c0[W], c1[W], c2[W], c3[W];
+    for (int i = 0; i < W; ++i) {
+        c0[i] = e0;
+        c1[i] = e1;
+        c2[i] = 2u * (q0 + (uint32_t)i) + 1u;
+        c3[i] = st;
+    }
+    for (int r = 0; r < 10; ++r) {
+        for (int i = 0; i < W; ++i) {
+            const uint64_t p0 = (uint64_t)0xD2511F53u * c0[i];
+            const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2[i];
+            const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1[i] ^ k0;
+            const uint32_t n1 = (uint32_t)p1;
+            const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3[i] ^ k1;
+            const uint32_t n3 = (uint32_t)p0;
+            c0[i] = n0; c1[i] = n1; c2[i] = n2; c3[i] = n3;
+        }
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    uint64_t h = 0;
+    for (int i = 0; i < W; ++i) {
+        const uint64_t bits = ((uint64_t)c0[i] << 32) | c1[i];
+        const double r = (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+        if (q0 + (uint32_t)i < n && r < p) h |= 1ull << (q0 + (uint32_t)i);
+    }
+    return h;
+}
+uint64_t noise_hits_generic(uint64_t seed, uint64_t stream, uint64_t event, uint32_t n, double p) {
+    uint64_t h = 0;
+    for (uint32_t q0 = 0; q0 < n; q0 += 8)
+        h |= hits8<8>((uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)event, (uint32_t)(event >> 32),
+                      (uint32_t)stream, q0, n, p);
+    return h;
+}
+#if defined(__x86_64__) && defined(__GNUC__)
+__attribute__((target("avx2"))) uint64_t noise_hits_avx2(uint64_t seed, uint64_t stream, uint64_t event, uint32_t n,
+                                                         double p) {
+    uint64_t h = 0;
+    for (uint32_t q0 = 0; q0 < n; q0 += 8)
+        h |= hits8<8>((uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)event, (uint32_t)(event >> 32),
+                      (uint32_t)stream, q0, n, p);
+    return h;
+}
+__attribute__((target("avx512f"))) uint64_t noise_hits_avx512(uint64_t seed, uint64_t stream, uint64_t event,
+                                                              uint32_t n, double p) {
+    uint64_t h = 0;
+    for (uint32_t q0 = 0; q0 < n; q0 += 16)
+        h |= hits8<16>((uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)event, (uint32_t)(event >> 32),
+                       (uint32_t)stream, q0, n, p);
+    return h;
+}
+#endif
+uint64_t noise_hits(uint64_t seed, uint64_t stream, uint64_t event, uint32_t n, double p) {
+#if defined(__x86_64__) && defined(__GNUC__)
+    static const int isa = __builtin_cpu_supports("avx512f") ? 2 : __builtin_cpu_supports("avx2") ? 1 : 0;
+    if (isa == 2) return noise_hits_avx512(seed, stream, event, n, p);
+    if (isa == 1) return noise_hits_avx2(seed, stream, event, n, p);
+#endif
+    return noise_hits_generic(seed, stream, event, n, p);
+}
+
 // ------------------------------------------------------------------ gates
 enum GateKind { K_G1 = 0, K_DIAG = 1, K_SWAP = 2, K_U2 = 3, K_MEASURE = 4, K_RESET = 5, K_RESETALL = 6, K_QINIT = 7,
                 K_PERM = 8 /* a block of disjoint SWAPs, made by the executor */ };
@@ -312,20 +383,19 @@ struct Expander {
         double p = s->noise_p;
         if (s->noise_mode == 2) p = 0.1 + 0.9 * uniform01(s->seed, s->noise_stream, ev, 0);
         if (s->noise_mode == 1 && !(p > 0.0)) return;
-        for (uint32_t q = 0; q < n; ++q) {
-            if ((flags & QOA_FLAG_NOISE_GATE_QUBITS) && !((touched >> q) & 1)) continue;
-            const double r = uniform01(s->seed, s->noise_stream, ev, 2 * q + 1);
-            if (r < p) {
-                const double u2 = uniform01(s->seed, s->noise_stream, ev, 2 * q + 2);
-                int e = (int)(u2 * 3.0);
-                if (e > 2) e = 2;
-                Gate g;
-                g.src = cur;
-                if (e == 0) g1(g, q, G1_X, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
-                else if (e == 1) g1(g, q, G1_Y, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
-                else diag_neg(g, 1ull << q);
-                out.push_back(g);
-            }
+        uint64_t hit = noise_hits(s->seed, s->noise_stream, ev, n, p);
+        if (flags & QOA_FLAG_NOISE_GATE_QUBITS) hit &= touched;
+        for (; hit; hit &= hit - 1) {  // hit qubits in ascending order, each with its Pauli type draw
+            const uint32_t q = (uint32_t)__builtin_ctzll(hit);
+            const double u2 = uniform01(s->seed, s->noise_stream, ev, 2 * q + 2);
+            int e = (int)(u2 * 3.0);
+            if (e > 2) e = 2;
+            Gate g;
+            g.src = cur;
+            if (e == 0) g1(g, q, G1_X, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
+            else if (e == 1) g1(g, q, G1_Y, d2(0, 0), d2(0, 0), d2(0, 0), d2(0, 0), 0);
+            else diag_neg(g, 1ull << q);
+            out.push_back(g);
         }
     }
 
@@ -3393,6 +3463,10 @@ int qoa_batch_traffic(qoa_batch_t b, double* arena_pass_bytes, uint32_t* rounds)
 
 double qoa_philox_uniform(uint64_t seed, uint32_t stream, uint64_t event, uint32_t slot) {
     return uniform01(seed, stream, event, slot);
+}
+
+uint64_t qoa_noise_hits(uint64_t seed, uint32_t stream, uint64_t event, uint32_t n, double p) {
+    return n > 64 ? 0 : noise_hits(seed, stream, event, n, p);
 }
 
 // ---- checkpoint I/O: exact binary dump of a handle's stored state ------------

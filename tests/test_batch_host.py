@@ -26,3 +26,14 @@ def unitary(n, ops):
 ])
 def test_ops_unitary(ops, want):
     assert unitary(6, ops) == want
+
+
+@pytest.mark.parametrize("n,p", [(1, 0.5), (7, 0.3), (15, 1e-3), (33, 0.05), (40, 0.9), (64, 0.2)])
+def test_noise_hits_equal_one_draw_per_qubit(n, p):
+    # the vectorised hit tests give exactly the per-qubit draws' outcomes
+    for seed, stream, ev in [(1, 0, 0), (123456789012345, 7, 99), (2 ** 63 + 5, 0xFFFFFFFF, 2 ** 40 + 3)]:
+        want = 0
+        for q in range(n):
+            if qb.lib.qoa_philox_uniform(seed, stream, ev, 2 * q + 1) < p:
+                want |= 1 << q
+        assert qb.lib.qoa_noise_hits(seed, stream, ev, n, p) == want
