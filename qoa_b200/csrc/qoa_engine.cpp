@@ -325,13 +325,66 @@ size_t partials_needed(uint32_t n) {
     return std::max(a, b);
 }
 
+// Device buffers of batches come from one stream-ordered memory pool per
+// device that keeps freed memory for the next batch (a batch of thousands of
+// circuits holds tens of GB; mapping that afresh for every batch, or
+// synchronising the device on every free, costs more than the batch's
+// launches). A state allocation that finds the device full first returns the
+// pools' unused memory and tries again.
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t batch_pool(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
+}
+
+// Returns the batch pools' unused memory to the device (after the work that
+// freed it has finished).
+void trim_batch_pools() {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    bool any = false;
+    for (cudaMemPool_t p : g_pools) any = any || p;
+    if (!any) return;
+    cudaDeviceSynchronize();
+    for (cudaMemPool_t p : g_pools)
+        if (p) cudaMemPoolTrimTo(p, 0);
+}
+
+// cudaMalloc, retried once after trimming the batch pools
+cudaError_t device_alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        trim_batch_pools();
+        e = cudaMalloc(p, bytes);
+    }
+    return e;
+}
+
 int alloc_state(qoa_state_t s, uint32_t n) {
     if (s->amps) { cudaFree(s->amps); s->amps = nullptr; }
     if (s->partials) { cudaFree(s->partials); s->partials = nullptr; }
     s->n = n;
-    CK(cudaMalloc(&s->amps, (s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2)) << n));
+    CK(device_alloc((void**)&s->amps, (s->precision == QOA_PREC_F32 ? sizeof(float2) : sizeof(double2)) << n));
     s->partials_cap = partials_needed(n);
-    CK(cudaMalloc(&s->partials, s->partials_cap * sizeof(double)));
+    CK(device_alloc((void**)&s->partials, s->partials_cap * sizeof(double)));
     return QOA_OK;
 }
 
@@ -2205,14 +2258,21 @@ void dfree(T*& p, cudaStream_t st) {
     p = nullptr;
 }
 
-// Device buffers of a batch come from the stream-ordered allocator on the
-// batch's first stream (a freed batch returns its memory to the pool without
-// synchronising the device, which matters when many batches come and go, as
-// in the server's trajectory chunks).
+// Device buffers of a batch: stream-ordered on the batch's first stream, from
+// the device's batch pool (a freed batch's memory goes back to the pool
+// without synchronising the device and serves the next batch, which matters
+// when many batches come and go, as in the server's trajectory chunks).
 template <typename T>
 cudaError_t dalloc(qoa_batch_t b, T*& dst, size_t bytes) {
     void* p = nullptr;
-    const cudaError_t e = cudaMallocAsync(&p, bytes, b->streams[0]);
+    cudaMemPool_t pool = batch_pool(b->device);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, b->streams[0])
+                         : cudaMallocAsync(&p, bytes, b->streams[0]);
+    if (e == cudaErrorMemoryAllocation && pool) {  // memory held elsewhere: retry once after a trim
+        cudaGetLastError();
+        trim_batch_pools();
+        e = cudaMallocFromPoolAsync(&p, bytes, pool, b->streams[0]);
+    }
     dst = static_cast<T*>(p);
     return e;
 }
