@@ -316,6 +316,49 @@ std::string swz_base(const Swizzle& z, const TileMap& m, const int* pos) {
     return e;
 }
 
+// The swizzled accesses arr[pb ^ K] of one exchange half, K the register
+// parts. pb is an XOR of constants selected by the lane and warp bits; above
+// the low three bits those constants and the K are different tile bits, so
+// pb ^ K = (pb ^ (K & 7)) + (K & ~7): one pointer per distinct K & 7, the
+// rest a constant offset that each load or store takes as its immediate
+// instead of an address computation per access. `pb_hi` is the OR of pb's
+// possible constants; where it overlaps a K (no such layout is made) the
+// accesses keep the XOR form. Returns the access expression of each K and
+// emits the pointers (named pfx0..pfx7) as it goes.
+std::vector<std::string> swz_access(Emit& E, const char* arr, const char* pfx, uint32_t pb_hi,
+                                    const std::vector<uint32_t>& ks) {
+    bool disjoint = true;
+    uint32_t lows = 0;
+    for (uint32_t k : ks) {
+        disjoint = disjoint && !(pb_hi & k & ~7u);
+        lows |= 1u << (k & 7u);
+    }
+    std::vector<std::string> out;
+    char b[96];
+    if (!disjoint) {
+        for (uint32_t k : ks) {
+            snprintf(b, sizeof b, "%s[pb ^ %uu]", arr, k);
+            out.push_back(b);
+        }
+        return out;
+    }
+    for (uint32_t m = 0; m < 8; ++m)
+        if ((lows >> m) & 1) E.line("auto* const %s%u = %s + (pb ^ %uu);", pfx, m, arr, m);
+    for (uint32_t k : ks) {
+        snprintf(b, sizeof b, "%s%u[%uu]", pfx, k & 7u, k & ~7u);
+        out.push_back(b);
+    }
+    return out;
+}
+
+// OR of the constants swz_base may XOR into pb (lane and warp bits)
+uint32_t swz_base_bits(const Swizzle& z, const TileMap& m, const int* pos) {
+    uint32_t r = 0;
+    for (int i = 0; i < LANE_BITS; ++i) r |= z.f(1u << pos[m.lane[i]]);
+    for (int i = 0; i < WARP_BITS; ++i) r |= z.f(1u << pos[m.warp[i]]);
+    return r;
+}
+
 }  // namespace
 
 // Kernel head shared by both precisions: the signature, shared memory, the
@@ -495,15 +538,24 @@ const TileMap* emit_ops128(Emit& E, const PassParams& P, bool arena, const char*
                             if ((v >> k) & 1) j |= 1u << m.reg[k];
                         return z.f(j);
                     };
+                    std::vector<uint32_t> ks(REGS);
                     E.line("{ const uint32_t pb = %s;", swz_base(z, mo, pos).c_str());
-                    for (int v = 0; v < REGS; ++v) E.line("tile[pb ^ %uu] = a[%d];", off(mo, v), v);
+                    for (int v = 0; v < REGS; ++v) ks[v] = off(mo, v);
+                    {
+                        const auto acc = swz_access(E, "tile", "ts", swz_base_bits(z, mo, pos), ks);
+                        for (int v = 0; v < REGS; ++v) E.line("%s = a[%d];", acc[v].c_str(), v);
+                    }
                     E.line("}");
                     // an exchange that keeps the warp bits moves data only within
                     // each warp: with the pass's one layout a warp stores to and
                     // loads from its own part of the tile, so a warp barrier does
                     E.line(shared_layout && same_warps(mo, mn) ? "__syncwarp();" : "__syncthreads();");
                     E.line("{ const uint32_t pb = %s;", swz_base(z, mn, pos).c_str());
-                    for (int v = 0; v < REGS; ++v) E.line("a[%d] = tile[pb ^ %uu];", v, off(mn, v));
+                    for (int v = 0; v < REGS; ++v) ks[v] = off(mn, v);
+                    {
+                        const auto acc = swz_access(E, "tile", "tl", swz_base_bits(z, mn, pos), ks);
+                        for (int v = 0; v < REGS; ++v) E.line("a[%d] = %s;", v, acc[v].c_str());
+                    }
                     E.line("}");
                     cur = &mn;
                     break;
@@ -834,16 +886,25 @@ const TileMap* emit_ops64(Emit& E, const PassParams& P, bool arena, const std::v
                         // it last loaded: only the first exchange waits first
                         if (!shared_layout || nxchg == 0) E.line("__syncthreads();");
                         ++nxchg;
+                        std::vector<uint32_t> ks(8);
                         E.line("{ ulonglong2* pt = reinterpret_cast<ulonglong2*>(tile); const uint32_t pb = %s;",
                                swz_base(z, mo, pos).c_str());
-                        for (int j = 0; j < 8; ++j)
-                            E.line("pt[pb ^ %uu] = make_ulonglong2(re[%d], im[%d]);", off(mo, j), j, j);
+                        for (int j = 0; j < 8; ++j) ks[j] = off(mo, j);
+                        {
+                            const auto acc = swz_access(E, "pt", "ts", swz_base_bits(z, mo, pos), ks);
+                            for (int j = 0; j < 8; ++j)
+                                E.line("%s = make_ulonglong2(re[%d], im[%d]);", acc[j].c_str(), j, j);
+                        }
                         E.line("}");
                         E.line(shared_layout && same_warps(mo, mn) ? "__syncwarp();" : "__syncthreads();");
                         E.line("{ const ulonglong2* pt = reinterpret_cast<const ulonglong2*>(tile); const uint32_t pb = %s;",
                                swz_base(z, mn, pos).c_str());
-                        for (int j = 0; j < 8; ++j)
-                            E.line("{ const ulonglong2 u = pt[pb ^ %uu]; re[%d] = u.x; im[%d] = u.y; }", off(mn, j), j, j);
+                        for (int j = 0; j < 8; ++j) ks[j] = off(mn, j);
+                        {
+                            const auto acc = swz_access(E, "pt", "tl", swz_base_bits(z, mn, pos), ks);
+                            for (int j = 0; j < 8; ++j)
+                                E.line("{ const ulonglong2 u = %s; re[%d] = u.x; im[%d] = u.y; }", acc[j].c_str(), j, j);
+                        }
                         E.line("}");
                         cur = &mn;
                         break;

@@ -16,21 +16,33 @@ TERM = re.compile(r"\(\(0u - \(\(\(uint32_t\)(lane|wid) >> (\d)\) & 1u\)\) & 0x(
 
 
 def exchanges(kernel, precision):
-    """[(barrier_before_store, store_units[thread][k], load_units[thread][k], warp_local)]"""
+    """[(barrier_before_store, store_units[thread][k], load_units[thread][k], warp_local)]
+
+    An exchange half declares one pointer per distinct low part m of its
+    swizzled offsets, `ptr_m = tile + (pb ^ m)`, and addresses unit
+    pb ^ (m | K) as ptr_m[K] (K: the offset's bits above the low three, which
+    pb never has); the units below are computed from that form, so the
+    checks also cover the pointer arithmetic."""
+    decl = r"(?:auto\* const t[sl]\d = (?:tile|pt) \+ \(pb \^ \du\);\n)+"
     if precision == "f64":
-        pat = re.compile(r"(__syncthreads\(\);\n)?\{ const uint32_t pb = (0u[^;]*);\n((?:tile\[pb \^ \d+u\] = a\[\d+\];\n){16})\}\n"
-                         r"(__syncthreads\(\);|__syncwarp\(\);)\n\{ const uint32_t pb = (0u[^;]*);\n((?:a\[\d+\] = tile\[pb \^ \d+u\];\n){16})")
+        pat = re.compile(r"(__syncthreads\(\);\n)?\{ const uint32_t pb = (0u[^;]*);\n(" + decl +
+                         r"(?:ts\d\[\d+u\] = a\[\d+\];\n){16})\}\n"
+                         r"(__syncthreads\(\);|__syncwarp\(\);)\n\{ const uint32_t pb = (0u[^;]*);\n(" + decl +
+                         r"(?:a\[\d+\] = tl\d\[\d+u\];\n){16})")
     else:
-        pat = re.compile(r"(__syncthreads\(\);\n)?\{ ulonglong2\* pt = reinterpret_cast<ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
-                         r"((?:pt\[pb \^ \d+u\] = .*\n){8})\}\n(__syncthreads\(\);|__syncwarp\(\);)\n"
-                         r"\{ const ulonglong2\* pt = reinterpret_cast<const ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n"
-                         r"((?:\{ const ulonglong2 u = pt\[pb \^ \d+u\].*\n){8})")
+        pat = re.compile(r"(__syncthreads\(\);\n)?\{ ulonglong2\* pt = reinterpret_cast<ulonglong2\*>\(tile\); "
+                         r"const uint32_t pb = (0u[^;]*);\n(" + decl + r"(?:ts\d\[\d+u\] = .*\n){8})\}\n"
+                         r"(__syncthreads\(\);|__syncwarp\(\);)\n"
+                         r"\{ const ulonglong2\* pt = reinterpret_cast<const ulonglong2\*>\(tile\); const uint32_t pb = (0u[^;]*);\n("
+                         + decl + r"(?:\{ const ulonglong2 u = tl\d\[\d+u\].*\n){8})")
     out = []
     for m in pat.finditer(kernel):
         def units(expr, body):
             terms = [(w, int(i), int(c, 16)) for w, i, c in TERM.findall(expr)]
             assert len(terms) == 7
-            offs = [int(x) for x in re.findall(r"pb \^ (\d+)u", body)]
+            low = {nm: int(v) for nm, v in re.findall(r"auto\* const (t[sl]\d) = \w+ \+ \(pb \^ (\d)u\);", body)}
+            accs = re.findall(r"(t[sl]\d)\[(\d+)u\]", body)
+            assert len(accs) in (8, 16)
             res = []
             for t in range(128):
                 lane, wid = t & 31, t >> 5
@@ -38,7 +50,7 @@ def exchanges(kernel, precision):
                 for w, i, c in terms:
                     if ((lane if w == "lane" else wid) >> i) & 1:
                         base ^= c
-                res.append([base ^ o for o in offs])
+                res.append([(base ^ low[nm]) + int(k) for nm, k in accs])
             return res
         out.append((m.group(1) is not None, units(m.group(2), m.group(3)), units(m.group(5), m.group(6)),
                     m.group(4) == "__syncwarp();"))
@@ -66,7 +78,7 @@ def test_generated_exchanges(name, n, make, flags, precision):
     for k in kernels:
         xs = exchanges(k, precision)
         # every exchange of the kernel was recognised
-        assert len(xs) == (k.count("tile[pb ^") // 32 if precision == "f64" else k.count("make_ulonglong2") // 8)
+        assert len(xs) == (k.count("= a[") // 16 if precision == "f64" else k.count("make_ulonglong2") // 8)
         prev_load = None
         for i, (barrier, st, ld, warp_local) in enumerate(xs):
             if warp_local:

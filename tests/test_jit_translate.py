@@ -58,7 +58,8 @@ def test_literal_exchange_and_condition_forms():
     ops = [C.Op(C.H, [q]) for q in range(n)] + [C.Op(C.CNOT, [q, (q + 7) % n]) for q in range(n)]
     src, npasses = qb.jit_translate(n, ops, compile=False)
     assert npasses >= 1
-    assert "tile[pb ^" in src
+    assert re.search(r"auto\* const ts\d = tile \+ \(pb \^ \du\);", src)  # exchange pointers: literal offsets
+    assert re.search(r"ts\d\[\d+u\] = a\[\d+\];", src)
     assert re.search(r"\(\(tw & 0x[0-9a-f]+u\) == 0x[0-9a-f]+u\)", src)
 
 
