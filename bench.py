@@ -388,7 +388,7 @@ def run_ours(args):
                   "inverse_roundtrip_rel_l2": r_inv, "inverse_roundtrip_infidelity": f_inv,
                   "tolerance": 1e-12,
                   "note": "full-size checks: the pass plan against the per-gate kernels, and circuit + inverse "
-                          "= identity; the oracle is compared on the same plans at 26 and 28 qubits (tests)"}
+                          "= identity; the oracle is compared on the same plans at 26 and 28 qubits (tests) and on this 30-qubit circuit by the slow test (QOA_SLOW_TESTS=1)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
