@@ -126,9 +126,15 @@ cudaError_t launch_small_batch(bool f32, const SmallCircuit* circs, uint32_t cou
                                const uint64_t* masks, double* out, unsigned int* counter, int max_n, int threads,
                                int ctas_per_sm, cudaStream_t st) {
     const size_t smem = (size_t)(f32 ? sizeof(float2) : sizeof(double2)) << max_n;
+    // the attribute allows the largest state the kernel takes, the same for
+    // every call: batches prepared on several host threads (the server's
+    // workers) launch it concurrently with different sizes, and a smaller
+    // setting made between another thread's set-up and launch fails that launch
+    const int smem_cap = (int)((f32 ? sizeof(float2) : sizeof(double2)) << (f32 ? SMALL_MAX_F32 : SMALL_MAX_F64));
+    if ((int)smem > smem_cap) return cudaErrorInvalidValue;
     cudaError_t e;
-    if (f32) e = cudaFuncSetAttribute(k_small_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else e = cudaFuncSetAttribute(k_small_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (f32) e = cudaFuncSetAttribute(k_small_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
+    else e = cudaFuncSetAttribute(k_small_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;

@@ -2198,6 +2198,14 @@ struct qoa_batch_s {
     SampleJob* d_sjobs = nullptr;
     double* d_trees = nullptr;
     uint32_t n_sjobs = 0;
+    // host copy of the arena passes' parameters, kept (growing only) across
+    // the batch's prepares: pinned for large batches, whose upload is then one
+    // DMA at link speed rather than a staged pageable copy; pageable below
+    // kPinnedMinPasses passes, where pinning pages (per batch handle, e.g.
+    // each server worker's) costs more than the copy it speeds up
+    PassParams* h_params = nullptr;
+    size_t h_params_cap = 0;
+    std::vector<PassParams> h_pageable;
     // view route
     std::vector<qoa_state_t> views;
     std::vector<int> view_circ;
@@ -2256,6 +2264,49 @@ template <typename T>
 void dfree(T*& p, cudaStream_t st) {
     if (p) cudaFreeAsync((void*)p, st);  // stream-ordered: no device-wide synchronisation
     p = nullptr;
+}
+
+// Pinned host buffers for batches' pass parameters, kept when a batch goes
+// so that the next one (a fresh batch per request, a server chunk) skips the
+// page pinning: up to four, the smallest dropped first.
+std::mutex g_hp_mu;
+std::vector<std::pair<PassParams*, size_t>> g_hp_free;
+constexpr size_t kPinnedMinPasses = 16384;  // ~460 MB of pass parameters
+
+cudaError_t pinned_params_take(size_t n, PassParams*& p, size_t& cap) {
+    {
+        std::lock_guard<std::mutex> lk(g_hp_mu);
+        size_t best = g_hp_free.size();
+        for (size_t i = 0; i < g_hp_free.size(); ++i)
+            if (g_hp_free[i].second >= n && (best == g_hp_free.size() || g_hp_free[i].second < g_hp_free[best].second))
+                best = i;
+        if (best < g_hp_free.size()) {
+            p = g_hp_free[best].first;
+            cap = g_hp_free[best].second;
+            g_hp_free.erase(g_hp_free.begin() + (long)best);
+            return cudaSuccess;
+        }
+    }
+    const cudaError_t e = cudaMallocHost((void**)&p, n * sizeof(PassParams));
+    cap = e == cudaSuccess ? n : 0;
+    if (e != cudaSuccess) p = nullptr;
+    return e;
+}
+
+void pinned_params_give(PassParams* p, size_t cap) {
+    PassParams* drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_hp_mu);
+        g_hp_free.push_back({p, cap});
+        if (g_hp_free.size() > 4) {
+            size_t small = 0;
+            for (size_t i = 1; i < g_hp_free.size(); ++i)
+                if (g_hp_free[i].second < g_hp_free[small].second) small = i;
+            drop = g_hp_free[small].first;
+            g_hp_free.erase(g_hp_free.begin() + (long)small);
+        }
+    }
+    if (drop) cudaFreeHost(drop);
 }
 
 // Device buffers of a batch: stream-ordered on the batch's first stream, from
@@ -2398,7 +2449,14 @@ int batch_prepare(qoa_batch_t b) {
         masks.insert(masks.end(), b->circs[i].masks.begin(), b->circs[i].masks.end());
     }
     // arena route: every pass of every circuit, built on the host
-    std::vector<PassParams> p64;
+    struct {
+        PassParams* p = nullptr;
+        size_t n = 0;
+        size_t size() const { return n; }
+        bool empty() const { return n == 0; }
+        PassParams& operator[](size_t i) const { return p[i]; }
+        const PassParams* data() const { return p; }
+    } p64;
     std::vector<F32PassParams> p32;
     F32Upload up;
     std::vector<std::vector<uint32_t>> pass_idx(b->circs.size());
@@ -2434,7 +2492,19 @@ int batch_prepare(qoa_batch_t b) {
                 for (size_t k = 0; k < steps_of[i].size(); ++k) jobs.push_back({i, k});
                 np += steps_of[i].size();
             }
-        p64.resize(np);
+        if (np >= kPinnedMinPasses) {
+            if (np > b->h_params_cap) {
+                if (b->h_params) pinned_params_give(b->h_params, b->h_params_cap);
+                b->h_params = nullptr;
+                b->h_params_cap = 0;
+                BCK(pinned_params_take(np, b->h_params, b->h_params_cap));
+            }
+            p64.p = b->h_params;
+        } else {
+            if (b->h_pageable.size() < np) b->h_pageable.resize(np);
+            p64.p = b->h_pageable.data();
+        }
+        p64.n = np;
         std::vector<char> step_ok(jobs.size(), 0);
         parallel_for(jobs.size(), [&](size_t x) {
             const size_t i = jobs[x].first, k = jobs[x].second;
@@ -3783,6 +3853,7 @@ int qoa_batch_destroy(qoa_batch_t b) {
     for (cudaStream_t st : b->streams) cudaStreamSynchronize(st);
     for (cudaStream_t st : b->rstreams) cudaStreamSynchronize(st);
     batch_free_device(b);
+    if (b->h_params) pinned_params_give(b->h_params, b->h_params_cap);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
     for (cudaStream_t st : b->streams) cudaStreamDestroy(st);
     for (cudaEvent_t e : b->revents) cudaEventDestroy(e);
