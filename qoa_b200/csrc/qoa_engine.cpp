@@ -1186,13 +1186,15 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
         if (!getenv("QOA_NO_ORDER_LANES")) order_lanes(nm);
         return exchange_to(nm);
     };
+    int outer_k[64];  // position of each outer qubit among outer_qubits (-1: in the tile)
+    for (int q = 0; q < 64; ++q) outer_k[q] = -1;
+    for (int k = 0; k < no; ++k) outer_k[P.outer_qubits[k]] = k;
     auto cond = [&](uint64_t mask, PassOp& op) {
-        for (int q = 0; q < 64; ++q) {
-            if (!((mask >> q) & 1)) continue;
+        for (uint64_t mm = mask; mm; mm &= mm - 1) {
+            const int q = __builtin_ctzll(mm);
             const int t = tbit(q);
             if (t < 0) {  // outside the tile: the CTA's tile-number bit of that qubit
-                for (int k = 0; k < no; ++k)
-                    if (P.outer_qubits[k] == q) op.tmask |= 1ull << (LANE_BITS + WARP_BITS + k);
+                if (outer_k[q] >= 0) op.tmask |= 1ull << (LANE_BITS + WARP_BITS + outer_k[q]);
                 continue;
             }
             for (int k = 0; k < LANE_BITS; ++k)
