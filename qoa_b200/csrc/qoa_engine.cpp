@@ -24,6 +24,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <array>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -938,11 +939,15 @@ int build_pass(const std::vector<Gate>& G, const Step& st, uint32_t n, PassParam
             }
         }
     }
-    auto next_use = [&](int from, int t) {
-        for (int i = from; i < ng; ++i)
-            if (need[i] == t) return i;
-        return 1 << 30;
-    };
+    // next_use(from, t): the first gate at or after `from` that needs tile
+    // bit t in a register (1 << 30: none), tabled by a backward sweep
+    std::vector<std::array<int, TILE_BITS>> nu((size_t)ng + 1);
+    nu[ng].fill(1 << 30);
+    for (int i = ng - 1; i >= 0; --i) {
+        nu[i] = nu[i + 1];
+        if (need[i] >= 0) nu[i][need[i]] = i;
+    }
+    auto next_use = [&](int from, int t) { return from >= ng ? (1 << 30) : nu[from][t]; };
 
     TileMap m;  // mapping in force
     // initial mapping: lanes on tile bits 0..4; registers = the four high
