@@ -9,6 +9,9 @@
 //   apply_noise / normalize        src/runtime/quantum_state.rs:839-907
 //   matrix set-up per gate         src/vectorization.rs:16-902
 #include <cuda_runtime.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include <algorithm>
 #include <memory>
@@ -180,13 +183,56 @@ __attribute__((target("avx2"))) uint64_t noise_hits_avx2(uint64_t seed, uint64_t
                       (uint32_t)stream, q0, n, p);
     return h;
 }
+// Sixteen counters per 512-bit register, one 32-bit word of each: a round's
+// 32 x 32 -> 64-bit products come from two even-lane multiplies (the odd
+// lanes shifted down), their high and low words blended back into lanes.
+// The hit test compares the 53-bit mantissa source m = (w0:w1) >> 11 with
+// U = ceil(p * 2^53) as the pair (w0, w1 >> 11) against (U >> 21, U mod
+// 2^21): m * 2^-53 < p exactly when m < U, for an integer m.
+__attribute__((target("avx512f"))) inline __m512i philox_hi(__m512i a, __m512i m) {
+    const __m512i ev = _mm512_mul_epu32(a, m);
+    const __m512i od = _mm512_mul_epu32(_mm512_srli_epi64(a, 32), m);
+    return _mm512_mask_blend_epi32((__mmask16)0xAAAA, _mm512_srli_epi64(ev, 32), od);
+}
+__attribute__((target("avx512f"))) inline __m512i philox_lo(__m512i a, __m512i m) {
+    return _mm512_mullo_epi32(a, m);
+}
 __attribute__((target("avx512f"))) uint64_t noise_hits_avx512(uint64_t seed, uint64_t stream, uint64_t event,
                                                               uint32_t n, double p) {
+    const double T = std::ceil(p * 9007199254740992.0);  // 2^53
+    if (!(T > 0.0)) return 0;
+    const uint64_t all = n >= 64 ? ~0ull : ((1ull << n) - 1);
+    if (T >= 9007199254740992.0) return all;  // p >= 1: every draw hits
+    const uint64_t U = (uint64_t)T;
+    const __m512i uh = _mm512_set1_epi32((int)(uint32_t)(U >> 21));
+    const __m512i ul = _mm512_set1_epi32((int)(uint32_t)(U & ((1u << 21) - 1)));
+    const __m512i M0 = _mm512_set1_epi32((int)0xD2511F53u), M1 = _mm512_set1_epi32((int)0xCD9E8D57u);
+    const __m512i lane = _mm512_set_epi32(15, 14, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0);
     uint64_t h = 0;
-    for (uint32_t q0 = 0; q0 < n; q0 += 16)
-        h |= hits8<16>((uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)event, (uint32_t)(event >> 32),
-                       (uint32_t)stream, q0, n, p);
-    return h;
+    for (uint32_t q0 = 0; q0 < n; q0 += 16) {
+        __m512i c0 = _mm512_set1_epi32((int)(uint32_t)event);
+        __m512i c1 = _mm512_set1_epi32((int)(uint32_t)(event >> 32));
+        // slot 2(q0 + i) + 1 of lane i
+        __m512i c2 = _mm512_add_epi32(_mm512_slli_epi32(_mm512_add_epi32(lane, _mm512_set1_epi32((int)q0)), 1),
+                                      _mm512_set1_epi32(1));
+        __m512i c3 = _mm512_set1_epi32((int)(uint32_t)stream);
+        uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+        for (int r = 0; r < 10; ++r) {
+            const __m512i h0 = philox_hi(c0, M0), l0 = philox_lo(c0, M0);
+            const __m512i h1 = philox_hi(c2, M1), l1 = philox_lo(c2, M1);
+            const __m512i n0 = _mm512_xor_si512(_mm512_xor_si512(h1, c1), _mm512_set1_epi32((int)k0));
+            const __m512i n2 = _mm512_xor_si512(_mm512_xor_si512(h0, c3), _mm512_set1_epi32((int)k1));
+            c0 = n0; c1 = l1; c2 = n2; c3 = l0;
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const __mmask16 lt = _mm512_cmplt_epu32_mask(c0, uh);
+        const __mmask16 eq = _mm512_cmpeq_epi32_mask(c0, uh);
+        const __mmask16 lo = _mm512_cmplt_epu32_mask(_mm512_srli_epi32(c1, 11), ul);
+        const uint64_t m16 = (uint64_t)(uint16_t)(lt | (eq & lo));
+        h |= m16 << q0;
+    }
+    return h & all;
 }
 #endif
 uint64_t noise_hits(uint64_t seed, uint64_t stream, uint64_t event, uint32_t n, double p) {

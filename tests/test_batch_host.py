@@ -28,7 +28,8 @@ def test_ops_unitary(ops, want):
     assert unitary(6, ops) == want
 
 
-@pytest.mark.parametrize("n,p", [(1, 0.5), (7, 0.3), (15, 1e-3), (33, 0.05), (40, 0.9), (64, 0.2)])
+@pytest.mark.parametrize("n,p", [(1, 0.5), (7, 0.3), (15, 1e-3), (33, 0.05), (40, 0.9), (64, 0.2), (17, 1.0),
+                                 (16, 0.0), (20, 1e-300), (12, 2.0 ** -53), (12, 3 * 2.0 ** -40), (31, 0.999999999)])
 def test_noise_hits_equal_one_draw_per_qubit(n, p):
     # the vectorised hit tests give exactly the per-qubit draws' outcomes
     for seed, stream, ev in [(1, 0, 0), (123456789012345, 7, 99), (2 ** 63 + 5, 0xFFFFFFFF, 2 ** 40 + 3)]:
